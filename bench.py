@@ -1,0 +1,347 @@
+#!/usr/bin/env python3
+"""Benchmark: FP64 FLA_LU_piv at n=16384 (and FLA_Chol) on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one factorization of a fresh matrix):
+  FLA_LU_piv, n = 16384, A i.i.d. U(-1,1) (seeded), column-major FP64 in HBM
+  (2 GiB, larger than L2; restoring A between steps also flushes L2).
+Metric: TFLOP/s = (2/3 n^3) / device time of the factorization, whole job.
+
+Rank 0 prints ONE JSON line.  `value` is the device-timed throughput with A
+resident in HBM (time = CUDA events the library records on its own stream
+around the factorization, max over ranks); `e2e` is the same metric through
+the LAPACK entry point dgetrf_ on pinned host buffers, host<->device copies
+inside the timed region.  `roofline` describes the dominant kernel (the FP64
+DMMA GEMM engine) against the FP64 peak measured in this run with cuBLAS
+DGEMM (MEASURED_PEAKS.json carries no FP64 figure).  `cpu_baseline` times
+the reference libflame's own multithreaded CPU path (SuperMatrix
+FLASH_LU_piv over its built-in BLAS, all host cores) on a bounded sample.
+
+Multi-GPU: a single factorization does not shard ("replicas only"): each
+rank factors its own matrix, `value` = all ranks' flops / max time.
+
+--impl reference: times the reference libflame on the host cores (rank 0
+only; other ranks exit 0) on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "FP64 Chol/LU TFLOP/s & %peak; mixed-IR solve speedup vs FP64 at equal error"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=16384)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region.
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# Reference CPU path.
+# ---------------------------------------------------------------------------
+def reference_lu_sample(n_cpu, reps, nthreads):
+    """FLASH_LU_piv (SuperMatrix, reference built-in BLAS) on `nthreads`
+    host threads; returns (TFLOP/s, seconds, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refbind as R
+    rng = np.random.default_rng(2026)
+    A = rng.uniform(-1, 1, (n_cpu, n_cpu))
+    times = []
+    for _ in range(reps):
+        _, _, r, dt = R.lu_piv_flash(A, nthreads, 256)
+        times.append(dt)
+    t = min(times)
+    tf = (2.0 / 3.0) * n_cpu ** 3 / t / 1e12
+    return tf, sum(times), ("FLASH_LU_piv (SuperMatrix, reference built-in f2c BLAS, block 256) "
+                            "n=%d, best of %d" % (n_cpu, reps))
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    nthreads = os.cpu_count() or 1
+    n_cpu = 3072
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(args.warmup):
+        reference_lu_sample(n_cpu, 1, nthreads)
+    tot = 0.0
+    for _ in range(args.steps):
+        tf, secs, desc = reference_lu_sample(n_cpu, 1, nthreads)
+        vals.append(tf)
+        tot += secs
+    v = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "TFLOP/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * tot / max(1, args.steps), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "FLA_LU_piv FP64, A iid U(-1,1); reference CPU path on a bounded "
+                               "sample (n=%d of the n=%d workload)" % (n_cpu, args.n),
+                   "n": n_cpu, "parallelism": "replicas"},
+        "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": nthreads, "kind": "reference",
+                         "sample": desc},
+        "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# Our path.
+# ---------------------------------------------------------------------------
+def measure_fp64_peak(torch, dev):
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def run_ours(args, rank, world):
+    import ctypes as C
+    import torch
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    sys.path.insert(0, ROOT)
+    import libflame_b200 as F
+    F.init()
+    L = F.lib()
+    n = args.n
+    flops = 2.0 / 3.0 * n ** 3
+    g = torch.Generator(device=dev).manual_seed(1234 + rank)
+    src = (torch.rand((n, n), dtype=torch.float64, device=dev, generator=g) * 2 - 1).t()
+    work = torch.empty((n, n), dtype=torch.float64, device=dev).t()
+    piv = torch.empty(n, dtype=torch.int32, device=dev)
+    vA, vp = F.View(work), F.View(piv)
+
+    def step():
+        work.copy_(src)  # restore the input (also evicts L2: 2 GiB written)
+        torch.cuda.synchronize()
+        r = L.FLA_LU_piv(vA.obj, vp.obj)
+        if r != F.FLA_SUCCESS:
+            raise RuntimeError("FLA_LU_piv returned %d: %s" % (r, F.last_error()))
+        return F.last_op_ms()
+
+    for _ in range(args.warmup):
+        step()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(dev.index if dev.index is not None else 0)
+    sampler.start()
+    l0 = F.kernel_launches()
+    t_wall = time.perf_counter()
+    times = [step() for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall
+    launches = F.kernel_launches() - l0
+    clocks = sampler.stop()
+    if world > 1:
+        torch.distributed.barrier()
+    ms = sum(times) / len(times)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * flops / (ms * 1e-3) / 1e12
+
+    # per-kernel-class profile of one more factorization (outside the timed region)
+    F.profile(True)
+    step()
+    prof = {name: F.profile_read(c) for name, c in
+            [("gemm", F.PROF_GEMM), ("panel", F.PROF_PANEL), ("trsm", F.PROF_TRSM),
+             ("swap", F.PROF_SWAP), ("diag", F.PROF_DIAG)]}
+    F.profile(False)
+    total_ms = F.last_op_ms()
+    gemm_ms, gemm_flops, gemm_n = prof["gemm"]
+
+    result = None
+    if rank == 0:
+        peak = measure_fp64_peak(torch, dev)
+        achieved = gemm_flops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None
+        roofline = {
+            "bound": "tensor", "kernel": "dgemm_tma_kernel (FP64 DMMA, trailing update A22 -= A21 A12)",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak if achieved else None,
+            "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul fp64) measured in this run; "
+                           "MEASURED_PEAKS.json has no FP64 figure",
+            "traffic": None,
+            "launches_per_step": gemm_n,
+            "share_of_step": gemm_ms / total_ms if total_ms > 0 else None,
+            "whole_factorization_frac_of_peak": value / world / peak,
+        }
+        breakdown = {k: {"ms": v[0], "launches": v[2]} for k, v in prof.items()}
+        result = {
+            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "FLA_LU_piv n=%d FP64, A iid U(-1,1) seeded, column-major in HBM" % n,
+                       "n": n, "blocksize": 128, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs (2 GiB) larger than L2; the per-step restore of A also flushes L2"},
+            "roofline": roofline, "breakdown_ms": breakdown,
+            "gpu_launches": launches, "clocks": clocks,
+            "wall_ms_per_step_incl_restore": 1000.0 * t_wall / args.steps,
+        }
+
+    # ---- e2e through the LAPACK ABI with pinned host buffers
+    if rank == 0 and args.e2e_steps > 0:
+        host_src = src.t().contiguous().t().cpu()  # column-major host copy
+        pinned = torch.empty((n, n), dtype=torch.float64).pin_memory().t()
+        ipiv = torch.empty(n, dtype=torch.int32).pin_memory()
+        nn = C.c_int(n)
+        info = C.c_int(0)
+        e2e_t = []
+        for i in range(args.e2e_steps + 1):
+            pinned.copy_(host_src)
+            t0 = time.perf_counter()
+            L.dgetrf_(C.byref(nn), C.byref(nn), C.c_void_p(pinned.data_ptr()), C.byref(nn),
+                      C.c_void_p(ipiv.data_ptr()), C.byref(info))
+            dt = time.perf_counter() - t0
+            if i > 0:  # first call warms the staging buffers
+                e2e_t.append(dt)
+        e2e = statistics.median(e2e_t)
+        result["e2e"] = {"value": flops / e2e / 1e12, "unit": "TFLOP/s",
+                         "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": n * n * 8 + n * 4,
+                         "path": "dgetrf_ on pinned host buffers (wall clock, includes H2D + D2H)"}
+        del pinned, host_src
+
+    # ---- secondary: FP64 FLA_Chol at n=16384 (north-star target)
+    if rank == 0 and not args.no_secondary:
+        del src
+        G = torch.randn((n, n), dtype=torch.float64, device=dev, generator=g)
+        spd_src = (G @ G.t()) / n
+        spd_src.diagonal().add_(1.0)
+        del G
+        vC = F.View(work)
+        ct = []
+        for i in range(4):
+            work.copy_(spd_src)
+            torch.cuda.synchronize()
+            r = L.FLA_Chol(F.FLA_LOWER_TRIANGULAR, vC.obj)
+            if r != F.FLA_SUCCESS:
+                raise RuntimeError("FLA_Chol returned %d" % r)
+            if i > 0:
+                ct.append(F.last_op_ms())
+        cms = statistics.median(ct)
+        result["secondary"] = {"FLA_Chol_n16384_fp64": {"tflops": n ** 3 / 3.0 / (cms * 1e-3) / 1e12,
+                                                        "ms": cms,
+                                                        "frac_of_peak": n ** 3 / 3.0 / (cms * 1e-3) / 1e12 / result["roofline"]["peak"]}}
+
+    # ---- CPU baseline: the reference's multithreaded path, bounded sample
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            nthreads = os.cpu_count() or 1
+            tf, secs, desc = reference_lu_sample(3072, 2, nthreads)
+            result["cpu_baseline"] = {"value": tf, "unit": "TFLOP/s", "cores": nthreads,
+                                      "kind": "reference", "sample": desc}
+        except Exception as e:  # the reference library is test infrastructure
+            result["cpu_baseline"] = {"value": None, "unit": "TFLOP/s", "cores": 0, "kind": "reference",
+                                      "sample": "unavailable: %s" % e}
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

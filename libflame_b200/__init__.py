@@ -1,0 +1,213 @@
+"""libflame_b200: B200-native dense factorizations behind libflame's FLA_Obj API.
+
+The product is the C-ABI shared library ``libflame_b200/libflame_b200.so``
+(built by ``libflame_b200.build``) whose entry points are declared in
+``include/FLAME.h``.  This module is the ctypes binding a Python caller uses
+to reach it: it mirrors the reference FLA_Obj interface (same names,
+argument meaning and return codes) and adds helpers that wrap torch CUDA
+tensors or NumPy arrays as FLA_Obj views.
+
+There is no CPU fallback: importing the binding fails loudly when the shared
+library has not been built.
+"""
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libflame_b200.so")
+
+# Constants: the reference's values (src/base/flamec/include/FLA_macro_defs.h).
+FLA_SUCCESS, FLA_FAILURE = -1, -2
+FLA_FLOAT, FLA_DOUBLE, FLA_INT = 100, 101, 104
+FLA_LEFT, FLA_RIGHT = 210, 211
+FLA_LOWER_TRIANGULAR, FLA_UPPER_TRIANGULAR = 300, 301
+FLA_NO_TRANSPOSE, FLA_TRANSPOSE, FLA_CONJ_TRANSPOSE = 400, 401, 402
+FLA_UNIT_DIAG, FLA_NONUNIT_DIAG = 500, 501
+FLA_NATIVE_PIVOTS, FLA_LAPACK_PIVOTS = 700, 701
+FLA_FORWARD, FLA_BACKWARD = 800, 801
+FLA_COLUMNWISE, FLA_ROWWISE = 900, 901
+FLA_NO_ERROR_CHECKING, FLA_MIN_ERROR_CHECKING, FLA_FULL_ERROR_CHECKING = 0, 1, 2
+
+
+class FLA_Obj(C.Structure):
+    """FLA_Obj view, passed by value (include/FLAME.h; reference layout
+    src/base/flamec/include/FLA_type_defs.h:168-180)."""
+    _fields_ = [("offm", C.c_ulong), ("offn", C.c_ulong), ("m", C.c_ulong), ("n", C.c_ulong),
+                ("m_inner", C.c_ulong), ("n_inner", C.c_ulong), ("base", C.c_void_p)]
+
+
+_lib = None
+
+_SIGS = {
+    # name: (restype, argtypes)
+    "FLA_Init": (None, []),
+    "FLA_Finalize": (None, []),
+    "FLA_Initialized": (C.c_int, []),
+    "FLA_Check_error_level": (C.c_uint, []),
+    "FLA_Check_error_level_set": (C.c_uint, [C.c_uint]),
+    "FLA_Obj_create": (C.c_int, [C.c_int, C.c_ulong, C.c_ulong, C.c_ulong, C.c_ulong, C.POINTER(FLA_Obj)]),
+    "FLA_Obj_create_without_buffer": (C.c_int, [C.c_int, C.c_ulong, C.c_ulong, C.POINTER(FLA_Obj)]),
+    "FLA_Obj_attach_buffer": (C.c_int, [C.c_void_p, C.c_ulong, C.c_ulong, C.POINTER(FLA_Obj)]),
+    "FLA_Obj_free": (C.c_int, [C.POINTER(FLA_Obj)]),
+    "FLA_Obj_free_without_buffer": (C.c_int, [C.POINTER(FLA_Obj)]),
+    "FLA_Obj_length": (C.c_ulong, [FLA_Obj]),
+    "FLA_Obj_width": (C.c_ulong, [FLA_Obj]),
+    "FLA_Obj_buffer_at_view": (C.c_void_p, [FLA_Obj]),
+    "FLA_Chol": (C.c_int, [C.c_int, FLA_Obj]),
+    "FLA_LU_piv": (C.c_int, [FLA_Obj, FLA_Obj]),
+    "FLA_Apply_pivots": (C.c_int, [C.c_int, C.c_int, FLA_Obj, FLA_Obj]),
+    "FLA_Shift_pivots_to": (C.c_int, [C.c_int, FLA_Obj]),
+    "FLA_Chol_solve": (C.c_int, [C.c_int, FLA_Obj, FLA_Obj, FLA_Obj]),
+    "FLA_LU_piv_solve": (C.c_int, [FLA_Obj, FLA_Obj, FLA_Obj, FLA_Obj]),
+    "FLA_B200_kernel_launches": (C.c_ulonglong, []),
+    "FLA_B200_last_error": (C.c_char_p, []),
+    "FLA_B200_num_sms": (C.c_int, []),
+    "FLA_B200_last_op_ms": (C.c_double, []),
+    "FLA_B200_profile": (None, [C.c_int]),
+    "FLA_B200_profile_read": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                        C.POINTER(C.c_ulonglong)]),
+    "FLA_B200_dgemm": (C.c_int, [C.c_int, C.c_int, C.c_long, C.c_long, C.c_long, C.c_double,
+                                 C.c_void_p, C.c_long, C.c_void_p, C.c_long, C.c_double,
+                                 C.c_void_p, C.c_long, C.c_int]),
+}
+
+_OPTIONAL = set()
+
+
+def lib():
+    """Load the shared library (raises when it is missing: no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libflame_b200.so is not built; run `python -m libflame_b200.build` "
+                              "(there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            try:
+                f = getattr(L, name)
+            except AttributeError:
+                if name in _OPTIONAL:
+                    continue
+                raise
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    """Names of the C entry points the binding declares."""
+    return list(_SIGS.keys())
+
+
+# ---------------------------------------------------------------------------
+# Wrapping buffers as FLA_Obj views.
+# ---------------------------------------------------------------------------
+class View:
+    """An FLA_Obj view over a caller-owned buffer (torch tensor or NumPy
+    array), column-major.  Keeps the buffer alive; frees the base object on
+    deletion (never the buffer, which is borrowed)."""
+
+    def __init__(self, buf, dt=None):
+        import numpy as np
+        self.buf = buf
+        if hasattr(buf, "data_ptr"):  # torch tensor
+            import torch
+            t = buf
+            if t.dim() == 1:
+                m, n, ld = t.shape[0], 1, max(t.shape[0], 1)
+                assert t.stride(0) == 1
+            else:
+                m, n = t.shape
+                assert t.stride(0) == 1, "tensor must be column-major (stride(0) == 1)"
+                ld = max(t.stride(1), 1)
+            ptr = t.data_ptr()
+            if dt is None:
+                dt = {torch.float64: FLA_DOUBLE, torch.float32: FLA_FLOAT, torch.int32: FLA_INT}[t.dtype]
+        else:
+            a = buf
+            if a.ndim == 1:
+                m, n, ld = a.shape[0], 1, max(a.shape[0], 1)
+            else:
+                assert a.flags["F_CONTIGUOUS"], "array must be Fortran-ordered"
+                m, n = a.shape
+                ld = max(m, 1)
+            ptr = a.ctypes.data
+            if dt is None:
+                dt = {np.dtype(np.float64): FLA_DOUBLE, np.dtype(np.float32): FLA_FLOAT,
+                      np.dtype(np.int32): FLA_INT}[a.dtype]
+        self.obj = FLA_Obj()
+        L = lib()
+        L.FLA_Obj_create_without_buffer(dt, m, n, C.byref(self.obj))
+        L.FLA_Obj_attach_buffer(C.c_void_p(ptr), 1, ld, C.byref(self.obj))
+
+    def __del__(self):
+        try:
+            lib().FLA_Obj_free_without_buffer(C.byref(self.obj))
+        except Exception:
+            pass
+
+
+def init():
+    lib().FLA_Init()
+
+
+def last_error():
+    return lib().FLA_B200_last_error().decode()
+
+
+def kernel_launches():
+    return int(lib().FLA_B200_kernel_launches())
+
+
+def last_op_ms():
+    """Device time of the last factorization/solve call (CUDA events)."""
+    return float(lib().FLA_B200_last_op_ms())
+
+
+PROF_GEMM, PROF_PANEL, PROF_TRSM, PROF_SWAP, PROF_DIAG, PROF_OTHER = range(6)
+
+
+def profile(on=True):
+    lib().FLA_B200_profile(1 if on else 0)
+
+
+def profile_read(cls):
+    ms, fl, n = C.c_double(), C.c_double(), C.c_ulonglong()
+    lib().FLA_B200_profile_read(cls, C.byref(ms), C.byref(fl), C.byref(n))
+    return ms.value, fl.value, n.value
+
+
+# Thin Python mirrors of the reference calls on buffers (return codes as in
+# C).  The views are held in locals for the duration of the call: a View
+# frees its FLA_Obj base when it is collected.
+def chol(A, uplo=FLA_LOWER_TRIANGULAR):
+    """FLA_Chol(uplo, A) on a column-major buffer, in place."""
+    va = View(A)
+    return lib().FLA_Chol(uplo, va.obj)
+
+
+def lu_piv(A, p):
+    """FLA_LU_piv(A, p) in place; p int32 vector of length >= min(m, n)."""
+    va, vp = View(A), View(p)
+    return lib().FLA_LU_piv(va.obj, vp.obj)
+
+
+def apply_pivots(p, A, trans=FLA_NO_TRANSPOSE):
+    vp, va = View(p), View(A)
+    return lib().FLA_Apply_pivots(FLA_LEFT, trans, vp.obj, va.obj)
+
+
+def chol_solve(A, B, X, uplo=FLA_LOWER_TRIANGULAR):
+    va, vb, vx = View(A), View(B), View(X)
+    return lib().FLA_Chol_solve(uplo, va.obj, vb.obj, vx.obj)
+
+
+def lu_piv_solve(A, p, B, X):
+    va, vp, vb, vx = View(A), View(p), View(B), View(X)
+    return lib().FLA_LU_piv_solve(va.obj, vp.obj, vb.obj, vx.obj)
+
+
+def shift_pivots_to(ptype, p):
+    vp = View(p)
+    return lib().FLA_Shift_pivots_to(ptype, vp.obj)

@@ -1,0 +1,221 @@
+// FP64 Cholesky factorization (FLA_Chol) on the GPU.
+//
+// Right-looking blocked algorithm with the reference's structure
+// (src/lapack/dec/chol/l/flamec/FLA_Chol_l_blk_var3.c:13-66):
+//   for each 128-column block:  A11 := chol(A11)        [potrf_diag_kernel]
+//                               A21 := A21 inv(A11)^T   [trsm_rlt_kernel]
+//                               A22 -= A21 A21^T (lower) [DMMA GEMM engine]
+// The diagonal block is factored in shared memory in 32-column steps (the
+// reference's inner blocksize, FLA_Chol_cntl_init.c:23-61): a warp factors
+// each 32x32 block (the unblocked var2/var3 leaf), the rows below are solved
+// against it and the trailing part of the block is updated, all in SMEM.
+// A failing pivot (<= 0 or NaN, bl1_dsqrte in
+// src/base/flamec/blis/include/blis_macro_defs.h:134-136) records the
+// zero-based global column in the status block; every later kernel of the
+// factorization sees it and returns without touching memory.
+#include <climits>
+
+#include "common.h"
+#include "dev_util.cuh"
+
+namespace fb {
+
+namespace {
+
+constexpr int NB = 128;        // outer block
+constexpr int IB = 32;         // inner block
+constexpr int LDS = NB + 1;    // SMEM leading dimension (odd: spreads banks)
+constexpr int POTRF_THREADS = 256;
+constexpr int POTRF_SMEM = NB * LDS * 8;
+
+__device__ __forceinline__ bool guard_failed(const int* info) {
+  return *((volatile const int*)info) != INT_MAX;
+}
+
+// Factor the b x b (b <= 128) lower-triangular diagonal block at A (ld) in
+// place.  gcol = global index of its first column (for the info word).
+__global__ void __launch_bounds__(POTRF_THREADS) potrf_diag_kernel(double* A, long ld, int b, int gcol,
+                                                                   int* info) {
+  extern __shared__ double S[];  // S[r + c*LDS]
+  __shared__ int s_fail;
+  if (guard_failed(info)) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // load lower triangle (and diagonal); upper part of S is never read
+  for (int c = warp; c < b; c += POTRF_THREADS / 32)
+    for (int r = c + lane; r < b; r += 32) S[r + c * LDS] = A[r + (long)c * ld];
+  if (tid == 0) s_fail = -1;
+  __syncthreads();
+
+  for (int jb = 0; jb < b; jb += IB) {
+    const int w = min(IB, b - jb);
+    // (a) warp 0: unblocked Cholesky of the w x w diagonal block
+    if (warp == 0) {
+      for (int j = 0; j < w; ++j) {
+        double d = 0.0;
+        int bad = 0;
+        if (lane == j) {
+          d = S[(jb + j) + (jb + j) * LDS];
+          if (!(d > 0.0)) bad = 1;  // <= 0 or NaN
+          else d = sqrt(d);
+        }
+        d = __shfl_sync(0xffffffffu, d, j);
+        bad = __shfl_sync(0xffffffffu, bad, j);
+        if (bad) {
+          if (lane == 0) s_fail = jb + j;
+          break;
+        }
+        if (lane == j) S[(jb + j) + (jb + j) * LDS] = d;
+        const double rinv = 1.0 / d;
+        if (lane > j && lane < w) S[(jb + lane) + (jb + j) * LDS] *= rinv;
+        __syncwarp();
+        if (lane > j && lane < w) {
+          const double lij = S[(jb + lane) + (jb + j) * LDS];
+          for (int c = j + 1; c <= lane; ++c)
+            S[(jb + lane) + (jb + c) * LDS] -= lij * S[(jb + c) + (jb + j) * LDS];
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    if (s_fail >= 0) break;
+    const int r0 = jb + w;  // first row below the diagonal block
+    // (b) rows below: X := X inv(D)^T, one thread per row (right-looking,
+    //     multiply by the reciprocal of the pivot like dtrsm R,L,T,N)
+    for (int r = r0 + tid; r < b; r += POTRF_THREADS) {
+      for (int j = 0; j < w; ++j) {
+        const double x = S[r + (jb + j) * LDS] * (1.0 / S[(jb + j) + (jb + j) * LDS]);
+        S[r + (jb + j) * LDS] = x;
+        for (int c = j + 1; c < w; ++c) S[r + (jb + c) * LDS] -= x * S[(jb + c) + (jb + j) * LDS];
+      }
+    }
+    __syncthreads();
+    // (c) trailing lower triangle of the block: S22 -= X X^T
+    const int m2 = b - r0;
+    const int nel = m2 * (m2 + 1) / 2;
+    for (int e = tid; e < nel; e += POTRF_THREADS) {
+      // map e -> (i, c) with c <= i, column-major over the lower triangle
+      int c = (int)((2.0 * m2 + 1.0 - sqrt((2.0 * m2 + 1.0) * (2.0 * m2 + 1.0) - 8.0 * e)) * 0.5);
+      int start = c * m2 - c * (c - 1) / 2;
+      while (start > e) { --c; start = c * m2 - c * (c - 1) / 2; }
+      while (start + (m2 - c) <= e) { start += m2 - c; ++c; }
+      const int i = c + (e - start);
+      double s = 0.0;
+      for (int j = 0; j < w; ++j) s += S[(r0 + i) + (jb + j) * LDS] * S[(r0 + c) + (jb + j) * LDS];
+      S[(r0 + i) + (r0 + c) * LDS] -= s;
+    }
+    __syncthreads();
+  }
+  // write back the lower triangle (the strictly upper part of A is untouched)
+  for (int c = warp; c < b; c += POTRF_THREADS / 32)
+    for (int r = c + lane; r < b; r += 32) A[r + (long)c * ld] = S[r + c * LDS];
+  if (tid == 0 && s_fail >= 0) atomicMin(info, gcol + s_fail);
+}
+
+// X := X inv(L)^T for the m x b block X (ld ldx) and the b x b lower L
+// (ld ldl), b <= 128.  64 rows per CTA, 4 threads per row, each thread
+// holding every 4th column of its row in registers.
+constexpr int TRSM_ROWS = 64;
+constexpr int TRSM_THREADS = TRSM_ROWS * 4;
+__global__ void __launch_bounds__(TRSM_THREADS) trsm_rlt_kernel(const double* L, long ldl, double* X,
+                                                                long ldx, int m, int b,
+                                                                const int* info) {
+  extern __shared__ double SL[];  // L lower, column-major, ld NB
+  __shared__ double sdinv[NB];
+  if (guard_failed(info)) return;
+  const int tid = threadIdx.x;
+  for (int c = tid >> 5; c < b; c += TRSM_THREADS / 32)
+    for (int r = (tid & 31); r < b; r += 32) SL[r + c * NB] = (r >= c) ? L[r + (long)c * ldl] : 0.0;
+  __syncthreads();
+  for (int j = tid; j < b; j += TRSM_THREADS) sdinv[j] = 1.0 / SL[j + j * NB];
+  __syncthreads();
+  const int q = tid & 3;              // column phase of this thread
+  const int row = blockIdx.x * TRSM_ROWS + (tid >> 2);
+  const bool active = row < m;
+  double x[NB / 4];
+#pragma unroll
+  for (int i = 0; i < NB / 4; ++i) {
+    int c = q + 4 * i;
+    x[i] = (active && c < b) ? X[row + (long)c * ldx] : 0.0;
+  }
+  // right-looking substitution over the columns of the row (fully unrolled
+  // so that every register index is a compile-time constant)
+#pragma unroll
+  for (int j = 0; j < NB; ++j) {
+    if (j >= b) break;
+    const int owner = j & 3, slot = j >> 2;
+    double xj = 0.0;
+#pragma unroll
+    for (int i = 0; i < NB / 4; ++i)
+      if (i == slot) xj = x[i];
+    xj = __shfl_sync(0xffffffffu, xj, (threadIdx.x & 31 & ~3) | owner);
+    xj *= sdinv[j];
+    if (q == owner) {
+#pragma unroll
+      for (int i = 0; i < NB / 4; ++i)
+        if (i == slot) x[i] = xj;
+    }
+#pragma unroll
+    for (int i = 0; i < NB / 4; ++i) {
+      int c = q + 4 * i;
+      if (c > j) x[i] -= xj * SL[c + j * NB];
+    }
+  }
+  if (active) {
+#pragma unroll
+    for (int i = 0; i < NB / 4; ++i) {
+      int c = q + 4 * i;
+      if (c < b) X[row + (long)c * ldx] = x[i];
+    }
+  }
+}
+
+bool g_attr_done = false;
+void set_attrs() {
+  if (g_attr_done) return;
+  cudaFuncSetAttribute(potrf_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, POTRF_SMEM);
+  cudaFuncSetAttribute(trsm_rlt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, NB * NB * 8);
+  g_attr_done = true;
+}
+
+}  // namespace
+
+// Enqueue the blocked factorization of the lower triangle of A on `st`.
+int chol_lower_enqueue(DMat A, cudaStream_t st) {
+  set_attrs();
+  const long n = A.m;
+  int* info = ctx().d_status + ST_INFO;
+  for (long k = 0; k < n; k += NB) {
+    const int b = (int)std::min<long>(NB, n - k);
+    double* A11 = A.p + k + k * A.ld;
+    int ps = prof_begin(st);
+    potrf_diag_kernel<<<1, POTRF_THREADS, POTRF_SMEM, st>>>(A11, A.ld, b, (int)k, info);
+    prof_end(ps, st, PROF_DIAG, (double)b * b * b / 3.0);
+    count_launch();
+    const long m2 = n - k - b;
+    if (m2 <= 0) break;
+    double* A21 = A.p + (k + b) + k * A.ld;
+    double* A22 = A.p + (k + b) + (k + b) * A.ld;
+    ps = prof_begin(st);
+    trsm_rlt_kernel<<<(unsigned)((m2 + TRSM_ROWS - 1) / TRSM_ROWS), TRSM_THREADS, NB * NB * 8, st>>>(
+        A11, A.ld, A21, A.ld, (int)m2, b, info);
+    prof_end(ps, st, PROF_TRSM, (double)m2 * b * b);
+    count_launch();
+    int r = gemm_f64(st, false, true, m2, m2, b, -1.0, A21, A.ld, A21, A.ld, 1.0, A22, A.ld,
+                     GEMM_LOWER, 0, info);
+    if (r != FLA_SUCCESS) return r;
+  }
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
+}
+
+int chol_lower_dev(DMat A, int* info) {
+  if (A.m == 0) {
+    *info = -1;
+    return FLA_SUCCESS;
+  }
+  if (status_reset() != FLA_SUCCESS) return FLA_FAILURE;
+  if (chol_lower_enqueue(A, ctx().stream) != FLA_SUCCESS) return FLA_FAILURE;
+  return status_read(info);
+}
+
+}  // namespace fb

@@ -1,0 +1,465 @@
+// LU factorization with partial pivoting (FLA_LU_piv) on the GPU, plus the
+// row-interchange kernel behind FLA_Apply_pivots.
+//
+// Blocked right-looking algorithm with the reference's structure
+// (src/lapack/dec/lu/piv/vars/flamec/FLA_LU_piv_blk_var5.c:13-114):
+//   for each block of nb columns:
+//     [A11;A21], p1 := LU_piv([A11;A21])   lu_panel_kernel (cooperative)
+//     pivot [A10;A20] and [A12;A22]         laswp_kernel
+//     A12 := inv(tril_unit(A11)) A12         trsm_llu_kernel
+//     A22 -= A21 A12                         DMMA GEMM engine
+// Pivot choice is the reference's: the entry of largest magnitude in the
+// current column, the first (smallest row) among equals (idamax,
+// src/flablas/f2c/idamax.c:41,60 via bl1_damax).  A zero pivot column is
+// not swapped or scaled and its index is reported (the first one), and the
+// factorization continues (FLA_LU_piv_opt_var4.c:272-331).
+//
+// Panel kernel: the (m-k) x nb panel is split in row slabs, one per CTA,
+// held in shared memory for the whole panel.  Per column: each CTA finds
+// its local pivot candidate and publishes it (value, row, the full panel
+// row) in global memory; one grid barrier; every CTA then picks the same
+// winner, the owners of rows j and p(j) exchange them, and every CTA
+// scales its part of column j and applies the rank-1 update to its slab.
+#include <climits>
+
+#include "common.h"
+#include "dev_util.cuh"
+
+namespace fb {
+
+namespace {
+
+constexpr int PANEL_THREADS = 256;
+constexpr int NBMAX = 128;
+constexpr size_t PANEL_SMEM_CAP = 200 * 1024;
+
+struct PanelArgs {
+  double* P;         // panel (row k, col k), column-major
+  long ld;
+  int M;             // panel rows (m - k)
+  int nb;            // panel columns
+  int R;             // rows per CTA
+  int lds;           // SMEM leading dimension
+  int G;             // CTAs
+  int gcol;          // global column of panel column 0
+  int* piv;          // out: nb relative pivots
+  double* cand_row;  // [2][G][nb]
+  double* cand_val;  // [2][G]
+  int* cand_idx;     // [2][G]
+  double* diag_row;  // [2][nb]
+  unsigned* bar;     // barrier counter (zeroed before launch)
+  int* err;
+  int* info;
+};
+
+__global__ void __launch_bounds__(PANEL_THREADS) lu_panel_kernel(PanelArgs a) {
+  extern __shared__ double S[];  // slab: S[i + col*lds], then u row
+  __shared__ double s_rv[PANEL_THREADS / 32];
+  __shared__ int s_ri[PANEL_THREADS / 32];
+  __shared__ int s_ci, s_w, s_r;
+  double* su = S + (size_t)a.lds * a.nb;  // nb doubles
+
+  const int c = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int r0 = c * a.R;
+  const int rows = min(a.R, a.M - r0);
+  const int nb = a.nb, lds = a.lds, G = a.G;
+
+  for (int col = 0; col < nb; ++col)
+    for (int i = tid; i < rows; i += PANEL_THREADS) S[i + col * lds] = a.P[(long)(r0 + i) + (long)col * a.ld];
+  __syncthreads();
+
+  int first_null = -1;
+  for (int j = 0; j < nb; ++j) {
+    const int par = j & 1;
+    // ---- 1. local candidate: max |a(i,j)|, smallest row on ties, rows >= j
+    double bv = -1.0;
+    int bi = INT_MAX;
+    for (int i = tid; i < rows; i += PANEL_THREADS) {
+      const int gi = r0 + i;
+      if (gi >= j) {
+        const double v = fabs(S[i + j * lds]);
+        if (v > bv || (v == bv && gi < bi)) { bv = v; bi = gi; }
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    }
+    if (lane == 0) { s_rv[warp] = bv; s_ri[warp] = bi; }
+    __syncthreads();
+    if (tid == 0) {
+      double v = s_rv[0];
+      int i0 = s_ri[0];
+      for (int w = 1; w < PANEL_THREADS / 32; ++w)
+        if (s_rv[w] > v || (s_rv[w] == v && s_ri[w] < i0)) { v = s_rv[w]; i0 = s_ri[w]; }
+      __stcg(a.cand_val + par * G + c, v);
+      __stcg(a.cand_idx + par * G + c, i0);
+      s_ci = i0;
+    }
+    __syncthreads();
+    // ---- 2. publish the candidate row and (owner of row j) the row j
+    if (s_ci != INT_MAX) {
+      const int li = s_ci - r0;
+      for (int col = tid; col < nb; col += PANEL_THREADS)
+        __stcg(a.cand_row + ((size_t)par * G + c) * nb + col, S[li + col * lds]);
+    }
+    if (j >= r0 && j < r0 + rows)
+      for (int col = tid; col < nb; col += PANEL_THREADS) __stcg(a.diag_row + par * nb + col, S[(j - r0) + col * lds]);
+    // ---- 3. grid barrier
+    if (!grid_barrier(a.bar, (unsigned)G, (unsigned)(j + 1), a.err, 21)) return;
+    // ---- 4. winner (same on every CTA)
+    if (warp == 0) {
+      double v = -2.0;
+      int i0 = INT_MAX, w0 = 0;
+      for (int w = lane; w < G; w += 32) {
+        const double cv = __ldcg(a.cand_val + par * G + w);
+        const int ci = __ldcg(a.cand_idx + par * G + w);
+        if (ci != INT_MAX && (cv > v || (cv == v && ci < i0))) { v = cv; i0 = ci; w0 = w; }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, i0, off);
+        const int ow = __shfl_xor_sync(0xffffffffu, w0, off);
+        if (ov > v || (ov == v && oi < i0)) { v = ov; i0 = oi; w0 = ow; }
+      }
+      if (lane == 0) { s_w = w0; s_r = i0; }
+    }
+    __syncthreads();
+    const int w = s_w, r = s_r;
+    const double* wrow = a.cand_row + ((size_t)par * G + w) * nb;
+    for (int col = tid; col < nb; col += PANEL_THREADS) su[col] = __ldcg(wrow + col);
+    __syncthreads();
+    const double piv = su[j];
+    if (c == 0 && tid == 0) a.piv[j] = r - j;
+    if (piv == 0.0) {
+      if (first_null < 0) first_null = j;
+    } else if (r != j) {
+      // ---- 5. interchange rows j and r (whole panel row)
+      if (j >= r0 && j < r0 + rows)
+        for (int col = tid; col < nb; col += PANEL_THREADS) S[(j - r0) + col * lds] = su[col];
+      if (r >= r0 && r < r0 + rows)
+        for (int col = tid; col < nb; col += PANEL_THREADS)
+          S[(r - r0) + col * lds] = __ldcg(a.diag_row + par * nb + col);
+    }
+    __syncthreads();
+    // ---- 6. scale column j below the pivot and update the slab
+    if (piv != 0.0) {
+      const double rinv = 1.0 / piv;  // reciprocal multiply, as bl1_dinvscalv
+      for (int i = tid; i < rows; i += PANEL_THREADS) {
+        if (r0 + i > j) {
+          const double l = S[i + j * lds] * rinv;
+          S[i + j * lds] = l;
+          for (int col = j + 1; col < nb; ++col) S[i + col * lds] -= l * su[col];
+        }
+      }
+    }
+    __syncthreads();
+  }
+  for (int col = 0; col < nb; ++col)
+    for (int i = tid; i < rows; i += PANEL_THREADS) a.P[(long)(r0 + i) + (long)col * a.ld] = S[i + col * lds];
+  if (c == 0 && tid == 0 && first_null >= 0) atomicMin(a.info, a.gcol + first_null);
+}
+
+// Row interchanges on a set of columns: for each column, rows row0+i and
+// row0+i+piv[i] are swapped for i = 0..npiv-1 in order (or in reverse when
+// `reverse`, which applies P^T).  Columns: [c0, c0+n0) and [c1, c1+n1).
+__global__ void laswp_kernel(double* A, long ld, int row0, const int* __restrict__ piv, int npiv,
+                             int c0, int n0, int c1, int n1, int reverse) {
+  extern __shared__ int sp[];
+  for (int i = threadIdx.x; i < npiv; i += blockDim.x) sp[i] = piv[i];
+  __syncthreads();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n0 + n1) return;
+  const int col = t < n0 ? c0 + t : c1 + (t - n0);
+  double* a = A + (long)col * ld;
+  if (!reverse) {
+    for (int i = 0; i < npiv; ++i) {
+      const int p = sp[i];
+      if (p != 0) {
+        const long r1 = row0 + i, r2 = r1 + p;
+        const double x = a[r1];
+        a[r1] = a[r2];
+        a[r2] = x;
+      }
+    }
+  } else {
+    for (int i = npiv - 1; i >= 0; --i) {
+      const int p = sp[i];
+      if (p != 0) {
+        const long r1 = row0 + i, r2 = r1 + p;
+        const double x = a[r1];
+        a[r1] = a[r2];
+        a[r2] = x;
+      }
+    }
+  }
+}
+
+// X := inv(op(T)) X for the b x n block X (ld ldx), T b x b triangular
+// (lower if LOWER, else upper; op = transpose if TRANS; unit diagonal if
+// UNIT), b <= 128.  The substitution runs forward when op(T) is lower and
+// backward when it is upper.  64 columns per CTA, 4 threads per column, each
+// holding every 4th row of its column in registers.
+constexpr int TRSM_COLS = 64;
+constexpr int TRSM_THREADS = TRSM_COLS * 4;
+template <bool LOWER, bool TRANS, bool UNIT>
+__global__ void __launch_bounds__(TRSM_THREADS) trsm_left_kernel(const double* T, long ldt, double* X,
+                                                                 long ldx, int b, int n) {
+  extern __shared__ double ST[];  // ld NBMAX, the stored triangle
+  __shared__ double sdinv[NBMAX];
+  constexpr bool FWD = (LOWER != TRANS);
+  const int tid = threadIdx.x;
+  for (int cc = tid >> 5; cc < b; cc += TRSM_THREADS / 32)
+    for (int r = (tid & 31); r < b; r += 32)
+      ST[r + cc * NBMAX] = (LOWER ? (r >= cc) : (r <= cc)) ? T[r + (long)cc * ldt] : 0.0;
+  __syncthreads();
+  if (!UNIT)
+    for (int j = tid; j < b; j += TRSM_THREADS) sdinv[j] = 1.0 / ST[j + j * NBMAX];
+  __syncthreads();
+  const int q = tid & 3;
+  const int col = blockIdx.x * TRSM_COLS + (tid >> 2);
+  const bool active = col < n;
+  double x[NBMAX / 4];
+#pragma unroll
+  for (int i = 0; i < NBMAX / 4; ++i) {
+    const int r = q + 4 * i;
+    x[i] = (active && r < b) ? X[r + (long)col * ldx] : 0.0;
+  }
+  // every register index below is a compile-time constant: the forward
+  // sweep visits j = 0..b-1, the backward sweep j = NBMAX-1..0 skipping the
+  // padding rows j >= b
+#pragma unroll
+  for (int jj = 0; jj < NBMAX; ++jj) {
+    const int j = FWD ? jj : (NBMAX - 1 - jj);
+    if (j < b) {
+      double xj = x[j >> 2];
+      xj = __shfl_sync(0xffffffffu, xj, (threadIdx.x & 31 & ~3) | (j & 3));
+      if (!UNIT) {
+        xj *= sdinv[j];
+        if (q == (j & 3)) x[j >> 2] = xj;
+      }
+#pragma unroll
+      for (int i = 0; i < NBMAX / 4; ++i) {
+        const int r = q + 4 * i;
+        const bool upd = FWD ? (r > j && r < b) : (r < j);
+        if (upd) x[i] -= (TRANS ? ST[j + r * NBMAX] : ST[r + j * NBMAX]) * xj;
+      }
+    }
+  }
+  if (active) {
+#pragma unroll
+    for (int i = 0; i < NBMAX / 4; ++i) {
+      const int r = q + 4 * i;
+      if (r < b) X[r + (long)col * ldx] = x[i];
+    }
+  }
+}
+
+bool g_attrs = false;
+void set_attrs() {
+  if (g_attrs) return;
+  cudaFuncSetAttribute(lu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(220 * 1024));
+#define FB_TRSM_ATTR(L, T, U) \
+  cudaFuncSetAttribute(trsm_left_kernel<L, T, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, NBMAX * NBMAX * 8);
+  FB_TRSM_ATTR(true, false, true) FB_TRSM_ATTR(true, false, false) FB_TRSM_ATTR(true, true, true)
+  FB_TRSM_ATTR(true, true, false) FB_TRSM_ATTR(false, false, true) FB_TRSM_ATTR(false, false, false)
+  FB_TRSM_ATTR(false, true, true) FB_TRSM_ATTR(false, true, false)
+#undef FB_TRSM_ATTR
+  g_attrs = true;
+}
+
+// Panel geometry for an M-row panel: rows per CTA, CTAs, SMEM stride and
+// the widest panel (<= 128, multiple of 16) whose slab fits in SMEM.
+struct PanelGeom {
+  int R, G, lds, nb;
+  size_t smem;
+};
+PanelGeom panel_geom(long M, int nb_max) {
+  Context& cx = ctx();
+  PanelGeom g;
+  int sms = cx.num_sms;
+  g.R = (int)std::max<long>(std::min<long>(M, 32), (M + sms - 1) / sms);
+  g.G = (int)((M + g.R - 1) / g.R);
+  g.lds = g.R | 1;
+  g.nb = nb_max;
+  while (g.nb > 16 && (size_t)g.lds * g.nb * 8 + g.nb * 8 > PANEL_SMEM_CAP) g.nb -= 16;
+  g.smem = (size_t)g.lds * g.nb * 8 + (size_t)g.nb * 8;
+  return g;
+}
+
+}  // namespace
+
+int laswp_dev(double* A, long ld, int row0, const int* d_piv, int npiv, int c0, int n0, int c1,
+              int n1, bool reverse, cudaStream_t st) {
+  const int ncols = n0 + n1;
+  if (ncols <= 0 || npiv <= 0) return FLA_SUCCESS;
+  const int threads = 128;
+  const int ps = prof_begin(st);
+  laswp_kernel<<<(ncols + threads - 1) / threads, threads, npiv * sizeof(int), st>>>(
+      A, ld, row0, d_piv, npiv, c0, n0, c1, n1, reverse ? 1 : 0);
+  prof_end(ps, st, PROF_SWAP, 0.0);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
+}
+
+int apply_pivots_dev(DMat A, const int* d_piv, int k1, int k2, bool reverse, cudaStream_t st) {
+  // FLA_Apply_pivots_ln_opd_var1 (src/lapack/util/app/piv/ln/flamec/
+  // FLA_Apply_pivots_ln_opt_var1.c:274-340): swap rows i and i + p[i].
+  // Pivot blocks of up to 4096 entries per launch (kernel SMEM).
+  const int chunk = 4096;
+  if (!reverse) {
+    for (int i0 = k1; i0 <= k2; i0 += chunk) {
+      int cnt = std::min(chunk, k2 - i0 + 1);
+      if (laswp_dev(A.p, A.ld, i0, d_piv + i0, cnt, 0, (int)A.n, 0, 0, false, st) != FLA_SUCCESS)
+        return FLA_FAILURE;
+    }
+  } else {
+    int nchunks = (k2 - k1 + chunk) / chunk;
+    for (int cidx = nchunks - 1; cidx >= 0; --cidx) {
+      int i0 = k1 + cidx * chunk;
+      int cnt = std::min(chunk, k2 - i0 + 1);
+      if (laswp_dev(A.p, A.ld, i0, d_piv + i0, cnt, 0, (int)A.n, 0, 0, true, st) != FLA_SUCCESS)
+        return FLA_FAILURE;
+    }
+  }
+  return FLA_SUCCESS;
+}
+
+// B := inv(op(T)) B for a b x n block B, T b x b (b <= 128) triangular.
+int trsm_block(const double* T, long ldt, double* B, long ldb, int b, long n, bool lower,
+               bool trans, bool unit, cudaStream_t st) {
+  set_attrs();
+  if (n <= 0 || b <= 0) return FLA_SUCCESS;
+  unsigned grid = (unsigned)((n + TRSM_COLS - 1) / TRSM_COLS);
+  const size_t sm = NBMAX * NBMAX * 8;
+  const int ps = prof_begin(st);
+#define FB_TRSM_LAUNCH(L, T_, U) \
+  trsm_left_kernel<L, T_, U><<<grid, TRSM_THREADS, sm, st>>>(T, ldt, B, ldb, b, (int)n)
+  if (lower) {
+    if (!trans) { if (unit) FB_TRSM_LAUNCH(true, false, true); else FB_TRSM_LAUNCH(true, false, false); }
+    else        { if (unit) FB_TRSM_LAUNCH(true, true, true);  else FB_TRSM_LAUNCH(true, true, false); }
+  } else {
+    if (!trans) { if (unit) FB_TRSM_LAUNCH(false, false, true); else FB_TRSM_LAUNCH(false, false, false); }
+    else        { if (unit) FB_TRSM_LAUNCH(false, true, true);  else FB_TRSM_LAUNCH(false, true, false); }
+  }
+#undef FB_TRSM_LAUNCH
+  prof_end(ps, st, PROF_TRSM, (double)b * (double)b * (double)n);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
+}
+
+// Blocked left triangular solve  B := inv(op(T)) B  for an n x n triangular
+// T and an n x nrhs block B: 128-row diagonal solves (trsm_block) and GEMM
+// updates of the rows not yet solved.  Replaces the dtrsm_ calls of
+// FLA_Chol_solve / FLA_LU_piv_solve (FLA_Chol_solve.c:24-33,
+// FLA_LU_piv_solve.c:22-27).
+int trsm_left_dev(DMat T, DMat B, bool lower, bool trans, bool unit, cudaStream_t st) {
+  const long n = T.m, nr = B.n;
+  if (n == 0 || nr == 0) return FLA_SUCCESS;
+  const bool fwd = (lower != trans);
+  const long nblk = (n + NBMAX - 1) / NBMAX;
+  for (long bi = 0; bi < nblk; ++bi) {
+    const long jb = fwd ? bi * NBMAX : (nblk - 1 - bi) * NBMAX;
+    const int b = (int)std::min<long>(NBMAX, n - jb);
+    const double* Tjj = T.p + jb + jb * T.ld;
+    double* Bj = B.p + jb;
+    if (trsm_block(Tjj, T.ld, Bj, B.ld, b, nr, lower, trans, unit, st) != FLA_SUCCESS) return FLA_FAILURE;
+    if (fwd) {
+      const long rest = n - jb - b;
+      if (rest <= 0) continue;
+      // rows below: B2 -= op(T)(jb+b:, jb:jb+b) Bj
+      const double* Tblk = trans ? (T.p + jb + (jb + b) * T.ld)   // stored b x rest (upper, transposed)
+                                 : (T.p + (jb + b) + jb * T.ld);  // stored rest x b (lower)
+      if (gemm_f64(st, trans, false, rest, nr, b, -1.0, Tblk, T.ld, Bj, B.ld, 1.0, B.p + jb + b, B.ld) !=
+          FLA_SUCCESS)
+        return FLA_FAILURE;
+    } else {
+      if (jb == 0) continue;
+      // rows above: B0 -= op(T)(0:jb, jb:jb+b) Bj
+      const double* Tblk = trans ? (T.p + jb)               // stored b x jb (lower, transposed)
+                                 : (T.p + jb * T.ld);       // stored jb x b (upper)
+      if (gemm_f64(st, trans, false, jb, nr, b, -1.0, Tblk, T.ld, Bj, B.ld, 1.0, B.p, B.ld) != FLA_SUCCESS)
+        return FLA_FAILURE;
+    }
+  }
+  return FLA_SUCCESS;
+}
+
+int lu_piv_dev(DMat A, int* d_piv, int* info) {
+  set_attrs();
+  Context& cx = ctx();
+  cudaStream_t st = cx.stream;
+  const long m = A.m, n = A.n, mn = std::min(m, n);
+  *info = -1;
+  if (mn == 0) return FLA_SUCCESS;
+  if (status_reset() != FLA_SUCCESS) return FLA_FAILURE;
+  PanelGeom g0 = panel_geom(m, NBMAX);
+  const int NBL = g0.nb;  // outer blocksize for the whole factorization
+  // panel scratch: candidates for the widest (first) panel
+  const int GMAX = cx.num_sms;  // every panel launch has G <= num_sms CTAs
+  size_t need = sizeof(double) * ((size_t)2 * GMAX * NBL + 2 * GMAX + 2 * NBL) + sizeof(int) * 2 * GMAX + 256;
+  char* ws = (char*)ws_get(WS_PANEL, need);
+  if (!ws) return FLA_FAILURE;
+  double* cand_row = (double*)ws;
+  double* cand_val = cand_row + (size_t)2 * GMAX * NBL;
+  double* diag_row = cand_val + 2 * GMAX;
+  int* cand_idx = (int*)(diag_row + 2 * NBL);
+  unsigned* bar = (unsigned*)(cx.d_status + ST_BAR);
+
+  for (long k = 0; k < mn; k += NBL) {
+    const int b = (int)std::min<long>(NBL, mn - k);
+    const long M = m - k;
+    PanelGeom g = panel_geom(M, NBL);
+    PanelArgs pa;
+    pa.P = A.p + k + k * A.ld;
+    pa.ld = A.ld;
+    pa.M = (int)M;
+    pa.nb = b;
+    pa.R = g.R;
+    pa.lds = g.lds;
+    pa.G = g.G;
+    pa.gcol = (int)k;
+    pa.piv = d_piv + k;
+    pa.cand_row = cand_row;
+    pa.cand_val = cand_val;
+    pa.cand_idx = cand_idx;
+    pa.diag_row = diag_row;
+    pa.bar = bar;
+    pa.err = cx.d_status + ST_ERROR;
+    pa.info = cx.d_status + ST_INFO;
+    FB_CK(cudaMemsetAsync(bar, 0, sizeof(unsigned), st));
+    size_t smem = (size_t)g.lds * b * 8 + (size_t)b * 8;
+    void* args[] = {&pa};
+    const int ps = prof_begin(st);
+    FB_CK(cudaLaunchCooperativeKernel((void*)lu_panel_kernel, dim3(g.G), dim3(PANEL_THREADS), args,
+                                      smem, st));
+    prof_end(ps, st, PROF_PANEL, 0.0);
+    count_launch();
+    // interchanges to the left and right of the panel
+    const long nr = n - k - b;
+    if (laswp_dev(A.p, A.ld, (int)k, d_piv + k, b, 0, (int)k, (int)(k + b), (int)nr, false, st) !=
+        FLA_SUCCESS)
+      return FLA_FAILURE;
+    if (nr > 0) {
+      double* A11 = A.p + k + k * A.ld;
+      double* A12 = A.p + k + (k + b) * A.ld;
+      if (trsm_block(A11, A.ld, A12, A.ld, b, nr, true, false, true, st) != FLA_SUCCESS) return FLA_FAILURE;
+      const long m2 = m - k - b;
+      if (m2 > 0) {
+        double* A21 = A.p + (k + b) + k * A.ld;
+        double* A22 = A.p + (k + b) + (k + b) * A.ld;
+        if (gemm_f64(st, false, false, m2, nr, b, -1.0, A21, A.ld, A12, A.ld, 1.0, A22, A.ld) !=
+            FLA_SUCCESS)
+          return FLA_FAILURE;
+      }
+    }
+  }
+  return status_read(info);
+}
+
+}  // namespace fb

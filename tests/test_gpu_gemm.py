@@ -1,0 +1,59 @@
+"""The FP64 DMMA GEMM engine against a plain torch fp64 reference
+(C := alpha op(A) op(B) + beta C, the four transposition cases, the
+lower-triangle mode used by the Cholesky update, ragged sizes)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import seeded
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (128, 64, 16), (130, 70, 33), (300, 257, 128), (513, 190, 200)])
+def test_dgemm_matches_torch(cuda, flame, ta, tb, m, n, k):
+    torch = cuda
+    g = torch.Generator(device="cuda").manual_seed(m * 1000 + n * 10 + k + 7 * ta + 3 * tb)
+    A = torch.randn((k, m) if ta else (m, k), dtype=torch.float64, device="cuda", generator=g)
+    B = torch.randn((n, k) if tb else (k, n), dtype=torch.float64, device="cuda", generator=g)
+    Cm = torch.randn((m, n), dtype=torch.float64, device="cuda", generator=g)
+    # column-major copies with an even leading dimension
+    def cm(t):
+        r, c = t.shape
+        ld = r + (r & 1)
+        buf = torch.zeros((c, ld), dtype=torch.float64, device="cuda")
+        buf[:, :r] = t.t()
+        return buf, ld
+    Ab, lda = cm(A)
+    Bb, ldb = cm(B)
+    Cb, ldc = cm(Cm)
+    alpha, beta = -1.0, 1.0
+    rc = flame.lib().FLA_B200_dgemm(ta, tb, m, n, k, alpha, C.c_void_p(Ab.data_ptr()), lda,
+                                    C.c_void_p(Bb.data_ptr()), ldb, beta, C.c_void_p(Cb.data_ptr()), ldc, 0)
+    assert rc == flame.FLA_SUCCESS, flame.last_error()
+    opA = A.t() if ta else A
+    opB = B.t() if tb else B
+    ref = alpha * (opA @ opB) + beta * Cm
+    got = Cb[:, :m].t()
+    err = (got - ref).abs().max().item() / max(1.0, ref.abs().max().item())
+    assert err < 1e-13 * max(1, k) ** 0.5
+
+
+def test_dgemm_lower_mode_leaves_upper_untouched(cuda, flame):
+    torch = cuda
+    n, k = 300, 128
+    g = torch.Generator(device="cuda").manual_seed(5)
+    A = torch.randn((n, k), dtype=torch.float64, device="cuda", generator=g)
+    Cm = torch.randn((n, n), dtype=torch.float64, device="cuda", generator=g)
+    Ab = A.t().contiguous()  # column-major n x k storage, ld = n
+    Cb = Cm.t().contiguous()
+    rc = flame.lib().FLA_B200_dgemm(0, 1, n, n, k, -1.0, C.c_void_p(Ab.data_ptr()), n,
+                                    C.c_void_p(Ab.data_ptr()), n, 1.0, C.c_void_p(Cb.data_ptr()), n, 1)
+    assert rc == flame.FLA_SUCCESS
+    got = Cb.t()
+    ref = Cm - A @ A.t()
+    low = torch.tril(torch.ones(n, n, dtype=torch.bool, device="cuda"))
+    assert (got[low] - ref[low]).abs().max().item() < 1e-12
+    assert torch.equal(got[~low], Cm[~low])
