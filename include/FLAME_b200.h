@@ -42,6 +42,22 @@ int           FLA_B200_dgemm( int transa, int transb, long m, long n, long k, do
                               const double* A, long lda, const double* B, long ldb,
                               double beta, double* C, long ldc, int lower_only );
 
+/* No counterpart in the reference libflame.  LU factorization with partial
+ * pivoting of one m x n panel (n <= 128, m >= n) held in device memory (A,
+ * column-major, lda >= m; piv receives n relative zero-based pivots, as
+ * FLA_LU_piv), for callers that cannot let a library allocate device
+ * memory: the call makes no cudaMalloc/cudaFree, and keeps its scratch in a
+ * fixed ~334 KB array in device memory that the library carries.  Runs on
+ * `stream` (a cudaStream_t, or NULL for the default stream) and returns
+ * when the panel is done: FLA_SUCCESS, the zero-based index of the first
+ * zero pivot, or FLA_FAILURE with the reason in FLA_B200_last_error()
+ * (sizes beyond the limits are rejected).  The first call on a device
+ * looks up the array's device address, so make it before any stream
+ * capture.  All calls on a device share the array: calls that overlap on
+ * the GPU race and must be serialized by the caller. */
+int           FLA_B200_LU_piv_panel_noalloc( int m, int n, double* A, int lda, int* piv,
+                                             void* stream );
+
 #ifdef __cplusplus
 }
 #endif

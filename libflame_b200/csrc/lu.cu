@@ -21,6 +21,7 @@
 // winner, the owners of rows j and p(j) exchange them, and every CTA
 // scales its part of column j and applies the rank-1 update to its slab.
 #include <climits>
+#include <mutex>
 
 #include "common.h"
 #include "dev_util.cuh"
@@ -463,3 +464,167 @@ int lu_piv_dev(DMat A, int* d_piv, int* info) {
 }
 
 }  // namespace fb
+
+namespace fb {
+
+// ===========================================================================
+// Allocation-free LU panel factorization.
+//
+// Some callers cannot let a library call cudaMalloc: a caller whose own
+// memory manager has reserved the device memory up front (an allocator
+// that owns the HBM pool, a service with a fixed memory budget) sees a
+// stray cudaMalloc fail or break its accounting, and a latency-bound caller
+// cannot afford cudaMalloc/cudaFree, which may synchronize the device.
+// FLA_B200_LU_piv_panel_noalloc gives them the LU panel factorization (the
+// kernel above) with its scratch (pivot candidates, exchanged rows, the
+// grid-barrier counter and the status words) in a fixed array in device
+// memory that is part of the loaded library, so the call allocates nothing.
+//
+// Limits: panels of at most kNaMaxCols columns, m >= n, and a panel
+// geometry of at most kNaMaxCtas CTAs whose row slab fits in shared memory
+// (m up to about 29,000 rows on a 148-SM B200 for 128 columns).  The array
+// (about 334 KB) is held by every GPU that loads the library until the
+// process exits.  Every call on a device uses the same array and finds the
+// previous call's contents there; the barrier counter and status words are
+// cleared at the start of each call.  Calls whose work overlaps on the GPU
+// (concurrent streams, or several host threads) race on the array and must
+// be serialized by the caller.
+// ===========================================================================
+namespace {
+
+constexpr int kNaMaxCtas = 160;
+constexpr int kNaMaxCols = 128;
+
+struct NoAllocScratch {
+  double cand_row[2 * kNaMaxCtas * kNaMaxCols];
+  double cand_val[2 * kNaMaxCtas];
+  double diag_row[2 * kNaMaxCols];
+  int cand_idx[2 * kNaMaxCtas];
+  unsigned bar;
+  int status[2];  // [0] wait-timeout flag, [1] first null pivot (INT_MAX: none)
+};
+
+// The scratch itself: a file-scope device array of fixed size.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+// Device address of g_noalloc_scratch, looked up once per device.  In host
+// code the array's name is only a host-side stand-in, so the address must
+// come from cudaGetSymbolAddress with that device current.
+constexpr int kNaMaxDevices = 64;
+NoAllocScratch* g_na_ptr[kNaMaxDevices] = {};
+std::mutex g_na_mutex;
+
+__global__ void noalloc_reset_kernel(NoAllocScratch* s) {
+  s->bar = 0u;
+  s->status[0] = 0;
+  s->status[1] = INT_MAX;
+}
+
+}  // namespace
+
+}  // namespace fb
+
+// No counterpart in the reference libflame (see include/FLAME_b200.h).
+extern "C" int FLA_B200_LU_piv_panel_noalloc(int m, int n, double* A, int lda, int* piv,
+                                             void* stream) {
+  using namespace fb;
+  if (m < 0 || n < 0 || n > kNaMaxCols || m < n) {
+    set_last_error("FLA_B200_LU_piv_panel_noalloc: need 0 <= n <= 128 and m >= n (got m=" +
+                   std::to_string(m) + ", n=" + std::to_string(n) + ")");
+    return FLA_FAILURE;
+  }
+  if (lda < (m > 1 ? m : 1)) {
+    set_last_error("FLA_B200_LU_piv_panel_noalloc: lda < max(1, m)");
+    return FLA_FAILURE;
+  }
+  if (n == 0) return FLA_SUCCESS;
+  if (!A || !piv || !is_device_ptr(A) || !is_device_ptr(piv)) {
+    set_last_error("FLA_B200_LU_piv_panel_noalloc: A and piv must be device pointers");
+    return FLA_FAILURE;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNaMaxDevices) {
+    cudaGetLastError();
+    set_last_error("FLA_B200_LU_piv_panel_noalloc: no usable current device");
+    return FLA_FAILURE;
+  }
+  NoAllocScratch* s = nullptr;
+  {
+    // Set-up, once per device, with that device current.  The first call on
+    // a device does it, so that first call should come before any stream
+    // capture.
+    std::lock_guard<std::mutex> lk(g_na_mutex);
+    if (!g_na_ptr[dev]) {
+      void* p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || p == nullptr) {
+        cudaGetLastError();
+        set_last_error(std::string("FLA_B200_LU_piv_panel_noalloc: cudaGetSymbolAddress failed: ") +
+                       cudaGetErrorString(e));
+        return FLA_FAILURE;
+      }
+      cudaFuncSetAttribute(lu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(220 * 1024));
+      g_na_ptr[dev] = reinterpret_cast<NoAllocScratch*>(p);
+    }
+    s = g_na_ptr[dev];
+  }
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    set_last_error("FLA_B200_LU_piv_panel_noalloc: cannot query the SM count");
+    return FLA_FAILURE;
+  }
+  // Panel geometry: the same rule as the library's LU driver.
+  const long M = m;
+  const int R = (int)std::max<long>(std::min<long>(M, 32), (M + sms - 1) / sms);
+  const int G = (int)((M + R - 1) / R);
+  const int lds = R | 1;
+  const size_t smem = (size_t)lds * n * 8 + (size_t)n * 8;
+  if (G > kNaMaxCtas || smem > PANEL_SMEM_CAP) {
+    set_last_error("FLA_B200_LU_piv_panel_noalloc: panel of " + std::to_string(m) + " x " +
+                   std::to_string(n) + " exceeds the fixed scratch / shared-memory limits");
+    return FLA_FAILURE;
+  }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  noalloc_reset_kernel<<<1, 1, 0, st>>>(s);
+  count_launch();
+  PanelArgs pa;
+  pa.P = A;
+  pa.ld = lda;
+  pa.M = m;
+  pa.nb = n;
+  pa.R = R;
+  pa.lds = lds;
+  pa.G = G;
+  pa.gcol = 0;
+  pa.piv = piv;
+  pa.cand_row = s->cand_row;
+  pa.cand_val = s->cand_val;
+  pa.cand_idx = s->cand_idx;
+  pa.diag_row = s->diag_row;
+  pa.bar = &s->bar;
+  pa.err = &s->status[0];
+  pa.info = &s->status[1];
+  void* args[] = {&pa};
+  cudaError_t e = cudaLaunchCooperativeKernel((void*)lu_panel_kernel, dim3(G), dim3(PANEL_THREADS), args,
+                                              smem, st);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_last_error(std::string("FLA_B200_LU_piv_panel_noalloc: launch failed: ") + cudaGetErrorString(e));
+    return FLA_FAILURE;
+  }
+  count_launch();
+  int h[2] = {0, 0};
+  e = cudaMemcpyAsync(h, s->status, sizeof(h), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_last_error(std::string("FLA_B200_LU_piv_panel_noalloc: ") + cudaGetErrorString(e));
+    return FLA_FAILURE;
+  }
+  if (h[0] != 0) {
+    set_last_error("FLA_B200_LU_piv_panel_noalloc: a grid barrier exceeded its wait limit");
+    return FLA_FAILURE;
+  }
+  return h[1] == INT_MAX ? FLA_SUCCESS : h[1];
+}
