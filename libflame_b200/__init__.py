@@ -58,6 +58,11 @@ _SIGS = {
     "FLA_Apply_pivots": (C.c_int, [C.c_int, C.c_int, FLA_Obj, FLA_Obj]),
     "FLA_Shift_pivots_to": (C.c_int, [C.c_int, FLA_Obj]),
     "FLA_Chol_solve": (C.c_int, [C.c_int, FLA_Obj, FLA_Obj, FLA_Obj]),
+    "FLA_QR_UT": (C.c_int, [FLA_Obj, FLA_Obj]),
+    "FLA_QR_UT_create_T": (C.c_int, [FLA_Obj, C.POINTER(FLA_Obj)]),
+    "FLA_QR_UT_recover_tau": (C.c_int, [FLA_Obj, FLA_Obj]),
+    "FLA_Apply_Q_UT": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, FLA_Obj, FLA_Obj, FLA_Obj, FLA_Obj]),
+    "FLA_Apply_Q_UT_create_workspace": (C.c_int, [FLA_Obj, FLA_Obj, C.POINTER(FLA_Obj)]),
     "FLA_LU_piv_solve": (C.c_int, [FLA_Obj, FLA_Obj, FLA_Obj, FLA_Obj]),
     "FLA_B200_kernel_launches": (C.c_ulonglong, []),
     "FLA_B200_last_error": (C.c_char_p, []),
@@ -206,6 +211,24 @@ def chol_solve(A, B, X, uplo=FLA_LOWER_TRIANGULAR):
 def lu_piv_solve(A, p, B, X):
     va, vp, vb, vx = View(A), View(p), View(B), View(X)
     return lib().FLA_LU_piv_solve(va.obj, vp.obj, vb.obj, vx.obj)
+
+
+def qr_ut(A, T):
+    """FLA_QR_UT(A, T) in place; T is b_alg x n (b_alg = min(32, min(m, n)))."""
+    va, vt = View(A), View(T)
+    return lib().FLA_QR_UT(va.obj, vt.obj)
+
+
+def apply_q_ut(A, T, B, trans=FLA_CONJ_TRANSPOSE):
+    """FLA_Apply_Q_UT(LEFT, trans, FORWARD, COLUMNWISE, A, T, W, B): B := Q^T B
+    (trans = FLA_CONJ_TRANSPOSE / FLA_TRANSPOSE) or Q B (FLA_NO_TRANSPOSE)."""
+    va, vt, vb = View(A), View(T), View(B)
+    return lib().FLA_Apply_Q_UT(FLA_LEFT, trans, FLA_FORWARD, FLA_COLUMNWISE, va.obj, vt.obj, vt.obj, vb.obj)
+
+
+def qr_ut_recover_tau(T, t):
+    vt, vv = View(T), View(t)
+    return lib().FLA_QR_UT_recover_tau(vt.obj, vv.obj)
 
 
 def shift_pivots_to(ptype, p):

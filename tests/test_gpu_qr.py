@@ -1,0 +1,98 @@
+"""FLA_QR_UT / FLA_Apply_Q_UT / FLA_QR_UT_recover_tau / dgeqrf_ on the GPU
+against the CPU oracle and the reference's fixtures.
+
+Bar: R and the Householder vectors (the factored A) agree with the oracle
+within 1e-12 normwise; the defined entries of T (upper triangle of each
+b x b block) within 1e-12 normwise; ||A - QR||_F/(max(m,n) eps ||A||_F) at
+most the oracle's own + 1.0; Q^T B within 1e-12 normwise."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import rel_fro, seeded, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def t_mask(T, k):
+    b = T.shape[0]
+    mask = np.zeros(T.shape, dtype=bool)
+    for j in range(k):
+        mask[: (j % b) + 1, j] = True
+    return mask
+
+
+def run_qr(cuda, flame, A):
+    m, n = A.shape
+    b = min(32, m, n)
+    Ad = to_dev(cuda, A)
+    Td = to_dev(cuda, np.zeros((b, n)))
+    r = flame.qr_ut(Ad, Td)
+    assert r == flame.FLA_SUCCESS, flame.last_error()
+    return to_host(Ad), to_host(Td)
+
+
+@pytest.mark.parametrize("m,n", [(1, 1), (5, 3), (3, 5), (40, 40), (64, 64), (65, 64), (130, 100),
+                                 (100, 130), (300, 200), (513, 257), (1000, 640)])
+def test_qr_ut_matches_oracle(cuda, flame, oracle, m, n):
+    rng = seeded(m * 13 + n)
+    A = rng.standard_normal((m, n))
+    QR, T = run_qr(cuda, flame, A)
+    QRo, To = oracle.qr_ut(A)
+    assert rel_fro(QR, QRo) < TOL
+    mask = t_mask(To, min(m, n))
+    assert rel_fro(T[mask], To[mask]) < TOL
+    be, be_o = oracle.qr_backward_error(A, QR, T), oracle.qr_backward_error(A, QRo, To)
+    assert be <= be_o + 1.0, (be, be_o)
+
+
+def test_qr_golden(cuda, flame, golden):
+    for key in ["40x40", "130x64", "160x80"]:
+        A = golden["qr_%s_A" % key]
+        QR, T = run_qr(cuda, flame, A)
+        assert rel_fro(QR, golden["qr_%s_QR" % key]) < TOL
+        Tg = golden["qr_%s_T" % key]
+        mask = t_mask(Tg, min(A.shape))
+        assert rel_fro(T[mask], Tg[mask]) < TOL
+        Bd = to_dev(cuda, golden["qr_%s_B" % key])
+        assert flame.apply_q_ut(to_dev(cuda, golden["qr_%s_QR" % key]), to_dev(cuda, Tg), Bd) == flame.FLA_SUCCESS
+        assert rel_fro(to_host(Bd), golden["qr_%s_QtB" % key]) < TOL
+
+
+@pytest.mark.parametrize("m,n,nrhs", [(200, 120, 7), (600, 600, 64), (1030, 500, 3)])
+def test_apply_q_ut(cuda, flame, oracle, m, n, nrhs):
+    rng = seeded(m + n + nrhs)
+    A = rng.standard_normal((m, n))
+    QRo, To = oracle.qr_ut(A)
+    B = rng.standard_normal((m, nrhs))
+    ref = oracle.apply_qt(QRo, To, B)
+    Ad, Td, Bd = to_dev(cuda, QRo), to_dev(cuda, To), to_dev(cuda, B)
+    assert flame.apply_q_ut(Ad, Td, Bd) == flame.FLA_SUCCESS
+    assert rel_fro(to_host(Bd), ref) < TOL
+    # Q (Q^T B) = B
+    assert flame.apply_q_ut(Ad, Td, Bd, flame.FLA_NO_TRANSPOSE) == flame.FLA_SUCCESS
+    assert rel_fro(to_host(Bd), B) < 1e-13
+
+
+def test_recover_tau_and_dgeqrf(cuda, flame, golden, oracle):
+    A = golden["dgeqrf_A"]
+    m, n = A.shape
+    QRo, To = oracle.qr_ut(A)
+    Td = to_dev(cuda, To)
+    t = cuda.zeros(min(m, n), dtype=cuda.float64, device="cuda")
+    assert flame.qr_ut_recover_tau(Td, t) == flame.FLA_SUCCESS
+    exp = np.array([To[j % To.shape[0], j] for j in range(min(m, n))])
+    assert np.array_equal(t.cpu().numpy(), exp)
+    a = np.asfortranarray(A.copy())
+    tau = np.zeros(min(m, n))
+    work = np.zeros(n * 32)
+    info = C.c_int(9)
+    mm, nn, lw = C.c_int(m), C.c_int(n), C.c_int(n * 32)
+    flame.lib().dgeqrf_(C.byref(mm), C.byref(nn), a.ctypes.data_as(C.c_void_p), C.byref(mm),
+                        tau.ctypes.data_as(C.c_void_p), work.ctypes.data_as(C.c_void_p), C.byref(lw), C.byref(info))
+    assert info.value == 0
+    assert rel_fro(a, golden["dgeqrf_QR"]) < TOL
+    assert rel_fro(tau, golden["dgeqrf_tau"]) < TOL
