@@ -3,7 +3,7 @@
 // Right-looking blocked algorithm with the reference's structure
 // (src/lapack/dec/chol/l/flamec/FLA_Chol_l_blk_var3.c:13-66):
 //   for each 128-column block:  A11 := chol(A11)        [potrf_diag_kernel]
-//                               A21 := A21 inv(A11)^T   [trsm_rlt_kernel]
+//                               A21 := A21 inv(A11)^T   [trsm_tile_kernel, trsm.cu]
 //                               A22 -= A21 A21^T (lower) [DMMA GEMM engine]
 // The diagonal block is factored in shared memory in 32-column steps (the
 // reference's inner blocksize, FLA_Chol_cntl_init.c:23-61): a warp factors
@@ -111,69 +111,10 @@ __global__ void __launch_bounds__(POTRF_THREADS) potrf_diag_kernel(double* A, lo
   if (tid == 0 && s_fail >= 0) atomicMin(info, gcol + s_fail);
 }
 
-// X := X inv(L)^T for the m x b block X (ld ldx) and the b x b lower L
-// (ld ldl), b <= 128.  64 rows per CTA, 4 threads per row, each thread
-// holding every 4th column of its row in registers.
-constexpr int TRSM_ROWS = 64;
-constexpr int TRSM_THREADS = TRSM_ROWS * 4;
-__global__ void __launch_bounds__(TRSM_THREADS) trsm_rlt_kernel(const double* L, long ldl, double* X,
-                                                                long ldx, int m, int b,
-                                                                const int* info) {
-  extern __shared__ double SL[];  // L lower, column-major, ld NB
-  __shared__ double sdinv[NB];
-  if (guard_failed(info)) return;
-  const int tid = threadIdx.x;
-  for (int c = tid >> 5; c < b; c += TRSM_THREADS / 32)
-    for (int r = (tid & 31); r < b; r += 32) SL[r + c * NB] = (r >= c) ? L[r + (long)c * ldl] : 0.0;
-  __syncthreads();
-  for (int j = tid; j < b; j += TRSM_THREADS) sdinv[j] = 1.0 / SL[j + j * NB];
-  __syncthreads();
-  const int q = tid & 3;              // column phase of this thread
-  const int row = blockIdx.x * TRSM_ROWS + (tid >> 2);
-  const bool active = row < m;
-  double x[NB / 4];
-#pragma unroll
-  for (int i = 0; i < NB / 4; ++i) {
-    int c = q + 4 * i;
-    x[i] = (active && c < b) ? X[row + (long)c * ldx] : 0.0;
-  }
-  // right-looking substitution over the columns of the row (fully unrolled
-  // so that every register index is a compile-time constant)
-#pragma unroll
-  for (int j = 0; j < NB; ++j) {
-    if (j >= b) break;
-    const int owner = j & 3, slot = j >> 2;
-    double xj = 0.0;
-#pragma unroll
-    for (int i = 0; i < NB / 4; ++i)
-      if (i == slot) xj = x[i];
-    xj = __shfl_sync(0xffffffffu, xj, (threadIdx.x & 31 & ~3) | owner);
-    xj *= sdinv[j];
-    if (q == owner) {
-#pragma unroll
-      for (int i = 0; i < NB / 4; ++i)
-        if (i == slot) x[i] = xj;
-    }
-#pragma unroll
-    for (int i = 0; i < NB / 4; ++i) {
-      int c = q + 4 * i;
-      if (c > j) x[i] -= xj * SL[c + j * NB];
-    }
-  }
-  if (active) {
-#pragma unroll
-    for (int i = 0; i < NB / 4; ++i) {
-      int c = q + 4 * i;
-      if (c < b) X[row + (long)c * ldx] = x[i];
-    }
-  }
-}
-
 bool g_attr_done = false;
 void set_attrs() {
   if (g_attr_done) return;
   cudaFuncSetAttribute(potrf_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, POTRF_SMEM);
-  cudaFuncSetAttribute(trsm_rlt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, NB * NB * 8);
   g_attr_done = true;
 }
 
@@ -195,11 +136,7 @@ int chol_lower_enqueue(DMat A, cudaStream_t st) {
     if (m2 <= 0) break;
     double* A21 = A.p + (k + b) + k * A.ld;
     double* A22 = A.p + (k + b) + (k + b) * A.ld;
-    ps = prof_begin(st);
-    trsm_rlt_kernel<<<(unsigned)((m2 + TRSM_ROWS - 1) / TRSM_ROWS), TRSM_THREADS, NB * NB * 8, st>>>(
-        A11, A.ld, A21, A.ld, (int)m2, b, info);
-    prof_end(ps, st, PROF_TRSM, (double)m2 * b * b);
-    count_launch();
+    if (trsm_right_lt_block(A11, A.ld, A21, A.ld, m2, b, info, st) != FLA_SUCCESS) return FLA_FAILURE;
     int r = gemm_f64(st, false, true, m2, m2, b, -1.0, A21, A.ld, A21, A.ld, 1.0, A22, A.ld,
                      GEMM_LOWER, 0, info);
     if (r != FLA_SUCCESS) return r;

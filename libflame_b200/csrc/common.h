@@ -189,5 +189,8 @@ int laswp_dev(double* A, long ld, int row0, const int* d_piv, int npiv, int c0, 
 int trsm_left_dev(DMat T, DMat B, bool lower, bool trans, bool unit, cudaStream_t st);
 int trsm_block(const double* T, long ldt, double* B, long ldb, int b, long n, bool lower,
                bool trans, bool unit, cudaStream_t st);
+// X := X inv(L)^T for an m x b block (b <= 128); no-op once *guard != INT_MAX.
+int trsm_right_lt_block(const double* L, long ldl, double* X, long ldx, long m, int b, const int* guard,
+                        cudaStream_t st);
 
 }  // namespace fb

@@ -76,6 +76,17 @@ __global__ void __launch_bounds__(THREADS, 2)
     long max_i = (long)tile_m + BM - 1, min_j = tile_n;
     if (max_i - min_j < diag_off) return;
   }
+  if (beta != 0.0) {
+    // Bring this tile of C from HBM into L2 while the k-loop runs, so the
+    // epilogue reads hit L2: 64 columns x 8 lines of 128 B (128 rows).
+    const int t = threadIdx.x;
+    for (int l = t; l < BN * (BM / 16); l += THREADS) {
+      const int col = l / (BM / 16), seg = l % (BM / 16);
+      const int r = tile_m + seg * 16, cc = tile_n + col;
+      if (r < M && cc < N)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(C + (long)r + (long)cc * ldc));
+    }
+  }
   uintptr_t base = (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023);
   unsigned char* sm = reinterpret_cast<unsigned char*>(base);
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + STAGES * STAGE_BYTES);
@@ -171,7 +182,9 @@ __global__ void __launch_bounds__(THREADS, 2)
     __syncwarp();
     if (lane == 0) mbar_arrive(empty0 + 8 * s);
   }
-  if (!ok) {
+  // Every thread reaches this barrier, also after a wait that ran out (each
+  // wait is bounded), so a failure cannot leave part of the CTA blocked.
+  if (!__syncthreads_and(ok ? 1 : 0)) {
     // drain: thread 0 waits (bounded) for the copies still in flight
     if (threadIdx.x == 0)
       for (int kt = (issued > STAGES ? issued - STAGES : 0); kt < issued; ++kt)
@@ -180,32 +193,49 @@ __global__ void __launch_bounds__(THREADS, 2)
   }
 
   // ---------------- epilogue ----------------
-  // acc[i][j][e] = C(row ra[i] of lane-group g, col rb[j] of lane-group 2t+e)
-  // The column for lane-group h of B fragment j:
-  int cb[4][2];
+  // acc[i][j][e] is C(ra[i] of lane group g, column of lane group h = 2t+e
+  // of B fragment j).  The accumulators go through shared memory (the stage
+  // buffers are free once every warp is past the k-loop) so that C is read
+  // and written in coalesced 16-byte pieces along its columns.
+  double* sC = reinterpret_cast<double*>(sm);  // BM x BN, ld LDC
+  constexpr int LDC = BM + 2;
 #pragma unroll
   for (int j = 0; j < 4; ++j)
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
-      int h = 2 * t + e;
-      cb[j][e] = B_K ? (wn * 32 + 8 * j + perm8_tab(h)) : (wn * 32 + 16 * (j >> 1) + perm16_tab(j & 1, h));
+      const int h = 2 * t + e;
+      const int col = B_K ? (wn * 32 + 8 * j + perm8_tab(h)) : (wn * 32 + 16 * (j >> 1) + perm16_tab(j & 1, h));
+#pragma unroll
+      for (int i = 0; i < 4; ++i) sC[ra[i] + col * LDC] = acc[i][j][e];
     }
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    int row = tile_m + ra[i];
-    if (row >= M) continue;
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        int col = tile_n + cb[j][e];
-        if (col >= N) continue;
-        if (mode == GEMM_LOWER && (long)row - (long)col < diag_off) continue;
-        double* cp = C + (long)row + (long)col * ldc;
-        double v = alpha * acc[i][j][e];
-        if (beta != 0.0) v = fma(beta, *cp, v);
-        *cp = v;
+  __syncthreads();
+  const bool vec = ((reinterpret_cast<uintptr_t>(C) & 15u) == 0) && ((ldc & 1) == 0);
+  // thread -> (row pair, column): 64 row pairs x 4 columns per pass
+  const int rp = threadIdx.x & 63, c0 = threadIdx.x >> 6;
+  const int row = tile_m + 2 * rp;
+#pragma unroll 4
+  for (int cl = c0; cl < BN; cl += THREADS / 64) {
+    const int col = tile_n + cl;
+    if (col >= N || row >= M) continue;
+    double* cp = C + (long)row + (long)col * ldc;
+    const double a0 = alpha * sC[2 * rp + cl * LDC], a1 = alpha * sC[2 * rp + 1 + cl * LDC];
+    const bool ok0 = mode != GEMM_LOWER || (long)row - (long)col >= diag_off;
+    const bool ok1 = (row + 1 < M) && (mode != GEMM_LOWER || (long)row + 1 - (long)col >= diag_off);
+    if (vec && ok0 && ok1) {
+      double2 v;
+      if (beta != 0.0) {
+        const double2 c = *reinterpret_cast<const double2*>(cp);
+        v.x = fma(beta, c.x, a0);
+        v.y = fma(beta, c.y, a1);
+      } else {
+        v.x = a0;
+        v.y = a1;
       }
+      *reinterpret_cast<double2*>(cp) = v;
+    } else {
+      if (ok0) cp[0] = (beta != 0.0) ? fma(beta, cp[0], a0) : a0;
+      if (ok1) cp[1] = (beta != 0.0) ? fma(beta, cp[1], a1) : a1;
+    }
   }
 }
 

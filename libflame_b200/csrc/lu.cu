@@ -6,7 +6,7 @@
 //   for each block of nb columns:
 //     [A11;A21], p1 := LU_piv([A11;A21])   lu_panel_kernel (cooperative)
 //     pivot [A10;A20] and [A12;A22]         laswp_kernel
-//     A12 := inv(tril_unit(A11)) A12         trsm_llu_kernel
+//     A12 := inv(tril_unit(A11)) A12         trsm_tile_kernel (trsm.cu)
 //     A22 -= A21 A12                         DMMA GEMM engine
 // Pivot choice is the reference's: the entry of largest magnitude in the
 // current column, the first (smallest row) among equals (idamax,
@@ -167,6 +167,79 @@ __global__ void __launch_bounds__(PANEL_THREADS) lu_panel_kernel(PanelArgs a) {
 // Row interchanges on a set of columns: for each column, rows row0+i and
 // row0+i+piv[i] are swapped for i = 0..npiv-1 in order (or in reverse when
 // `reverse`, which applies P^T).  Columns: [c0, c0+n0) and [c1, c1+n1).
+//
+// laswp_block_kernel (npiv <= LASWP_MAXP): the interchanges touch at most
+// 2*npiv rows ("slots": rows row0..row0+npiv-1, then each distinct target
+// below them).  Each CTA composes the whole sequence of interchanges into one
+// permutation of the slots (a serial pass over an int array in SMEM), then
+// moves its columns' values with independent, coalesced loads and stores.
+constexpr int LASWP_MAXP = 128;
+constexpr int LASWP_NC = 16;  // columns per CTA (static SMEM < 48 KB)
+__global__ void __launch_bounds__(256) laswp_block_kernel(double* A, long ld, int row0,
+                                                          const int* __restrict__ piv, int npiv, int c0,
+                                                          int n0, int c1, int n1, int reverse) {
+  __shared__ int s_tgt[LASWP_MAXP];          // slot of the target of interchange i
+  __shared__ int s_row[2 * LASWP_MAXP];      // row offset (from row0) of each slot, -1 unused
+  __shared__ int s_src[2 * LASWP_MAXP];      // final content of slot s = original slot s_src[s]
+  __shared__ double s_val[LASWP_NC][2 * LASWP_MAXP + 1];
+  const int tid = threadIdx.x;
+  const int nslot = 2 * npiv;
+  for (int s = tid; s < nslot; s += blockDim.x) s_row[s] = (s < npiv) ? s : -1;
+  __syncthreads();
+  if (tid < npiv) {
+    const int t = tid + piv[tid];  // target row offset
+    int slot;
+    if (t < npiv) {
+      slot = t;
+    } else {
+      int first = tid;  // first interchange with the same far target owns the slot
+      for (int i2 = 0; i2 < tid; ++i2)
+        if (i2 + piv[i2] == t) { first = i2; break; }
+      slot = npiv + first;
+      if (first == tid) s_row[slot] = t;
+    }
+    s_tgt[tid] = slot;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int s = 0; s < nslot; ++s) s_src[s] = s;
+    if (!reverse) {
+      for (int i = 0; i < npiv; ++i) {
+        const int a = i, b = s_tgt[i];
+        const int x = s_src[a];
+        s_src[a] = s_src[b];
+        s_src[b] = x;
+      }
+    } else {
+      for (int i = npiv - 1; i >= 0; --i) {
+        const int a = i, b = s_tgt[i];
+        const int x = s_src[a];
+        s_src[a] = s_src[b];
+        s_src[b] = x;
+      }
+    }
+  }
+  __syncthreads();
+  const int ncols = n0 + n1;
+  const int cbase = blockIdx.x * LASWP_NC;
+  // load: consecutive threads take consecutive slots of one column
+  for (int e = tid; e < LASWP_NC * nslot; e += blockDim.x) {
+    const int cl = e / nslot, s = e % nslot;
+    const int t = cbase + cl;
+    if (t >= ncols || s_row[s] < 0) continue;
+    const int col = t < n0 ? c0 + t : c1 + (t - n0);
+    s_val[cl][s] = A[(long)row0 + s_row[s] + (long)col * ld];
+  }
+  __syncthreads();
+  for (int e = tid; e < LASWP_NC * nslot; e += blockDim.x) {
+    const int cl = e / nslot, s = e % nslot;
+    const int t = cbase + cl;
+    if (t >= ncols || s_row[s] < 0 || s_src[s] == s) continue;
+    const int col = t < n0 ? c0 + t : c1 + (t - n0);
+    A[(long)row0 + s_row[s] + (long)col * ld] = s_val[cl][s_src[s]];
+  }
+}
+
 __global__ void laswp_kernel(double* A, long ld, int row0, const int* __restrict__ piv, int npiv,
                              int c0, int n0, int c1, int n1, int reverse) {
   extern __shared__ int sp[];
@@ -199,76 +272,10 @@ __global__ void laswp_kernel(double* A, long ld, int row0, const int* __restrict
   }
 }
 
-// X := inv(op(T)) X for the b x n block X (ld ldx), T b x b triangular
-// (lower if LOWER, else upper; op = transpose if TRANS; unit diagonal if
-// UNIT), b <= 128.  The substitution runs forward when op(T) is lower and
-// backward when it is upper.  64 columns per CTA, 4 threads per column, each
-// holding every 4th row of its column in registers.
-constexpr int TRSM_COLS = 64;
-constexpr int TRSM_THREADS = TRSM_COLS * 4;
-template <bool LOWER, bool TRANS, bool UNIT>
-__global__ void __launch_bounds__(TRSM_THREADS) trsm_left_kernel(const double* T, long ldt, double* X,
-                                                                 long ldx, int b, int n) {
-  extern __shared__ double ST[];  // ld NBMAX, the stored triangle
-  __shared__ double sdinv[NBMAX];
-  constexpr bool FWD = (LOWER != TRANS);
-  const int tid = threadIdx.x;
-  for (int cc = tid >> 5; cc < b; cc += TRSM_THREADS / 32)
-    for (int r = (tid & 31); r < b; r += 32)
-      ST[r + cc * NBMAX] = (LOWER ? (r >= cc) : (r <= cc)) ? T[r + (long)cc * ldt] : 0.0;
-  __syncthreads();
-  if (!UNIT)
-    for (int j = tid; j < b; j += TRSM_THREADS) sdinv[j] = 1.0 / ST[j + j * NBMAX];
-  __syncthreads();
-  const int q = tid & 3;
-  const int col = blockIdx.x * TRSM_COLS + (tid >> 2);
-  const bool active = col < n;
-  double x[NBMAX / 4];
-#pragma unroll
-  for (int i = 0; i < NBMAX / 4; ++i) {
-    const int r = q + 4 * i;
-    x[i] = (active && r < b) ? X[r + (long)col * ldx] : 0.0;
-  }
-  // every register index below is a compile-time constant: the forward
-  // sweep visits j = 0..b-1, the backward sweep j = NBMAX-1..0 skipping the
-  // padding rows j >= b
-#pragma unroll
-  for (int jj = 0; jj < NBMAX; ++jj) {
-    const int j = FWD ? jj : (NBMAX - 1 - jj);
-    if (j < b) {
-      double xj = x[j >> 2];
-      xj = __shfl_sync(0xffffffffu, xj, (threadIdx.x & 31 & ~3) | (j & 3));
-      if (!UNIT) {
-        xj *= sdinv[j];
-        if (q == (j & 3)) x[j >> 2] = xj;
-      }
-#pragma unroll
-      for (int i = 0; i < NBMAX / 4; ++i) {
-        const int r = q + 4 * i;
-        const bool upd = FWD ? (r > j && r < b) : (r < j);
-        if (upd) x[i] -= (TRANS ? ST[j + r * NBMAX] : ST[r + j * NBMAX]) * xj;
-      }
-    }
-  }
-  if (active) {
-#pragma unroll
-    for (int i = 0; i < NBMAX / 4; ++i) {
-      const int r = q + 4 * i;
-      if (r < b) X[r + (long)col * ldx] = x[i];
-    }
-  }
-}
-
 bool g_attrs = false;
 void set_attrs() {
   if (g_attrs) return;
   cudaFuncSetAttribute(lu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(220 * 1024));
-#define FB_TRSM_ATTR(L, T, U) \
-  cudaFuncSetAttribute(trsm_left_kernel<L, T, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, NBMAX * NBMAX * 8);
-  FB_TRSM_ATTR(true, false, true) FB_TRSM_ATTR(true, false, false) FB_TRSM_ATTR(true, true, true)
-  FB_TRSM_ATTR(true, true, false) FB_TRSM_ATTR(false, false, true) FB_TRSM_ATTR(false, false, false)
-  FB_TRSM_ATTR(false, true, true) FB_TRSM_ATTR(false, true, false)
-#undef FB_TRSM_ATTR
   g_attrs = true;
 }
 
@@ -297,10 +304,15 @@ int laswp_dev(double* A, long ld, int row0, const int* d_piv, int npiv, int c0, 
               int n1, bool reverse, cudaStream_t st) {
   const int ncols = n0 + n1;
   if (ncols <= 0 || npiv <= 0) return FLA_SUCCESS;
-  const int threads = 128;
   const int ps = prof_begin(st);
-  laswp_kernel<<<(ncols + threads - 1) / threads, threads, npiv * sizeof(int), st>>>(
-      A, ld, row0, d_piv, npiv, c0, n0, c1, n1, reverse ? 1 : 0);
+  if (npiv <= LASWP_MAXP) {
+    laswp_block_kernel<<<(ncols + LASWP_NC - 1) / LASWP_NC, 256, 0, st>>>(A, ld, row0, d_piv, npiv, c0, n0,
+                                                                          c1, n1, reverse ? 1 : 0);
+  } else {
+    const int threads = 128;
+    laswp_kernel<<<(ncols + threads - 1) / threads, threads, npiv * sizeof(int), st>>>(
+        A, ld, row0, d_piv, npiv, c0, n0, c1, n1, reverse ? 1 : 0);
+  }
   prof_end(ps, st, PROF_SWAP, 0.0);
   count_launch();
   FB_CK(cudaGetLastError());
@@ -327,30 +339,6 @@ int apply_pivots_dev(DMat A, const int* d_piv, int k1, int k2, bool reverse, cud
         return FLA_FAILURE;
     }
   }
-  return FLA_SUCCESS;
-}
-
-// B := inv(op(T)) B for a b x n block B, T b x b (b <= 128) triangular.
-int trsm_block(const double* T, long ldt, double* B, long ldb, int b, long n, bool lower,
-               bool trans, bool unit, cudaStream_t st) {
-  set_attrs();
-  if (n <= 0 || b <= 0) return FLA_SUCCESS;
-  unsigned grid = (unsigned)((n + TRSM_COLS - 1) / TRSM_COLS);
-  const size_t sm = NBMAX * NBMAX * 8;
-  const int ps = prof_begin(st);
-#define FB_TRSM_LAUNCH(L, T_, U) \
-  trsm_left_kernel<L, T_, U><<<grid, TRSM_THREADS, sm, st>>>(T, ldt, B, ldb, b, (int)n)
-  if (lower) {
-    if (!trans) { if (unit) FB_TRSM_LAUNCH(true, false, true); else FB_TRSM_LAUNCH(true, false, false); }
-    else        { if (unit) FB_TRSM_LAUNCH(true, true, true);  else FB_TRSM_LAUNCH(true, true, false); }
-  } else {
-    if (!trans) { if (unit) FB_TRSM_LAUNCH(false, false, true); else FB_TRSM_LAUNCH(false, false, false); }
-    else        { if (unit) FB_TRSM_LAUNCH(false, true, true);  else FB_TRSM_LAUNCH(false, true, false); }
-  }
-#undef FB_TRSM_LAUNCH
-  prof_end(ps, st, PROF_TRSM, (double)b * (double)b * (double)n);
-  count_launch();
-  FB_CK(cudaGetLastError());
   return FLA_SUCCESS;
 }
 

@@ -1,0 +1,164 @@
+// Triangular solves with one diagonal block (b <= 128) on the GPU.
+//
+//   left:  X := inv(op(T)) X   for a b x n block X      (LU: A12 := inv(L11) A12,
+//                                                      solves, QR: W := T^-T W)
+//   right: X := X inv(L)^T     for an m x b block X      (Chol: A21 := A21 inv(L11)^T)
+//
+// Replaces the dtrsm_ calls of the reference's blocked algorithms
+// (FLA_Trsm_external, src/base/flamec/wrappers/blas/3/external/
+// FLA_Trsm_external.c:72).  Substitution order follows dtrsm: forward when
+// op(T) is lower, backward when upper; non-unit diagonals are applied as a
+// multiplication by the reciprocal of the pivot (as dtrsm's R,L,T,N case,
+// src/flablas/f2c/dtrsm.c).
+//
+// One CTA owns 64 right-hand sides (columns of X for left, rows for right),
+// kept in shared memory with the triangle, and sweeps the b steps: scale the
+// current unknown (one thread per right-hand side), then update the
+// remaining unknowns (all threads).  The step loop is not unrolled, so the
+// kernel stays small in the instruction cache.
+#include "common.h"
+
+namespace fb {
+
+namespace {
+
+constexpr int TB = 128;             // max triangle order
+constexpr int NV = 64;              // right-hand sides per CTA
+constexpr int THREADS = 256;
+constexpr int LDT = TB + 1;         // SMEM stride of the triangle
+constexpr int LDX = TB + 1;         // SMEM stride of one right-hand side
+constexpr size_t SMEM = (size_t)(TB * LDT + NV * LDX + NV + TB) * sizeof(double);
+
+// coef(r, j): entry of op(T) at (r, j), from the stored triangle S
+template <bool TRANS>
+__device__ __forceinline__ double coef(const double* S, int r, int j) {
+  return TRANS ? S[j + r * LDT] : S[r + j * LDT];
+}
+
+template <bool LOWER, bool TRANS, bool UNIT, bool RIGHT>
+__global__ void __launch_bounds__(THREADS) trsm_tile_kernel(const double* __restrict__ T, long ldt,
+                                                            double* __restrict__ X, long ldx, int b,
+                                                            int nvec, const int* guard) {
+  extern __shared__ double sm[];
+  double* ST = sm;                    // b x b triangle (stored part only)
+  double* SX = ST + TB * LDT;         // NV right-hand sides, SX[r + v*LDX]
+  double* sx = SX + NV * LDX;         // scaled current unknown per rhs
+  double* sd = sx + NV;               // reciprocal diagonal
+  if (guard && *((volatile const int*)guard) != 0x7fffffff) return;
+  constexpr bool FWD = (LOWER != TRANS);
+  const int tid = threadIdx.x;
+  const int v0 = blockIdx.x * NV;
+  const int nv = min(NV, nvec - v0);
+  for (int c = tid >> 5; c < b; c += THREADS / 32)
+    for (int r = tid & 31; r < b; r += 32)
+      ST[r + c * LDT] = (LOWER ? (r >= c) : (r <= c)) ? T[r + (long)c * ldt] : 0.0;
+  // right-hand side v, unknown r: left -> X(r, v0+v); right -> X(v0+v, r)
+  if (!RIGHT) {
+    for (int v = tid >> 5; v < nv; v += THREADS / 32)
+      for (int r = tid & 31; r < b; r += 32) SX[r + v * LDX] = X[r + (long)(v0 + v) * ldx];
+  } else {
+    for (int r = tid >> 6; r < b; r += THREADS / 64)
+      for (int v = tid & 63; v < nv; v += 64) SX[r + v * LDX] = X[(long)(v0 + v) + (long)r * ldx];
+  }
+  __syncthreads();
+  if (!UNIT)
+    for (int j = tid; j < b; j += THREADS) sd[j] = 1.0 / ST[j + j * LDT];
+  __syncthreads();
+  for (int jj = 0; jj < b; ++jj) {
+    const int j = FWD ? jj : (b - 1 - jj);
+    if (tid < nv) {
+      double x = SX[j + tid * LDX];
+      if (!UNIT) {
+        x *= sd[j];
+        SX[j + tid * LDX] = x;
+      }
+      sx[tid] = x;
+    }
+    __syncthreads();
+    // remaining unknowns: FWD r in (j, b), BWD r in [0, j)
+    const int r_lo = FWD ? j + 1 : 0;
+    const int cnt = (FWD ? (b - j - 1) : j) * nv;
+    if (nv == NV) {
+      for (int e = tid; e < cnt; e += THREADS) {
+        const int r = r_lo + (e >> 6), v = e & (NV - 1);
+        SX[r + v * LDX] -= coef<TRANS>(ST, r, j) * sx[v];
+      }
+    } else {
+      for (int e = tid; e < cnt; e += THREADS) {
+        const int r = r_lo + e / nv, v = e % nv;
+        SX[r + v * LDX] -= coef<TRANS>(ST, r, j) * sx[v];
+      }
+    }
+    __syncthreads();
+  }
+  if (!RIGHT) {
+    for (int v = tid >> 5; v < nv; v += THREADS / 32)
+      for (int r = tid & 31; r < b; r += 32) X[r + (long)(v0 + v) * ldx] = SX[r + v * LDX];
+  } else {
+    for (int r = tid >> 6; r < b; r += THREADS / 64)
+      for (int v = tid & 63; v < nv; v += 64) X[(long)(v0 + v) + (long)r * ldx] = SX[r + v * LDX];
+  }
+}
+
+template <bool L, bool T, bool U, bool R>
+void set_attr_one() {
+  cudaFuncSetAttribute(trsm_tile_kernel<L, T, U, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+}
+
+bool g_attr = false;
+void set_attrs() {
+  if (g_attr) return;
+  set_attr_one<true, false, true, false>();
+  set_attr_one<true, false, false, false>();
+  set_attr_one<true, true, true, false>();
+  set_attr_one<true, true, false, false>();
+  set_attr_one<false, false, true, false>();
+  set_attr_one<false, false, false, false>();
+  set_attr_one<false, true, true, false>();
+  set_attr_one<false, true, false, false>();
+  set_attr_one<true, false, false, true>();
+  g_attr = true;
+}
+
+}  // namespace
+
+// B := inv(op(T)) B for a b x n block B, T b x b (b <= 128) triangular.
+int trsm_block(const double* T, long ldt, double* B, long ldb, int b, long n, bool lower, bool trans,
+               bool unit, cudaStream_t st) {
+  set_attrs();
+  if (n <= 0 || b <= 0) return FLA_SUCCESS;
+  const unsigned grid = (unsigned)((n + NV - 1) / NV);
+  const int ps = prof_begin(st);
+#define FB_TRSM_LAUNCH(L, T_, U) \
+  trsm_tile_kernel<L, T_, U, false><<<grid, THREADS, SMEM, st>>>(T, ldt, B, ldb, b, (int)n, nullptr)
+  if (lower) {
+    if (!trans) { if (unit) FB_TRSM_LAUNCH(true, false, true); else FB_TRSM_LAUNCH(true, false, false); }
+    else        { if (unit) FB_TRSM_LAUNCH(true, true, true);  else FB_TRSM_LAUNCH(true, true, false); }
+  } else {
+    if (!trans) { if (unit) FB_TRSM_LAUNCH(false, false, true); else FB_TRSM_LAUNCH(false, false, false); }
+    else        { if (unit) FB_TRSM_LAUNCH(false, true, true);  else FB_TRSM_LAUNCH(false, true, false); }
+  }
+#undef FB_TRSM_LAUNCH
+  prof_end(ps, st, PROF_TRSM, (double)b * (double)b * (double)n);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
+}
+
+// X := X inv(L)^T for an m x b block X, L b x b lower non-unit (b <= 128);
+// the kernel returns at once when *guard no longer holds INT_MAX.
+int trsm_right_lt_block(const double* L, long ldl, double* X, long ldx, long m, int b, const int* guard,
+                        cudaStream_t st) {
+  set_attrs();
+  if (m <= 0 || b <= 0) return FLA_SUCCESS;
+  const unsigned grid = (unsigned)((m + NV - 1) / NV);
+  const int ps = prof_begin(st);
+  // X L^T = B  <=>  L X^T = B^T: a forward solve with L per row of X
+  trsm_tile_kernel<true, false, false, true><<<grid, THREADS, SMEM, st>>>(L, ldl, X, ldx, b, (int)m, guard);
+  prof_end(ps, st, PROF_TRSM, (double)m * (double)b * (double)b);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
+}
+
+}  // namespace fb
