@@ -3,8 +3,10 @@
 // Right-looking blocked algorithm with the reference's structure
 // (src/lapack/dec/chol/l/flamec/FLA_Chol_l_blk_var3.c:13-66):
 //   for each 128-column block:  A11 := chol(A11)        [potrf_diag_kernel]
-//                               A21 := A21 inv(A11)^T   [trsm_tile_kernel, trsm.cu]
+//                               A21 := A21 inv(A11)^T   [DMMA GEMM with inv(L11)]
 //                               A22 -= A21 A21^T (lower) [DMMA GEMM engine]
+// with the next block column factored on a second stream while the rest of
+// the trailing update runs (chol_lower_enqueue).
 // The diagonal block is factored in shared memory in 32-column steps (the
 // reference's inner blocksize, FLA_Chol_cntl_init.c:23-61): a warp factors
 // each 32x32 block (the unblocked var2/var3 leaf), the rows below are solved
@@ -120,26 +122,69 @@ void set_attrs() {
 
 }  // namespace
 
-// Enqueue the blocked factorization of the lower triangle of A on `st`.
+// Enqueue the blocked factorization of the lower triangle of A on `st`, with
+// a lookahead of one panel when `st` is the library's main stream:
+//   panel k (side stream):  A11 := chol(A11); inv(L11) formed next to it;
+//                           A21 := A21 inv(L11)^T as a DMMA GEMM
+//   main stream, step k:    A22(:, next panel) -= A21 A21(next rows)^T,
+//                           then the next panel goes to the side stream,
+//                           A22(rest) -= A21 A21^T (lower) concurrently.
+// Failure semantics follow FLA_Chol_l_blk_var3: the updates of step k run
+// unless a column before k + b has failed (the guard limit of each launch),
+// so a failure in the next panel does not cut short step k's update.
 int chol_lower_enqueue(DMat A, cudaStream_t st) {
   set_attrs();
-  const long n = A.m;
-  int* info = ctx().d_status + ST_INFO;
+  Context& cx = ctx();
+  const long n = A.m, ld = A.ld;
+  if (n <= 0) return FLA_SUCCESS;
+  int* info = cx.d_status + ST_INFO;
+  const bool lookahead = (st == cx.stream);
+  cudaStream_t sd = lookahead ? cx.side : st;
+  double* Linv = (double*)ws_get(WS_MISC, sizeof(double) * NB * NB);
+  double* W = (double*)ws_get(WS_MISC2, sizeof(double) * NB * (size_t)(std::max<long>(0, n - NB) + 2));
+  if (!Linv || !W) return FLA_FAILURE;
+  cudaEvent_t ev_look = cx.ev[2], ev_panel = cx.ev[3];
+  auto at = [&](long i, long j) { return A.p + i + j * ld; };
+
+  // Panel k: diagonal block, its inverse, and the block column below it.
+  auto panel = [&](long k, cudaStream_t s) -> int {
+    const int b = (int)std::min<long>(NB, n - k);
+    int ps = prof_begin(s);
+    potrf_diag_kernel<<<1, POTRF_THREADS, POTRF_SMEM, s>>>(at(k, k), ld, b, (int)k, info);
+    prof_end(ps, s, PROF_DIAG, (double)b * b * b / 3.0);
+    count_launch();
+    FB_CK(cudaGetLastError());
+    const long m2 = n - k - b;
+    if (m2 <= 0) return FLA_SUCCESS;
+    const long ldl = (b + 1) & ~1L;  // TMA: 16-byte leading dimensions
+    if (tri_inverse_lower(at(k, k), ld, b, false, Linv, ldl, s) != FLA_SUCCESS) return FLA_FAILURE;
+    const long ldw = (m2 + 1) & ~1L;
+    FB_CK(cudaMemcpy2DAsync(W, sizeof(double) * ldw, at(k + b, k), sizeof(double) * ld, sizeof(double) * m2, b,
+                            cudaMemcpyDeviceToDevice, s));
+    return gemm_f64(s, false, true, m2, b, b, 1.0, W, ldw, Linv, ldl, 0.0, at(k + b, k), ld, GEMM_FULL, 0, info,
+                    (int)(k + b));
+  };
+
+  if (panel(0, st) != FLA_SUCCESS) return FLA_FAILURE;
   for (long k = 0; k < n; k += NB) {
     const int b = (int)std::min<long>(NB, n - k);
-    double* A11 = A.p + k + k * A.ld;
-    int ps = prof_begin(st);
-    potrf_diag_kernel<<<1, POTRF_THREADS, POTRF_SMEM, st>>>(A11, A.ld, b, (int)k, info);
-    prof_end(ps, st, PROF_DIAG, (double)b * b * b / 3.0);
-    count_launch();
     const long m2 = n - k - b;
     if (m2 <= 0) break;
-    double* A21 = A.p + (k + b) + k * A.ld;
-    double* A22 = A.p + (k + b) + (k + b) * A.ld;
-    if (trsm_right_lt_block(A11, A.ld, A21, A.ld, m2, b, info, st) != FLA_SUCCESS) return FLA_FAILURE;
-    int r = gemm_f64(st, false, true, m2, m2, b, -1.0, A21, A.ld, A21, A.ld, 1.0, A22, A.ld,
-                     GEMM_LOWER, 0, info);
-    if (r != FLA_SUCCESS) return r;
+    const int lim = (int)(k + b);
+    const int nb2 = (int)std::min<long>(NB, m2);
+    // the next panel's columns first
+    if (gemm_f64(st, false, true, m2, nb2, b, -1.0, at(k + b, k), ld, at(k + b, k), ld, 1.0, at(k + b, k + b), ld,
+                 GEMM_LOWER, 0, info, lim) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    FB_CK(cudaEventRecord(ev_look, st));
+    FB_CK(cudaStreamWaitEvent(sd, ev_look, 0));
+    if (panel(k + b, sd) != FLA_SUCCESS) return FLA_FAILURE;
+    FB_CK(cudaEventRecord(ev_panel, sd));
+    if (m2 > nb2 &&
+        gemm_f64(st, false, true, m2 - nb2, m2 - nb2, b, -1.0, at(k + b + nb2, k), ld, at(k + b + nb2, k), ld, 1.0,
+                 at(k + b + nb2, k + b + nb2), ld, GEMM_LOWER, 0, info, lim) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    FB_CK(cudaStreamWaitEvent(st, ev_panel, 0));
   }
   FB_CK(cudaGetLastError());
   return FLA_SUCCESS;

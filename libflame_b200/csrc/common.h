@@ -162,9 +162,10 @@ enum GemmMode : int { GEMM_FULL = 0, GEMM_LOWER = 1 };
 int gemm_f64(cudaStream_t st, bool ta, bool tb, long m, long n, long k, double alpha,
              const double* A, long lda, const double* B, long ldb, double beta, double* C,
              long ldc, GemmMode mode = GEMM_FULL, long diag_off = 0,
-             const int* guard = nullptr);
-// The guard pointer is the status block's info word: kernels return at once
-// when it no longer holds INT_MAX (a factorization step has failed).
+             const int* guard = nullptr, int guard_limit = 0x7fffffff);
+// The guard pointer is the status block's info word (INT_MAX, or the first
+// failing column): the kernel returns at once when it holds a column below
+// guard_limit, i.e. when a factorization step this update follows has failed.
 inline const int* info_guard() { return ctx().d_status + ST_INFO; }
 
 // TMA needs 16-byte aligned base and ld*8 % 16 == 0.
@@ -189,6 +190,11 @@ int laswp_dev(double* A, long ld, int row0, const int* d_piv, int npiv, int c0, 
 int trsm_left_dev(DMat T, DMat B, bool lower, bool trans, bool unit, cudaStream_t st);
 int trsm_block(const double* T, long ldt, double* B, long ldb, int b, long n, bool lower,
                bool trans, bool unit, cudaStream_t st);
+// X := inv(L), L b x b lower triangular (unit diagonal if unit), X ld ldx.
+int tri_inverse_lower(const double* L, long ldl, int b, bool unit, double* X, long ldx, cudaStream_t st);
+// LU panel: factor the M x w panel at P with partial pivoting (M >= w);
+// d_piv gets w relative pivots; gcol = global index of the first column.
+int lu_panel_factor(double* P, long ld, long M, int w, int* d_piv, int gcol, cudaStream_t st);
 // X := X inv(L)^T for an m x b block (b <= 128); no-op once *guard != INT_MAX.
 int trsm_right_lt_block(const double* L, long ldl, double* X, long ldx, long m, int b, const int* guard,
                         cudaStream_t st);

@@ -40,7 +40,7 @@ constexpr int THREADS = CONSUMER_WARPS * 32;
 constexpr int A_STAGE_BYTES = BM * BK * 8;  // 16 KB
 constexpr int B_STAGE_BYTES = BN * BK * 8;  // 8 KB
 constexpr int STAGE_BYTES = A_STAGE_BYTES + B_STAGE_BYTES;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 2048 /*align*/ + 256 /*barriers*/;
 
 // Row order of the 8 lane groups of a fragment when the operand's MMA-row
 // index is contiguous in memory (16-row box, two 8-row halves):
@@ -52,13 +52,30 @@ __device__ __forceinline__ int perm16_tab(int half, int g) {
 __device__ __forceinline__ int perm8_tab(int g) { return (g & 3) * 2 + (g >> 2); }
 
 // Byte offset in a stage tile of element (r, k) where r is the MMA-row index
-// (m for A, n for B), for the two storage kinds.
-__device__ __forceinline__ uint32_t off_rcontig(int r, int k) {
-  return (uint32_t)((r >> 4) * (BK * 128) + k * 128 + (((((r & 15) >> 1) ^ (k & 7))) << 4) +
-                    ((r & 1) << 3));
+// (m for A, n for B), for the two storage kinds:
+//   r contiguous: (r>>4)*2048 + k*128 + ((((r&15)>>1) ^ (k&7)) << 4) + (r&1)*8
+//   k contiguous: r*128 + (((k>>1) ^ (r&7)) << 4) + (k&1)*8
+// A lane reads k = 4*kk + t (kk = 0..3 inside a 16-wide k stage, t = lane&3).
+// Every term above occupies its own bits, so the offset splits into a
+// per-lane base (independent of kk) XOR a per-kk constant:
+//   r contiguous: base ^ ((kk << 9) | ((kk & 1) << 6))
+//   k contiguous: base ^ (kk << 5)
+// and, the stage tiles being 2048-byte aligned, the XOR can be applied to the
+// shared-memory address itself (one LOP3 per fragment load).
+__device__ __forceinline__ uint32_t base_rcontig(int r, int t) {
+  return (uint32_t)((r >> 4) * 2048 + t * 128 + ((((r & 15) >> 1) ^ t) << 4) + ((r & 1) << 3));
 }
-__device__ __forceinline__ uint32_t off_kcontig(int r, int k) {
-  return (uint32_t)(r * 128 + ((((k >> 1) ^ (r & 7))) << 4) + ((k & 1) << 3));
+__device__ __forceinline__ uint32_t base_kcontig(int r, int t) {
+  return (uint32_t)(r * 128 + ((t & 1) << 3) + ((((t >> 1) ^ (r & 1))) << 4) + (((r & 7) >> 1) << 5));
+}
+template <bool KC>
+__device__ __forceinline__ constexpr uint32_t kk_xor(int kk) {
+  return KC ? (uint32_t)(kk << 5) : (uint32_t)((kk << 9) | ((kk & 1) << 6));
+}
+__device__ __forceinline__ double lds_f64(uint32_t addr) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(addr));
+  return v;
 }
 
 template <bool A_K, bool B_K>
@@ -66,9 +83,9 @@ __global__ void __launch_bounds__(THREADS, 2)
     dgemm_tma_kernel(const __grid_constant__ CUtensorMap mapA,
                      const __grid_constant__ CUtensorMap mapB, double* __restrict__ C, long ldc,
                      int M, int N, int K, double alpha, double beta, int mode, long diag_off,
-                     int* err, const int* guard) {
+                     int* err, const int* guard, int guard_limit) {
   extern __shared__ unsigned char smem_raw[];
-  if (guard && *((volatile const int*)guard) != 0x7fffffff) return;
+  if (guard && *((volatile const int*)guard) < guard_limit) return;
   const int tile_m = blockIdx.x * BM;
   const int tile_n = blockIdx.y * BN;
   if (mode == GEMM_LOWER) {
@@ -87,7 +104,7 @@ __global__ void __launch_bounds__(THREADS, 2)
         asm volatile("prefetch.global.L2 [%0];" ::"l"(C + (long)r + (long)cc * ldc));
     }
   }
-  uintptr_t base = (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023);
+  uintptr_t base = (reinterpret_cast<uintptr_t>(smem_raw) + 2047) & ~uintptr_t(2047);
   unsigned char* sm = reinterpret_cast<unsigned char*>(base);
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + STAGES * STAGE_BYTES);
   const uint32_t sm_base = smem_u32(sm);
@@ -136,11 +153,14 @@ __global__ void __launch_bounds__(THREADS, 2)
   const int wm = warp & 3, wn = warp >> 2;
   const int g = lane >> 2, t = lane & 3;
   // Fragment row indices within the CTA tile.
-  int ra[4], rb[4];
+  int ra[4];
+  uint32_t aoff[4], boff[4];  // shared-memory bases of the fragments
 #pragma unroll
   for (int f = 0; f < 4; ++f) {
     ra[f] = A_K ? (wm * 32 + 8 * f + perm8_tab(g)) : (wm * 32 + 16 * (f >> 1) + perm16_tab(f & 1, g));
-    rb[f] = B_K ? (wn * 32 + 8 * f + perm8_tab(g)) : (wn * 32 + 16 * (f >> 1) + perm16_tab(f & 1, g));
+    const int rb = B_K ? (wn * 32 + 8 * f + perm8_tab(g)) : (wn * 32 + 16 * (f >> 1) + perm16_tab(f & 1, g));
+    aoff[f] = A_K ? base_kcontig(ra[f], t) : base_rcontig(ra[f], t);
+    boff[f] = A_STAGE_BYTES + (B_K ? base_kcontig(rb, t) : base_rcontig(rb, t));
   }
   double acc[4][4][2];
 #pragma unroll
@@ -163,16 +183,20 @@ __global__ void __launch_bounds__(THREADS, 2)
     }
     if (!ok) break;
     if (!mbar_wait(full0 + 8 * s, (kt / STAGES) & 1, err, 12)) { ok = false; break; }
-    const unsigned char* tA = sm + s * STAGE_BYTES;
-    const unsigned char* tB = tA + A_STAGE_BYTES;
+    const uint32_t tS = sm_base + s * STAGE_BYTES;  // 2048-byte aligned
+    uint32_t pa[4], pb[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      pa[f] = tS + aoff[f];
+      pb[f] = tS + boff[f];
+    }
 #pragma unroll
     for (int kk = 0; kk < BK / 4; ++kk) {
-      int k = kk * 4 + t;
       double a[4], b[4];
 #pragma unroll
       for (int f = 0; f < 4; ++f) {
-        a[f] = *reinterpret_cast<const double*>(tA + (A_K ? off_kcontig(ra[f], k) : off_rcontig(ra[f], k)));
-        b[f] = *reinterpret_cast<const double*>(tB + (B_K ? off_kcontig(rb[f], k) : off_rcontig(rb[f], k)));
+        a[f] = lds_f64(pa[f] ^ kk_xor<A_K>(kk));
+        b[f] = lds_f64(pb[f] ^ kk_xor<B_K>(kk));
       }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
@@ -286,7 +310,7 @@ void set_attrs() {
 
 int gemm_f64(cudaStream_t st, bool ta, bool tb, long m, long n, long k, double alpha,
              const double* A, long lda, const double* B, long ldb, double beta, double* C,
-             long ldc, GemmMode mode, long diag_off, const int* guard) {
+             long ldc, GemmMode mode, long diag_off, const int* guard, int guard_limit) {
   if (m <= 0 || n <= 0) return FLA_SUCCESS;
   if (k <= 0 || alpha == 0.0) {
     // C := beta*C only; k == 0 never occurs on the factorization path with
@@ -313,16 +337,16 @@ int gemm_f64(cudaStream_t st, bool ta, bool tb, long m, long n, long k, double a
   const int pslot = prof_begin(st);
   if (ta && !tb) {
     set_attrs<true, true>();
-    dgemm_tma_kernel<true, true><<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard);
+    dgemm_tma_kernel<true, true><<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard, guard_limit);
   } else if (ta && tb) {
     set_attrs<true, false>();
-    dgemm_tma_kernel<true, false><<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard);
+    dgemm_tma_kernel<true, false><<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard, guard_limit);
   } else if (!ta && !tb) {
     set_attrs<false, true>();
-    dgemm_tma_kernel<false, true><<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard);
+    dgemm_tma_kernel<false, true><<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard, guard_limit);
   } else {
     set_attrs<false, false>();
-    dgemm_tma_kernel<false, false><<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard);
+    dgemm_tma_kernel<false, false><<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard, guard_limit);
   }
   prof_end(pslot, st, PROF_GEMM,
            mode == GEMM_LOWER && m == n ? (double)m * (double)(m + 1) * (double)k

@@ -1,25 +1,29 @@
 // LU factorization with partial pivoting (FLA_LU_piv) on the GPU, plus the
-// row-interchange kernel behind FLA_Apply_pivots.
+// row-interchange kernels behind FLA_Apply_pivots and the blocked left
+// triangular solve of the solves.
 //
 // Blocked right-looking algorithm with the reference's structure
 // (src/lapack/dec/lu/piv/vars/flamec/FLA_LU_piv_blk_var5.c:13-114):
 //   for each block of nb columns:
-//     [A11;A21], p1 := LU_piv([A11;A21])   lu_panel_kernel (cooperative)
-//     pivot [A10;A20] and [A12;A22]         laswp_kernel
-//     A12 := inv(tril_unit(A11)) A12         trsm_tile_kernel (trsm.cu)
+//     [A11;A21], p1 := LU_piv([A11;A21])   lu_panel_factor (lu_panel.cu)
+//     pivot [A10;A20] and [A12;A22]         laswp_block_kernel
+//     A12 := inv(tril_unit(A11)) A12         DMMA GEMM with inv(L11)
 //     A22 -= A21 A12                         DMMA GEMM engine
-// Pivot choice is the reference's: the entry of largest magnitude in the
-// current column, the first (smallest row) among equals (idamax,
-// src/flablas/f2c/idamax.c:41,60 via bl1_damax).  A zero pivot column is
-// not swapped or scaled and its index is reported (the first one), and the
-// factorization continues (FLA_LU_piv_opt_var4.c:272-331).
+// with the next panel factored on a second stream while the trailing update
+// runs (lu_piv_dev below).  Pivot choice is the reference's: the entry of
+// largest magnitude in the current column, the first (smallest row) among
+// equals (idamax, src/flablas/f2c/idamax.c:41,60 via bl1_damax).  A zero
+// pivot column is not swapped or scaled and its index is reported (the first
+// one), and the factorization continues (FLA_LU_piv_opt_var4.c:272-331).
 //
-// Panel kernel: the (m-k) x nb panel is split in row slabs, one per CTA,
-// held in shared memory for the whole panel.  Per column: each CTA finds
-// its local pivot candidate and publishes it (value, row, the full panel
-// row) in global memory; one grid barrier; every CTA then picks the same
-// winner, the owners of rows j and p(j) exchange them, and every CTA
+// lu_panel_kernel (below) is the grid-wide form of the panel: the
+// (m-k) x nb panel is split in row slabs, one per CTA of a cooperative
+// launch, held in shared memory for the whole panel.  Per column: each CTA
+// finds its local pivot candidate and publishes it (value, row, the full
+// panel row) in global memory; one grid barrier; every CTA then picks the
+// same winner, the owners of rows j and p(j) exchange them, and every CTA
 // scales its part of column j and applies the rank-1 update to its slab.
+// It serves the allocation-free single-panel entry point.
 #include <climits>
 #include <mutex>
 
@@ -379,74 +383,85 @@ int trsm_left_dev(DMat T, DMat B, bool lower, bool trans, bool unit, cudaStream_
   return FLA_SUCCESS;
 }
 
+// Outer blocksize of FLA_LU_piv (the reference's 128,
+// FLA_LU_piv_cntl_init.c:29-74); FLA_B200_LU_BLOCKSIZE (a multiple of 16,
+// 16..256) overrides it for tuning.
+int lu_blocksize() {
+  static int nb = 0;
+  if (nb == 0) {
+    nb = NBMAX;
+    if (const char* e = std::getenv("FLA_B200_LU_BLOCKSIZE")) {
+      const int v = std::atoi(e);
+      if (v >= 16 && v <= 256 && v % 16 == 0) nb = v;
+    }
+  }
+  return nb;
+}
+
+// Blocked right-looking LU with a lookahead of one panel:
+//   main stream, step k:  row interchanges of panel k left and right of it;
+//                         A12 := inv(L11) A12 as a DMMA GEMM (inv(L11) was
+//                         formed next to the panel);
+//                         A22(:, next panel) -= A21 A12(:, next panel);
+//   side stream:          factor the next panel (cluster leaves, recursive
+//                         split) and invert its unit lower triangle;
+//   main stream:          A22(:, rest) -= A21 A12(:, rest), concurrently;
+//                         then wait for the side stream.
+// The side stream has the higher priority, so the panel's CTAs are placed
+// as soon as trailing-update CTAs retire.
 int lu_piv_dev(DMat A, int* d_piv, int* info) {
   set_attrs();
   Context& cx = ctx();
-  cudaStream_t st = cx.stream;
+  cudaStream_t st = cx.stream, sd = cx.side;
   const long m = A.m, n = A.n, mn = std::min(m, n);
   *info = -1;
   if (mn == 0) return FLA_SUCCESS;
+  const int NBL = (int)std::min<long>(lu_blocksize(), mn);
+  double* Linv = (double*)ws_get(WS_MISC, sizeof(double) * (size_t)(NBL + 1) * (NBL + 1));
+  double* W = (double*)ws_get(WS_MISC2, sizeof(double) * (size_t)(NBL + 1) * (size_t)std::max<long>(1, n - NBL));
+  if (!Linv || !W) return FLA_FAILURE;
   if (status_reset() != FLA_SUCCESS) return FLA_FAILURE;
-  PanelGeom g0 = panel_geom(m, NBMAX);
-  const int NBL = g0.nb;  // outer blocksize for the whole factorization
-  // panel scratch: candidates for the widest (first) panel
-  const int GMAX = cx.num_sms;  // every panel launch has G <= num_sms CTAs
-  size_t need = sizeof(double) * ((size_t)2 * GMAX * NBL + 2 * GMAX + 2 * NBL) + sizeof(int) * 2 * GMAX + 256;
-  char* ws = (char*)ws_get(WS_PANEL, need);
-  if (!ws) return FLA_FAILURE;
-  double* cand_row = (double*)ws;
-  double* cand_val = cand_row + (size_t)2 * GMAX * NBL;
-  double* diag_row = cand_val + 2 * GMAX;
-  int* cand_idx = (int*)(diag_row + 2 * NBL);
-  unsigned* bar = (unsigned*)(cx.d_status + ST_BAR);
+  cudaEvent_t ev_look = cx.ev[0], ev_panel = cx.ev[1];
+  const long ld = A.ld;
+  auto at = [&](long i, long j) { return A.p + i + j * ld; };
+  auto even = [](long x) { return (x + 1) & ~1L; };  // TMA: 16-byte leading dimensions
 
+  // first panel and its inverse triangle, on the main stream
+  {
+    const int b = (int)std::min<long>(NBL, mn);
+    if (lu_panel_factor(A.p, ld, m, b, d_piv, 0, st) != FLA_SUCCESS) return FLA_FAILURE;
+    if (n > b && tri_inverse_lower(A.p, ld, b, true, Linv, even(b), st) != FLA_SUCCESS) return FLA_FAILURE;
+  }
   for (long k = 0; k < mn; k += NBL) {
     const int b = (int)std::min<long>(NBL, mn - k);
-    const long M = m - k;
-    PanelGeom g = panel_geom(M, NBL);
-    PanelArgs pa;
-    pa.P = A.p + k + k * A.ld;
-    pa.ld = A.ld;
-    pa.M = (int)M;
-    pa.nb = b;
-    pa.R = g.R;
-    pa.lds = g.lds;
-    pa.G = g.G;
-    pa.gcol = (int)k;
-    pa.piv = d_piv + k;
-    pa.cand_row = cand_row;
-    pa.cand_val = cand_val;
-    pa.cand_idx = cand_idx;
-    pa.diag_row = diag_row;
-    pa.bar = bar;
-    pa.err = cx.d_status + ST_ERROR;
-    pa.info = cx.d_status + ST_INFO;
-    FB_CK(cudaMemsetAsync(bar, 0, sizeof(unsigned), st));
-    size_t smem = (size_t)g.lds * b * 8 + (size_t)b * 8;
-    void* args[] = {&pa};
-    const int ps = prof_begin(st);
-    FB_CK(cudaLaunchCooperativeKernel((void*)lu_panel_kernel, dim3(g.G), dim3(PANEL_THREADS), args,
-                                      smem, st));
-    prof_end(ps, st, PROF_PANEL, 0.0);
-    count_launch();
-    // interchanges to the left and right of the panel
-    const long nr = n - k - b;
-    if (laswp_dev(A.p, A.ld, (int)k, d_piv + k, b, 0, (int)k, (int)(k + b), (int)nr, false, st) !=
-        FLA_SUCCESS)
+    const long nr = n - k - b, m2 = m - k - b;
+    if (laswp_dev(A.p, ld, (int)k, d_piv + k, b, 0, (int)k, (int)(k + b), (int)nr, false, st) != FLA_SUCCESS)
       return FLA_FAILURE;
-    if (nr > 0) {
-      double* A11 = A.p + k + k * A.ld;
-      double* A12 = A.p + k + (k + b) * A.ld;
-      if (trsm_block(A11, A.ld, A12, A.ld, b, nr, true, false, true, st) != FLA_SUCCESS) return FLA_FAILURE;
-      const long m2 = m - k - b;
-      if (m2 > 0) {
-        double* A21 = A.p + (k + b) + k * A.ld;
-        double* A22 = A.p + (k + b) + (k + b) * A.ld;
-        if (gemm_f64(st, false, false, m2, nr, b, -1.0, A21, A.ld, A12, A.ld, 1.0, A22, A.ld) !=
-            FLA_SUCCESS)
-          return FLA_FAILURE;
-      }
+    if (nr <= 0) continue;
+    // A12 := inv(L11) A12
+    FB_CK(cudaMemcpy2DAsync(W, sizeof(double) * even(b), at(k, k + b), sizeof(double) * ld, sizeof(double) * b, nr,
+                            cudaMemcpyDeviceToDevice, st));
+    if (gemm_f64(st, false, false, b, nr, b, 1.0, Linv, even(b), W, even(b), 0.0, at(k, k + b), ld) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    if (m2 <= 0) continue;
+    const int nb2 = (int)std::min<long>(NBL, mn - k - b);  // next panel's width (0: none)
+    if (nb2 > 0) {
+      if (gemm_f64(st, false, false, m2, nb2, b, -1.0, at(k + b, k), ld, at(k, k + b), ld, 1.0,
+                   at(k + b, k + b), ld) != FLA_SUCCESS)
+        return FLA_FAILURE;
+      FB_CK(cudaEventRecord(ev_look, st));
+      FB_CK(cudaStreamWaitEvent(sd, ev_look, 0));
+      if (lu_panel_factor(at(k + b, k + b), ld, m2, nb2, d_piv + k + b, (int)(k + b), sd) != FLA_SUCCESS)
+        return FLA_FAILURE;
+      if (nr > nb2 && tri_inverse_lower(at(k + b, k + b), ld, nb2, true, Linv, even(nb2), sd) != FLA_SUCCESS)
+        return FLA_FAILURE;
+      FB_CK(cudaEventRecord(ev_panel, sd));
     }
+    if (nr > nb2 &&
+        gemm_f64(st, false, false, m2, nr - nb2, b, -1.0, at(k + b, k), ld, at(k, k + b + nb2), ld, 1.0,
+                 at(k + b, k + b + nb2), ld) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    if (nb2 > 0) FB_CK(cudaStreamWaitEvent(st, ev_panel, 0));
   }
   return status_read(info);
 }

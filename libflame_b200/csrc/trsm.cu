@@ -16,6 +16,8 @@
 // current unknown (one thread per right-hand side), then update the
 // remaining unknowns (all threads).  The step loop is not unrolled, so the
 // kernel stays small in the instruction cache.
+#include <algorithm>
+
 #include "common.h"
 
 namespace fb {
@@ -159,6 +161,35 @@ int trsm_right_lt_block(const double* L, long ldl, double* X, long ldx, long m, 
   count_launch();
   FB_CK(cudaGetLastError());
   return FLA_SUCCESS;
+}
+
+
+__global__ void set_identity_kernel(double* X, long ldx, int n) {
+  const long total = (long)n * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long r = e % n, c = e / n;
+    X[r + c * ldx] = (r == c) ? 1.0 : 0.0;
+  }
+}
+
+// X := inv(L) for the b x b lower-triangular L (unit diagonal if `unit`),
+// X b x b with leading dimension ldx: X := I, then the blocked left solve
+// L X = I (128-row diagonal solves and GEMM updates).  Used to turn the
+// factorizations' panel triangular solves into DMMA GEMMs.
+int tri_inverse_lower(const double* L, long ldl, int b, bool unit, double* X, long ldx, cudaStream_t st) {
+  if (b <= 0) return FLA_SUCCESS;
+  const int blocks = (int)std::min<long>(1024, ((long)b * b + 255) / 256);
+  set_identity_kernel<<<blocks, 256, 0, st>>>(X, ldx, b);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  DMat T, B;
+  T.p = const_cast<double*>(L);
+  T.ld = ldl;
+  T.m = T.n = b;
+  B.p = X;
+  B.ld = ldx;
+  B.m = B.n = b;
+  return trsm_left_dev(T, B, true, false, unit, st);
 }
 
 }  // namespace fb

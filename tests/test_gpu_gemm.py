@@ -57,3 +57,43 @@ def test_dgemm_lower_mode_leaves_upper_untouched(cuda, flame):
     low = torch.tril(torch.ones(n, n, dtype=torch.bool, device="cuda"))
     assert (got[low] - ref[low]).abs().max().item() < 1e-12
     assert torch.equal(got[~low], Cm[~low])
+
+
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0)])
+@pytest.mark.parametrize("alpha,beta", [(-1.0, 1.0), (0.5, 2.0), (1.0, 0.0)])
+def test_dgemm_many_tiles(cuda, flame, ta, tb, alpha, beta):
+    """More tiles than resident CTAs (several waves), general alpha/beta."""
+    torch = cuda
+    m, n, k = 2000, 3000, 144
+    g = torch.Generator(device="cuda").manual_seed(11 + ta + 2 * tb)
+    A = torch.randn((k, m) if ta else (m, k), dtype=torch.float64, device="cuda", generator=g)
+    B = torch.randn((n, k) if tb else (k, n), dtype=torch.float64, device="cuda", generator=g)
+    Cm = torch.randn((m, n), dtype=torch.float64, device="cuda", generator=g)
+    Ab, Bb, Cb = A.t().contiguous(), B.t().contiguous(), Cm.t().contiguous()
+    rc = flame.lib().FLA_B200_dgemm(ta, tb, m, n, k, alpha, C.c_void_p(Ab.data_ptr()), A.shape[0],
+                                    C.c_void_p(Bb.data_ptr()), B.shape[0], beta,
+                                    C.c_void_p(Cb.data_ptr()), m, 0)
+    assert rc == flame.FLA_SUCCESS, flame.last_error()
+    opA = A.t() if ta else A
+    opB = B.t() if tb else B
+    ref = alpha * (opA @ opB) + beta * Cm
+    err = (Cb.t() - ref).abs().max().item() / ref.abs().max().item()
+    assert err < 1e-14 * k
+
+
+def test_dgemm_lower_mode_many_tiles(cuda, flame):
+    torch = cuda
+    n, k = 2500, 128
+    g = torch.Generator(device="cuda").manual_seed(6)
+    A = torch.randn((n, k), dtype=torch.float64, device="cuda", generator=g)
+    Cm = torch.randn((n, n), dtype=torch.float64, device="cuda", generator=g)
+    Ab = A.t().contiguous()
+    Cb = Cm.t().contiguous()
+    rc = flame.lib().FLA_B200_dgemm(0, 1, n, n, k, -1.0, C.c_void_p(Ab.data_ptr()), n,
+                                    C.c_void_p(Ab.data_ptr()), n, 1.0, C.c_void_p(Cb.data_ptr()), n, 1)
+    assert rc == flame.FLA_SUCCESS
+    got = Cb.t()
+    ref = Cm - A @ A.t()
+    low = torch.tril(torch.ones(n, n, dtype=torch.bool, device="cuda"))
+    assert (got[low] - ref[low]).abs().max().item() < 1e-12
+    assert torch.equal(got[~low], Cm[~low])
