@@ -192,6 +192,23 @@ int trsm_block(const double* T, long ldt, double* B, long ldb, int b, long n, bo
                bool trans, bool unit, cudaStream_t st);
 // X := inv(L), L b x b lower triangular (unit diagonal if unit), X ld ldx.
 int tri_inverse_lower(const double* L, long ldl, int b, bool unit, double* X, long ldx, cudaStream_t st);
+// X := inv(T), T b x b triangular (lower or upper; unit diagonal if unit).
+int tri_inverse(const double* T, long ldt, int b, bool lower, bool unit, double* X, long ldx, cudaStream_t st);
+// X := X inv(op(T)) ^T row by row: every row x of the m x b block X is
+// replaced by the solution of op(T) y = x (b <= 128).
+int trsm_right_block(const double* T, long ldt, double* X, long ldx, long m, int b, bool lower, bool trans,
+                     bool unit, cudaStream_t st);
+// dst := src^T for an m x n src (dst n x m); upper_only writes i <= j only.
+int transpose_dev(const double* src, long lds, double* dst, long ldd, long m, long n, bool upper_only,
+                  cudaStream_t st);
+// Row interchanges on a matrix stored transposed (AT = A^T, column-major):
+// rows row0+i and row0+i+piv[i] of A (columns of AT) are exchanged, in
+// order, over the A-columns [c0, c0+n0) and [c1, c1+n1) (rows of AT).
+int laswp_t_dev(double* AT, long ldt, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
+                cudaStream_t st);
+// LU panel on the transposed matrix: the M x w panel of A whose element
+// (i, j) is at P[i * ld + j] (rows of A are the columns of AT).
+int lu_panel_factor_t(double* P, long ld, long M, int w, int* d_piv, int gcol, cudaStream_t st);
 // LU panel: factor the M x w panel at P with partial pivoting (M >= w);
 // d_piv gets w relative pivots; gcol = global index of the first column.
 int lu_panel_factor(double* P, long ld, long M, int w, int* d_piv, int gcol, cudaStream_t st);

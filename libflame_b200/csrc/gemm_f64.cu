@@ -263,6 +263,48 @@ __global__ void __launch_bounds__(THREADS, 2)
   }
 }
 
+// Fallback for operands the TMA path cannot address (a base or leading
+// dimension that is not 16-byte aligned; only small odd-sized blocks at the
+// edge of a factorization reach it): 32x32 C tiles, 16-deep k slices in SMEM,
+// one thread per C element column pair.
+__global__ void __launch_bounds__(256) dgemm_simt_kernel(int ta, int tb, int M, int N, int K, double alpha,
+                                                         const double* __restrict__ A, long lda,
+                                                         const double* __restrict__ B, long ldb, double beta,
+                                                         double* __restrict__ C, long ldc, int mode, long diag_off,
+                                                         const int* guard, int guard_limit) {
+  if (guard && *((volatile const int*)guard) < guard_limit) return;
+  __shared__ double sA[16][33], sB[16][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int k0 = 0; k0 < K; k0 += 16) {
+    for (int e = threadIdx.x; e < 16 * 32; e += 256) {
+      const int kk = e >> 5, r = e & 31;
+      const int i = i0 + r, j = j0 + r, k = k0 + kk;
+      sA[kk][r] = (i < M && k < K) ? (ta ? A[k + (long)i * lda] : A[i + (long)k * lda]) : 0.0;
+      sB[kk][r] = (j < N && k < K) ? (tb ? B[j + (long)k * ldb] : B[k + (long)j * ldb]) : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = fma(sA[kk][tx], sB[kk][ty + 8 * q], acc[q]);
+    __syncthreads();
+  }
+  const int i = i0 + tx;
+  if (i >= M) return;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int j = j0 + ty + 8 * q;
+    if (j >= N) continue;
+    if (mode == GEMM_LOWER && (long)i - (long)j < diag_off) continue;
+    double* cp = C + i + (long)j * ldc;
+    double v = alpha * acc[q];
+    if (beta != 0.0) v = fma(beta, *cp, v);
+    *cp = v;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Host side: tensor maps through the driver entry point (no -lcuda).
 // ---------------------------------------------------------------------------
@@ -318,8 +360,14 @@ int gemm_f64(cudaStream_t st, bool ta, bool tb, long m, long n, long k, double a
     if (beta == 1.0) return FLA_SUCCESS;
   }
   if (!tma_ok(A, lda) || !tma_ok(B, ldb)) {
-    set_last_error("gemm_f64: operand not 16-byte aligned (base or leading dimension)");
-    return FLA_FAILURE;
+    dim3 g((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));
+    const int ps = prof_begin(st);
+    dgemm_simt_kernel<<<g, 256, 0, st>>>(ta ? 1 : 0, tb ? 1 : 0, (int)m, (int)n, (int)k, alpha, A, lda, B, ldb, beta,
+                                         C, ldc, mode, diag_off, guard, guard_limit);
+    prof_end(ps, st, PROF_GEMM, 2.0 * (double)m * (double)n * (double)k);
+    count_launch();
+    FB_CK(cudaGetLastError());
+    return FLA_SUCCESS;
   }
   // A operand: op(A) is m x k.  ta = false: stored m x k, m contiguous.
   //            ta = true: stored k x m, k contiguous.

@@ -9,8 +9,8 @@
 //     pivot [A10;A20] and [A12;A22]         laswp_block_kernel
 //     A12 := inv(tril_unit(A11)) A12         DMMA GEMM with inv(L11)
 //     A22 -= A21 A12                         DMMA GEMM engine
-// with the next panel factored on a second stream while the trailing update
-// runs (lu_piv_dev below).  Pivot choice is the reference's: the entry of
+// run on the transposed matrix, with the next panel factored on a second
+// stream while the trailing update runs (lu_piv_dev below).  Pivot choice is the reference's: the entry of
 // largest magnitude in the current column, the first (smallest row) among
 // equals (idamax, src/flablas/f2c/idamax.c:41,60 via bl1_damax).  A zero
 // pivot column is not swapped or scaled and its index is reported (the first
@@ -177,8 +177,12 @@ __global__ void __launch_bounds__(PANEL_THREADS) lu_panel_kernel(PanelArgs a) {
 // below them).  Each CTA composes the whole sequence of interchanges into one
 // permutation of the slots (a serial pass over an int array in SMEM), then
 // moves its columns' values with independent, coalesced loads and stores.
+// TR: the matrix is stored transposed (element (row, col) of A at
+// A[col + row * ld]); consecutive threads then take consecutive columns of
+// one slot row, which are contiguous.
 constexpr int LASWP_MAXP = 128;
 constexpr int LASWP_NC = 16;  // columns per CTA (static SMEM < 48 KB)
+template <bool TR>
 __global__ void __launch_bounds__(256) laswp_block_kernel(double* A, long ld, int row0,
                                                           const int* __restrict__ piv, int npiv, int c0,
                                                           int n0, int c1, int n1, int reverse) {
@@ -227,20 +231,23 @@ __global__ void __launch_bounds__(256) laswp_block_kernel(double* A, long ld, in
   const int ncols = n0 + n1;
   const int cbase = blockIdx.x * LASWP_NC;
   // load: consecutive threads take consecutive slots of one column
+  // (consecutive columns of one slot when TR)
   for (int e = tid; e < LASWP_NC * nslot; e += blockDim.x) {
-    const int cl = e / nslot, s = e % nslot;
+    const int cl = TR ? e % LASWP_NC : e / nslot, s = TR ? e / LASWP_NC : e % nslot;
     const int t = cbase + cl;
     if (t >= ncols || s_row[s] < 0) continue;
-    const int col = t < n0 ? c0 + t : c1 + (t - n0);
-    s_val[cl][s] = A[(long)row0 + s_row[s] + (long)col * ld];
+    const long col = t < n0 ? c0 + t : c1 + (t - n0);
+    const long row = (long)row0 + s_row[s];
+    s_val[cl][s] = TR ? A[col + row * ld] : A[row + col * ld];
   }
   __syncthreads();
   for (int e = tid; e < LASWP_NC * nslot; e += blockDim.x) {
-    const int cl = e / nslot, s = e % nslot;
+    const int cl = TR ? e % LASWP_NC : e / nslot, s = TR ? e / LASWP_NC : e % nslot;
     const int t = cbase + cl;
     if (t >= ncols || s_row[s] < 0 || s_src[s] == s) continue;
-    const int col = t < n0 ? c0 + t : c1 + (t - n0);
-    A[(long)row0 + s_row[s] + (long)col * ld] = s_val[cl][s_src[s]];
+    const long col = t < n0 ? c0 + t : c1 + (t - n0);
+    const long row = (long)row0 + s_row[s];
+    (TR ? A[col + row * ld] : A[row + col * ld]) = s_val[cl][s_src[s]];
   }
 }
 
@@ -310,7 +317,7 @@ int laswp_dev(double* A, long ld, int row0, const int* d_piv, int npiv, int c0, 
   if (ncols <= 0 || npiv <= 0) return FLA_SUCCESS;
   const int ps = prof_begin(st);
   if (npiv <= LASWP_MAXP) {
-    laswp_block_kernel<<<(ncols + LASWP_NC - 1) / LASWP_NC, 256, 0, st>>>(A, ld, row0, d_piv, npiv, c0, n0,
+    laswp_block_kernel<false><<<(ncols + LASWP_NC - 1) / LASWP_NC, 256, 0, st>>>(A, ld, row0, d_piv, npiv, c0, n0,
                                                                           c1, n1, reverse ? 1 : 0);
   } else {
     const int threads = 128;
@@ -320,6 +327,24 @@ int laswp_dev(double* A, long ld, int row0, const int* d_piv, int npiv, int c0, 
   prof_end(ps, st, PROF_SWAP, 0.0);
   count_launch();
   FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
+}
+
+// Row interchanges on a transposed matrix (see laswp_block_kernel<true>),
+// npiv <= 128 per launch; longer pivot sequences go in chunks of 128.
+int laswp_t_dev(double* AT, long ldt, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
+                cudaStream_t st) {
+  const int ncols = n0 + n1;
+  if (ncols <= 0 || npiv <= 0) return FLA_SUCCESS;
+  for (int i0 = 0; i0 < npiv; i0 += LASWP_MAXP) {
+    const int cnt = std::min(LASWP_MAXP, npiv - i0);
+    const int ps = prof_begin(st);
+    laswp_block_kernel<true><<<(ncols + LASWP_NC - 1) / LASWP_NC, 256, 0, st>>>(AT, ldt, row0 + i0, d_piv + i0, cnt,
+                                                                               c0, n0, c1, n1, 0);
+    prof_end(ps, st, PROF_SWAP, 0.0);
+    count_launch();
+    FB_CK(cudaGetLastError());
+  }
   return FLA_SUCCESS;
 }
 
@@ -398,14 +423,23 @@ int lu_blocksize() {
   return nb;
 }
 
-// Blocked right-looking LU with a lookahead of one panel:
+// Blocked right-looking LU with a lookahead of one panel, run on A^T.
+//
+// Row interchanges are the costly part of partial pivoting in column-major
+// storage: every interchange touches one element per column, 8-byte pieces
+// scattered over HBM.  The factorization therefore works on AT = A^T (a
+// workspace, n x m column-major), where a row of A is a contiguous column
+// of AT and every interchange moves contiguous pieces; A is transposed in
+// at the start and back at the end (two streaming passes).
+//
 //   main stream, step k:  row interchanges of panel k left and right of it;
-//                         A12 := inv(L11) A12 as a DMMA GEMM (inv(L11) was
-//                         formed next to the panel);
-//                         A22(:, next panel) -= A21 A12(:, next panel);
+//                         U12^T := A12^T inv(L11)^T as a DMMA GEMM
+//                         (inv(L11)^T = inv(L11^T) was formed next to the
+//                         panel);
+//                         A22^T(next panel rows) -= U12^T(next) A21^T;
 //   side stream:          factor the next panel (cluster leaves, recursive
-//                         split) and invert its unit lower triangle;
-//   main stream:          A22(:, rest) -= A21 A12(:, rest), concurrently;
+//                         split) and invert its triangle;
+//   main stream:          A22^T(rest) -= U12^T(rest) A21^T, concurrently;
 //                         then wait for the side stream.
 // The side stream has the higher priority, so the panel's CTAs are placed
 // as soon as trailing-update CTAs retire.
@@ -416,53 +450,58 @@ int lu_piv_dev(DMat A, int* d_piv, int* info) {
   const long m = A.m, n = A.n, mn = std::min(m, n);
   *info = -1;
   if (mn == 0) return FLA_SUCCESS;
+  auto even = [](long x) { return (x + 1) & ~1L; };  // TMA: 16-byte leading dimensions
   const int NBL = (int)std::min<long>(lu_blocksize(), mn);
-  double* Linv = (double*)ws_get(WS_MISC, sizeof(double) * (size_t)(NBL + 1) * (NBL + 1));
-  double* W = (double*)ws_get(WS_MISC2, sizeof(double) * (size_t)(NBL + 1) * (size_t)std::max<long>(1, n - NBL));
-  if (!Linv || !W) return FLA_FAILURE;
+  const long ldT = even(n);
+  double* AT = (double*)ws_get(WS_REPACK, sizeof(double) * (size_t)ldT * (size_t)m);
+  double* X = (double*)ws_get(WS_MISC, sizeof(double) * (size_t)(NBL + 1) * (NBL + 1));
+  double* W = (double*)ws_get(WS_MISC2, sizeof(double) * (size_t)(NBL + 1) * (size_t)even(n));
+  if (!AT || !X || !W) return FLA_FAILURE;
   if (status_reset() != FLA_SUCCESS) return FLA_FAILURE;
   cudaEvent_t ev_look = cx.ev[0], ev_panel = cx.ev[1];
-  const long ld = A.ld;
-  auto at = [&](long i, long j) { return A.p + i + j * ld; };
-  auto even = [](long x) { return (x + 1) & ~1L; };  // TMA: 16-byte leading dimensions
+  // element (i, j) of A inside AT
+  auto t_at = [&](long i, long j) { return AT + j + i * ldT; };
+  if (transpose_dev(A.p, A.ld, AT, ldT, m, n, false, st) != FLA_SUCCESS) return FLA_FAILURE;
 
   // first panel and its inverse triangle, on the main stream
   {
     const int b = (int)std::min<long>(NBL, mn);
-    if (lu_panel_factor(A.p, ld, m, b, d_piv, 0, st) != FLA_SUCCESS) return FLA_FAILURE;
-    if (n > b && tri_inverse_lower(A.p, ld, b, true, Linv, even(b), st) != FLA_SUCCESS) return FLA_FAILURE;
+    if (lu_panel_factor_t(AT, ldT, m, b, d_piv, 0, st) != FLA_SUCCESS) return FLA_FAILURE;
+    if (n > b && tri_inverse(AT, ldT, b, false, true, X, even(b), st) != FLA_SUCCESS) return FLA_FAILURE;
   }
   for (long k = 0; k < mn; k += NBL) {
     const int b = (int)std::min<long>(NBL, mn - k);
     const long nr = n - k - b, m2 = m - k - b;
-    if (laswp_dev(A.p, ld, (int)k, d_piv + k, b, 0, (int)k, (int)(k + b), (int)nr, false, st) != FLA_SUCCESS)
+    if (laswp_t_dev(AT, ldT, (int)k, d_piv + k, b, 0, (int)k, (int)(k + b), (int)nr, st) != FLA_SUCCESS)
       return FLA_FAILURE;
     if (nr <= 0) continue;
-    // A12 := inv(L11) A12
-    FB_CK(cudaMemcpy2DAsync(W, sizeof(double) * even(b), at(k, k + b), sizeof(double) * ld, sizeof(double) * b, nr,
-                            cudaMemcpyDeviceToDevice, st));
-    if (gemm_f64(st, false, false, b, nr, b, 1.0, Linv, even(b), W, even(b), 0.0, at(k, k + b), ld) != FLA_SUCCESS)
+    // U12^T := A12^T inv(L11^T): A12^T is the nr x b block at t_at(k, k + b)
+    FB_CK(cudaMemcpy2DAsync(W, sizeof(double) * even(nr), t_at(k, k + b), sizeof(double) * ldT,
+                            sizeof(double) * nr, b, cudaMemcpyDeviceToDevice, st));
+    if (gemm_f64(st, false, false, nr, b, b, 1.0, W, even(nr), X, even(b), 0.0, t_at(k, k + b), ldT) !=
+        FLA_SUCCESS)
       return FLA_FAILURE;
     if (m2 <= 0) continue;
     const int nb2 = (int)std::min<long>(NBL, mn - k - b);  // next panel's width (0: none)
     if (nb2 > 0) {
-      if (gemm_f64(st, false, false, m2, nb2, b, -1.0, at(k + b, k), ld, at(k, k + b), ld, 1.0,
-                   at(k + b, k + b), ld) != FLA_SUCCESS)
+      if (gemm_f64(st, false, false, nb2, m2, b, -1.0, t_at(k, k + b), ldT, t_at(k + b, k), ldT, 1.0,
+                   t_at(k + b, k + b), ldT) != FLA_SUCCESS)
         return FLA_FAILURE;
       FB_CK(cudaEventRecord(ev_look, st));
       FB_CK(cudaStreamWaitEvent(sd, ev_look, 0));
-      if (lu_panel_factor(at(k + b, k + b), ld, m2, nb2, d_piv + k + b, (int)(k + b), sd) != FLA_SUCCESS)
+      if (lu_panel_factor_t(t_at(k + b, k + b), ldT, m2, nb2, d_piv + k + b, (int)(k + b), sd) != FLA_SUCCESS)
         return FLA_FAILURE;
-      if (nr > nb2 && tri_inverse_lower(at(k + b, k + b), ld, nb2, true, Linv, even(nb2), sd) != FLA_SUCCESS)
+      if (nr > nb2 && tri_inverse(t_at(k + b, k + b), ldT, nb2, false, true, X, even(nb2), sd) != FLA_SUCCESS)
         return FLA_FAILURE;
       FB_CK(cudaEventRecord(ev_panel, sd));
     }
     if (nr > nb2 &&
-        gemm_f64(st, false, false, m2, nr - nb2, b, -1.0, at(k + b, k), ld, at(k, k + b + nb2), ld, 1.0,
-                 at(k + b, k + b + nb2), ld) != FLA_SUCCESS)
+        gemm_f64(st, false, false, nr - nb2, m2, b, -1.0, t_at(k, k + b + nb2), ldT, t_at(k + b, k), ldT, 1.0,
+                 t_at(k + b, k + b + nb2), ldT) != FLA_SUCCESS)
       return FLA_FAILURE;
     if (nb2 > 0) FB_CK(cudaStreamWaitEvent(st, ev_panel, 0));
   }
+  if (transpose_dev(AT, ldT, A.p, A.ld, n, m, false, st) != FLA_SUCCESS) return FLA_FAILURE;
   return status_read(info);
 }
 

@@ -69,6 +69,9 @@ __host__ __device__ inline size_t leaf_smem_bytes(int lds, int w, int C) {
   return sizeof(double) * ((size_t)lds * w + 2 * (size_t)C * w + 2 * C + 2 * w) + sizeof(int) * 2 * C + 64;
 }
 
+// RM: the panel is stored transposed (element (i, col) at P[i * ld + col],
+// rows of A being columns of A^T); otherwise column-major.
+template <bool RM>
 __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafArgs a) {
   extern __shared__ double S[];
   __shared__ double s_rv[LEAF_THREADS / 32];
@@ -88,8 +91,15 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
 
   const int r0 = c * a.R;
   const int rows = max(0, min(a.R, a.M - r0));
-  for (int col = 0; col < w; ++col)
-    for (int i = tid; i < rows; i += LEAF_THREADS) slab[i + col * lds] = a.P[(long)(r0 + i) + (long)col * a.ld];
+  if (RM) {
+    for (int e = tid; e < rows * w; e += LEAF_THREADS) {
+      const int i = e / w, col = e - i * w;
+      slab[i + col * lds] = a.P[(long)(r0 + i) * a.ld + col];
+    }
+  } else {
+    for (int col = 0; col < w; ++col)
+      for (int i = tid; i < rows; i += LEAF_THREADS) slab[i + col * lds] = a.P[(long)(r0 + i) + (long)col * a.ld];
+  }
   __syncthreads();
 
   int first_null = -1;
@@ -198,8 +208,15 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
     }
     __syncthreads();
   }
-  for (int col = 0; col < w; ++col)
-    for (int i = tid; i < rows; i += LEAF_THREADS) a.P[(long)(r0 + i) + (long)col * a.ld] = slab[i + col * lds];
+  if (RM) {
+    for (int e = tid; e < rows * w; e += LEAF_THREADS) {
+      const int i = e / w, col = e - i * w;
+      a.P[(long)(r0 + i) * a.ld + col] = slab[i + col * lds];
+    }
+  } else {
+    for (int col = 0; col < w; ++col)
+      for (int i = tid; i < rows; i += LEAF_THREADS) a.P[(long)(r0 + i) + (long)col * a.ld] = slab[i + col * lds];
+  }
   if (c == 0 && tid == 0 && first_null >= 0) atomicMin(a.info, a.gcol + first_null);
 }
 
@@ -214,9 +231,10 @@ int leaf_setup() {
   if (g_leaf.ready) return FLA_SUCCESS;
   Context& cx = ctx();
   g_leaf.smem_cap = std::min<size_t>(cx.smem_optin, 227 * 1024) - 1024;
-  FB_CK(cudaFuncSetAttribute(lu_leaf_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)g_leaf.smem_cap));
-  FB_CK(cudaFuncSetAttribute(lu_leaf_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  for (auto kern : {lu_leaf_cluster_kernel<false>, lu_leaf_cluster_kernel<true>}) {
+    FB_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g_leaf.smem_cap));
+    FB_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  }
   // Largest cluster (16, else 8, 4 ...) that can be resident with a full
   // shared-memory slab per CTA.
   g_leaf.max_cluster = 1;
@@ -233,7 +251,7 @@ int leaf_setup() {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int nclusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&nclusters, lu_leaf_cluster_kernel, &cfg) == cudaSuccess &&
+    if (cudaOccupancyMaxActiveClusters(&nclusters, lu_leaf_cluster_kernel<false>, &cfg) == cudaSuccess &&
         nclusters > 0) {
       g_leaf.max_cluster = cs;
       break;
@@ -265,7 +283,7 @@ bool leaf_geometry(long M, int w, int* C, int* R, int* lds, size_t* smem) {
   return false;
 }
 
-int leaf_launch(double* P, long ld, long M, int w, int* d_piv, int gcol, cudaStream_t st) {
+int leaf_launch(double* P, long ld, long M, int w, int* d_piv, int gcol, bool rm, cudaStream_t st) {
   int C = 0, R = 0, lds = 0;
   size_t smem = 0;
   if (!leaf_geometry(M, w, &C, &R, &lds, &smem)) {
@@ -295,7 +313,10 @@ int leaf_launch(double* P, long ld, long M, int w, int* d_piv, int gcol, cudaStr
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   const int ps = prof_begin(st);
-  FB_CK(cudaLaunchKernelEx(&cfg, lu_leaf_cluster_kernel, la));
+  if (rm)
+    FB_CK(cudaLaunchKernelEx(&cfg, lu_leaf_cluster_kernel<true>, la));
+  else
+    FB_CK(cudaLaunchKernelEx(&cfg, lu_leaf_cluster_kernel<false>, la));
   prof_end(ps, st, PROF_PANEL, 0.0);
   count_launch();
   return FLA_SUCCESS;
@@ -310,7 +331,7 @@ int lu_panel_factor(double* P, long ld, long M, int w, int* d_piv, int gcol, cud
   if (w <= 0 || M <= 0) return FLA_SUCCESS;
   int C, R, lds;
   size_t smem;
-  if (leaf_geometry(M, w, &C, &R, &lds, &smem) || w <= 2) return leaf_launch(P, ld, M, w, d_piv, gcol, st);
+  if (leaf_geometry(M, w, &C, &R, &lds, &smem) || w <= 2) return leaf_launch(P, ld, M, w, d_piv, gcol, false, st);
   // split: left half a multiple of 2 columns (keeps 16-byte alignment)
   const int w1 = std::max(2, (w / 2) & ~1);
   const int w2 = w - w1;
@@ -323,6 +344,35 @@ int lu_panel_factor(double* P, long ld, long M, int w, int* d_piv, int gcol, cud
       return FLA_FAILURE;
     if (lu_panel_factor(P12 + w1, ld, M - w1, w2, d_piv + w1, gcol + w1, st) != FLA_SUCCESS) return FLA_FAILURE;
     if (laswp_dev(P, ld, w1, d_piv + w1, (int)std::min<long>(w2, M - w1), 0, w1, 0, 0, false, st) != FLA_SUCCESS)
+      return FLA_FAILURE;
+  }
+  return FLA_SUCCESS;
+}
+
+
+// The same recursion on a panel stored transposed (element (i, j) of the
+// panel at P[i * ld + j]): row interchanges move contiguous pieces of
+// columns of A^T, the top-right solve is a row-wise solve with L11 (held as
+// the upper triangle L11^T), and the update is A22^T -= U12^T A21^T.
+int lu_panel_factor_t(double* P, long ld, long M, int w, int* d_piv, int gcol, cudaStream_t st) {
+  if (leaf_setup() != FLA_SUCCESS) return FLA_FAILURE;
+  if (w <= 0 || M <= 0) return FLA_SUCCESS;
+  int C, R, lds;
+  size_t smem;
+  if (leaf_geometry(M, w, &C, &R, &lds, &smem) || w <= 2) return leaf_launch(P, ld, M, w, d_piv, gcol, true, st);
+  const int w1 = std::max(2, (w / 2) & ~1);
+  const int w2 = w - w1;
+  if (lu_panel_factor_t(P, ld, M, w1, d_piv, gcol, st) != FLA_SUCCESS) return FLA_FAILURE;
+  if (laswp_t_dev(P, ld, 0, d_piv, w1, w1, w2, 0, 0, st) != FLA_SUCCESS) return FLA_FAILURE;
+  // U12^T (w2 x w1 at P + w1): each row y solves L11 y = x
+  if (trsm_right_block(P, ld, P + w1, ld, w2, w1, false, true, true, st) != FLA_SUCCESS) return FLA_FAILURE;
+  if (M > w1) {
+    if (gemm_f64(st, false, false, w2, M - w1, w1, -1.0, P + w1, ld, P + (long)w1 * ld, ld, 1.0,
+                 P + w1 + (long)w1 * ld, ld) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    if (lu_panel_factor_t(P + w1 + (long)w1 * ld, ld, M - w1, w2, d_piv + w1, gcol + w1, st) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    if (laswp_t_dev(P, ld, w1, d_piv + w1, (int)std::min<long>(w2, M - w1), 0, w1, 0, 0, st) != FLA_SUCCESS)
       return FLA_FAILURE;
   }
   return FLA_SUCCESS;

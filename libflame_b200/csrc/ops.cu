@@ -12,8 +12,6 @@ int trsm_left_dev(DMat T, DMat B, bool lower, bool trans, bool unit, cudaStream_
 int laswp_dev(double* A, long ld, int row0, const int* d_piv, int npiv, int c0, int n0, int c1,
               int n1, bool reverse, cudaStream_t st);
 
-namespace {
-
 // dst := src^T for an m x n src (dst is n x m).  tri = 1: only the upper
 // triangle of dst (i <= j) is written.
 __global__ void transpose_kernel(const double* __restrict__ src, long lds, double* __restrict__ dst,
@@ -40,6 +38,8 @@ int transpose_dev(const double* src, long lds, double* dst, long ldd, long m, lo
   FB_CK(cudaGetLastError());
   return FLA_SUCCESS;
 }
+
+namespace {
 
 __global__ void shift_pivots_kernel(int* p, int n, int delta_sign) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -119,6 +119,13 @@ void set_attrs() {
   set_attr_one<false, true, true, false>();
   set_attr_one<false, true, false, false>();
   set_attr_one<true, false, false, true>();
+  set_attr_one<true, false, true, true>();
+  set_attr_one<true, true, false, true>();
+  set_attr_one<true, true, true, true>();
+  set_attr_one<false, false, false, true>();
+  set_attr_one<false, false, true, true>();
+  set_attr_one<false, true, false, true>();
+  set_attr_one<false, true, true, true>();
   g_attr = true;
 }
 
@@ -190,6 +197,48 @@ int tri_inverse_lower(const double* L, long ldl, int b, bool unit, double* X, lo
   B.ld = ldx;
   B.m = B.n = b;
   return trsm_left_dev(T, B, true, false, unit, st);
+}
+
+
+// Every row x of the m x b block X := solution y of op(T) y = x, i.e.
+// X := X inv(op(T))^T (T b x b, b <= 128).
+int trsm_right_block(const double* T, long ldt, double* X, long ldx, long m, int b, bool lower, bool trans,
+                     bool unit, cudaStream_t st) {
+  set_attrs();
+  if (m <= 0 || b <= 0) return FLA_SUCCESS;
+  const unsigned grid = (unsigned)((m + NV - 1) / NV);
+  const int ps = prof_begin(st);
+#define FB_TRSM_R(L, T_, U) \
+  trsm_tile_kernel<L, T_, U, true><<<grid, THREADS, SMEM, st>>>(T, ldt, X, ldx, b, (int)m, nullptr)
+  if (lower) {
+    if (!trans) { if (unit) FB_TRSM_R(true, false, true); else FB_TRSM_R(true, false, false); }
+    else        { if (unit) FB_TRSM_R(true, true, true);  else FB_TRSM_R(true, true, false); }
+  } else {
+    if (!trans) { if (unit) FB_TRSM_R(false, false, true); else FB_TRSM_R(false, false, false); }
+    else        { if (unit) FB_TRSM_R(false, true, true);  else FB_TRSM_R(false, true, false); }
+  }
+#undef FB_TRSM_R
+  prof_end(ps, st, PROF_TRSM, (double)m * (double)b * (double)b);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
+}
+
+// X := inv(T) for a b x b triangular T: X := I, then the blocked left solve.
+int tri_inverse(const double* T, long ldt, int b, bool lower, bool unit, double* X, long ldx, cudaStream_t st) {
+  if (b <= 0) return FLA_SUCCESS;
+  const int blocks = (int)std::min<long>(1024, ((long)b * b + 255) / 256);
+  set_identity_kernel<<<blocks, 256, 0, st>>>(X, ldx, b);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  DMat Tm, B;
+  Tm.p = const_cast<double*>(T);
+  Tm.ld = ldt;
+  Tm.m = Tm.n = b;
+  B.p = X;
+  B.ld = ldx;
+  B.m = B.n = b;
+  return trsm_left_dev(Tm, B, lower, false, unit, st);
 }
 
 }  // namespace fb
