@@ -9,11 +9,12 @@
 // FLA_Herk_external.c:83).  GEMM_LOWER writes only the lower triangle
 // (i - j >= diag_off), which is the SYRK update of the Cholesky.
 //
-// Tile: 128 (m) x 64 (n) per CTA, k staged 16 at a time, 4 stages.
-// 8 warps in a 4 x 2 grid, each owning a 32 x 32 sub-tile as 4 x 4 m8n8
-// DMMA accumulators; thread 0 also issues the TMA loads (refilling a stage
-// once all 8 warps have released it).  Two CTAs share an SM so one CTA's
-// epilogue overlaps the other's MMAs.
+// Tile: 64 (m) x 64 (n) per CTA with 4 warps and 3 stages, four CTAs per SM
+// (or 128 x 64 with 8 warps and 4 stages, two CTAs per SM); k staged 16 at a
+// time.  Warps form a (BM/32) x 2 grid, each owning a 32 x 32 sub-tile as
+// 4 x 4 m8n8 DMMA accumulators; thread 0 also issues the TMA loads
+// (refilling a stage once all warps have released it).  Several CTAs share
+// an SM so one CTA's prologue and epilogue overlap the others' MMAs.
 //
 // Shared-memory layout: TMA boxes are 128 bytes wide (16 doubles) with the
 // 128-byte swizzle (16-byte chunk index XOR row index mod 8).  An operand
@@ -34,13 +35,23 @@ namespace fb {
 
 namespace {
 
-constexpr int BM = 128, BN = 64, BK = 16, STAGES = 4;
-constexpr int CONSUMER_WARPS = 8;
-constexpr int THREADS = CONSUMER_WARPS * 32;
-constexpr int A_STAGE_BYTES = BM * BK * 8;  // 16 KB
-constexpr int B_STAGE_BYTES = BN * BK * 8;  // 8 KB
-constexpr int STAGE_BYTES = A_STAGE_BYTES + B_STAGE_BYTES;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 2048 /*align*/ + 256 /*barriers*/;
+constexpr int BN = 64, BK = 16;
+
+// Tile shapes: BM = 128 (8 warps, 4 stages, 2 CTAs per SM) or BM = 64
+// (4 warps, 3 stages, 4 CTAs per SM).  Each warp owns a 32 x 32 sub-tile.
+template <int BM_>
+struct Tile {
+  static constexpr int BM = BM_;
+  static constexpr int WM = BM / 32;                 // warps along m (2 along n)
+  static constexpr int WARPS = WM * 2;
+  static constexpr int THREADS = WARPS * 32;
+  static constexpr int STAGES = BM == 128 ? 4 : 3;
+  static constexpr int MINB = BM == 128 ? 2 : 4;      // CTAs per SM
+  static constexpr int A_STAGE_BYTES = BM * BK * 8;
+  static constexpr int B_STAGE_BYTES = BN * BK * 8;
+  static constexpr int STAGE_BYTES = A_STAGE_BYTES + B_STAGE_BYTES;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 2048 /*align*/ + 256 /*barriers*/;
+};
 
 // Row order of the 8 lane groups of a fragment when the operand's MMA-row
 // index is contiguous in memory (16-row box, two 8-row halves):
@@ -78,12 +89,15 @@ __device__ __forceinline__ double lds_f64(uint32_t addr) {
   return v;
 }
 
-template <bool A_K, bool B_K>
-__global__ void __launch_bounds__(THREADS, 2)
+template <bool A_K, bool B_K, int BM_>
+__global__ void __launch_bounds__(Tile<BM_>::THREADS, Tile<BM_>::MINB)
     dgemm_tma_kernel(const __grid_constant__ CUtensorMap mapA,
                      const __grid_constant__ CUtensorMap mapB, double* __restrict__ C, long ldc,
                      int M, int N, int K, double alpha, double beta, int mode, long diag_off,
                      int* err, const int* guard, int guard_limit) {
+  using TC = Tile<BM_>;
+  constexpr int BM = TC::BM, STAGES = TC::STAGES, THREADS = TC::THREADS, CONSUMER_WARPS = TC::WARPS;
+  constexpr int A_STAGE_BYTES = TC::A_STAGE_BYTES, STAGE_BYTES = TC::STAGE_BYTES;
   extern __shared__ unsigned char smem_raw[];
   if (guard && *((volatile const int*)guard) < guard_limit) return;
   const int tile_m = blockIdx.x * BM;
@@ -150,7 +164,7 @@ __global__ void __launch_bounds__(THREADS, 2)
   }
 
   // ---------------- consumers ----------------
-  const int wm = warp & 3, wn = warp >> 2;
+  const int wm = warp % TC::WM, wn = warp / TC::WM;
   const int g = lane >> 2, t = lane & 3;
   // Fragment row indices within the CTA tile.
   int ra[4];
@@ -234,11 +248,12 @@ __global__ void __launch_bounds__(THREADS, 2)
     }
   __syncthreads();
   const bool vec = ((reinterpret_cast<uintptr_t>(C) & 15u) == 0) && ((ldc & 1) == 0);
-  // thread -> (row pair, column): 64 row pairs x 4 columns per pass
-  const int rp = threadIdx.x & 63, c0 = threadIdx.x >> 6;
+  // thread -> (row pair, column): BM/2 row pairs x THREADS/(BM/2) columns per pass
+  constexpr int RP = BM / 2;
+  const int rp = threadIdx.x % RP, c0 = threadIdx.x / RP;
   const int row = tile_m + 2 * rp;
 #pragma unroll 4
-  for (int cl = c0; cl < BN; cl += THREADS / 64) {
+  for (int cl = c0; cl < BN; cl += THREADS / RP) {
     const int col = tile_n + cl;
     if (col >= N || row >= M) continue;
     double* cp = C + (long)row + (long)col * ldc;
@@ -338,14 +353,37 @@ bool make_map(CUtensorMap* map, const double* p, long rows, long cols, long ld, 
   return r == CUDA_SUCCESS;
 }
 
-template <bool A_K, bool B_K>
+template <bool A_K, bool B_K, int BM_>
 void set_attrs() {
   static bool done = false;
   if (!done) {
-    cudaFuncSetAttribute(dgemm_tma_kernel<A_K, B_K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         SMEM_BYTES);
+    cudaFuncSetAttribute(dgemm_tma_kernel<A_K, B_K, BM_>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         Tile<BM_>::SMEM_BYTES);
     done = true;
   }
+}
+
+template <bool A_K, bool B_K, int BM_>
+void launch(dim3 grid, cudaStream_t st, const CUtensorMap& mA, const CUtensorMap& mB, double* C, long ldc, long m,
+            long n, long k, double alpha, double beta, GemmMode mode, long diag_off, int* err, const int* guard,
+            int guard_limit) {
+  set_attrs<A_K, B_K, BM_>();
+  dgemm_tma_kernel<A_K, B_K, BM_><<<grid, Tile<BM_>::THREADS, Tile<BM_>::SMEM_BYTES, st>>>(
+      mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard, guard_limit);
+}
+
+// Tile height: 64 (four CTAs per SM hide one another's prologue and
+// epilogue best on the rank-128 updates of the factorizations: 26.6 against
+// 25.0 TFLOP/s at 16256 x 16256 x 128); FLA_B200_GEMM_BM=128 selects the
+// 128-row tile.
+int tile_bm() {
+  static int bm = 0;
+  if (bm == 0) {
+    bm = 64;
+    if (const char* e = std::getenv("FLA_B200_GEMM_BM"))
+      if (std::atoi(e) == 128) bm = 128;
+  }
+  return bm;
 }
 
 }  // namespace
@@ -374,28 +412,26 @@ int gemm_f64(cudaStream_t st, bool ta, bool tb, long m, long n, long k, double a
   // B operand: op(B) is k x n.  tb = false: stored k x n, k contiguous.
   //            tb = true: stored n x k, n contiguous.
   CUtensorMap mA, mB;
-  bool okA = ta ? make_map(&mA, A, k, m, lda, 16, BM) : make_map(&mA, A, m, k, lda, 16, BK);
+  const int BMv = tile_bm();
+  bool okA = ta ? make_map(&mA, A, k, m, lda, 16, BMv) : make_map(&mA, A, m, k, lda, 16, BK);
   bool okB = tb ? make_map(&mB, B, n, k, ldb, 16, BK) : make_map(&mB, B, k, n, ldb, 16, BN);
   if (!okA || !okB) {
     set_last_error("gemm_f64: cuTensorMapEncodeTiled failed");
     return FLA_FAILURE;
   }
-  dim3 grid((unsigned)((m + BM - 1) / BM), (unsigned)((n + BN - 1) / BN));
+  dim3 grid((unsigned)((m + BMv - 1) / BMv), (unsigned)((n + BN - 1) / BN));
   int* err = ctx().d_status + ST_ERROR;
   const int pslot = prof_begin(st);
-  if (ta && !tb) {
-    set_attrs<true, true>();
-    dgemm_tma_kernel<true, true><<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard, guard_limit);
-  } else if (ta && tb) {
-    set_attrs<true, false>();
-    dgemm_tma_kernel<true, false><<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard, guard_limit);
-  } else if (!ta && !tb) {
-    set_attrs<false, true>();
-    dgemm_tma_kernel<false, true><<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard, guard_limit);
-  } else {
-    set_attrs<false, false>();
-    dgemm_tma_kernel<false, false><<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard, guard_limit);
-  }
+#define FB_GEMM_LAUNCH(AK, BK_)                                                                                  \
+  (BMv == 64 ? launch<AK, BK_, 64>(grid, st, mA, mB, C, ldc, m, n, k, alpha, beta, mode, diag_off, err, guard,  \
+                                   guard_limit)                                                                 \
+             : launch<AK, BK_, 128>(grid, st, mA, mB, C, ldc, m, n, k, alpha, beta, mode, diag_off, err, guard, \
+                                    guard_limit))
+  if (ta && !tb) FB_GEMM_LAUNCH(true, true);
+  else if (ta && tb) FB_GEMM_LAUNCH(true, false);
+  else if (!ta && !tb) FB_GEMM_LAUNCH(false, true);
+  else FB_GEMM_LAUNCH(false, false);
+#undef FB_GEMM_LAUNCH
   prof_end(pslot, st, PROF_GEMM,
            mode == GEMM_LOWER && m == n ? (double)m * (double)(m + 1) * (double)k
                                         : 2.0 * (double)m * (double)n * (double)k);
