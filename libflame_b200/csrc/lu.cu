@@ -6,7 +6,7 @@
 // (src/lapack/dec/lu/piv/vars/flamec/FLA_LU_piv_blk_var5.c:13-114):
 //   for each block of nb columns:
 //     [A11;A21], p1 := LU_piv([A11;A21])   lu_panel_factor (lu_panel.cu)
-//     pivot [A10;A20] and [A12;A22]         laswp_block_kernel
+//     pivot [A10;A20] and [A12;A22]         laswp_compose/apply kernels
 //     A12 := inv(tril_unit(A11)) A12         DMMA GEMM with inv(L11)
 //     A22 -= A21 A12                         DMMA GEMM engine
 // run on the transposed matrix, with the next panel factored on a second
@@ -172,37 +172,41 @@ __global__ void __launch_bounds__(PANEL_THREADS) lu_panel_kernel(PanelArgs a) {
 // row0+i+piv[i] are swapped for i = 0..npiv-1 in order (or in reverse when
 // `reverse`, which applies P^T).  Columns: [c0, c0+n0) and [c1, c1+n1).
 //
-// laswp_block_kernel (npiv <= LASWP_MAXP): the interchanges touch at most
-// 2*npiv rows ("slots": rows row0..row0+npiv-1, then each distinct target
-// below them).  Each CTA composes the whole sequence of interchanges into one
-// permutation of the slots (a serial pass over an int array in SMEM), then
-// moves its columns' values with independent, coalesced loads and stores.
+// Blocked form (npiv <= LASWP_MAXP): the interchanges touch at most 2*npiv
+// rows ("slots": rows row0..row0+npiv-1, then each distinct target below
+// them).  laswp_compose_kernel (one CTA) composes the whole sequence of
+// interchanges into one permutation of the slots and writes it to a small
+// device table; laswp_apply_kernel then moves every column's slot values
+// with independent, coalesced loads and stores, LASWP_NC columns per CTA.
 // TR: the matrix is stored transposed (element (row, col) of A at
 // A[col + row * ld]); consecutive threads then take consecutive columns of
 // one slot row, which are contiguous.
 constexpr int LASWP_MAXP = 128;
 constexpr int LASWP_NC = 16;  // columns per CTA (static SMEM < 48 KB)
-template <bool TR>
-__global__ void __launch_bounds__(256) laswp_block_kernel(double* A, long ld, int row0,
-                                                          const int* __restrict__ piv, int npiv, int c0,
-                                                          int n0, int c1, int n1, int reverse) {
+// table layout (ints): [0] nslot, [1 .. 2*MAXP] slot rows (offset from row0,
+// -1 unused), [1 + 2*MAXP .. 4*MAXP] slot sources
+constexpr int LASWP_TABLE_INTS = 1 + 4 * LASWP_MAXP;
+
+__global__ void __launch_bounds__(256) laswp_compose_kernel(const int* __restrict__ piv, int npiv, int reverse,
+                                                            int* __restrict__ table) {
+  __shared__ int s_piv[LASWP_MAXP];
   __shared__ int s_tgt[LASWP_MAXP];          // slot of the target of interchange i
   __shared__ int s_row[2 * LASWP_MAXP];      // row offset (from row0) of each slot, -1 unused
   __shared__ int s_src[2 * LASWP_MAXP];      // final content of slot s = original slot s_src[s]
-  __shared__ double s_val[LASWP_NC][2 * LASWP_MAXP + 1];
   const int tid = threadIdx.x;
   const int nslot = 2 * npiv;
   for (int s = tid; s < nslot; s += blockDim.x) s_row[s] = (s < npiv) ? s : -1;
+  if (tid < npiv) s_piv[tid] = piv[tid];
   __syncthreads();
   if (tid < npiv) {
-    const int t = tid + piv[tid];  // target row offset
+    const int t = tid + s_piv[tid];  // target row offset
     int slot;
     if (t < npiv) {
       slot = t;
     } else {
       int first = tid;  // first interchange with the same far target owns the slot
       for (int i2 = 0; i2 < tid; ++i2)
-        if (i2 + piv[i2] == t) { first = i2; break; }
+        if (i2 + s_piv[i2] == t) { first = i2; break; }
       slot = npiv + first;
       if (first == tid) s_row[slot] = t;
     }
@@ -226,6 +230,26 @@ __global__ void __launch_bounds__(256) laswp_block_kernel(double* A, long ld, in
         s_src[b] = x;
       }
     }
+    table[0] = nslot;
+  }
+  __syncthreads();
+  for (int s = tid; s < nslot; s += blockDim.x) {
+    table[1 + s] = s_row[s];
+    table[1 + 2 * LASWP_MAXP + s] = s_src[s];
+  }
+}
+
+template <bool TR>
+__global__ void __launch_bounds__(256) laswp_apply_kernel(double* A, long ld, int row0, const int* __restrict__ table,
+                                                          int c0, int n0, int c1, int n1) {
+  __shared__ int s_row[2 * LASWP_MAXP];
+  __shared__ int s_src[2 * LASWP_MAXP];
+  __shared__ double s_val[LASWP_NC][2 * LASWP_MAXP + 1];
+  const int tid = threadIdx.x;
+  const int nslot = table[0];
+  for (int s = tid; s < nslot; s += blockDim.x) {
+    s_row[s] = table[1 + s];
+    s_src[s] = table[1 + 2 * LASWP_MAXP + s];
   }
   __syncthreads();
   const int ncols = n0 + n1;
@@ -311,39 +335,57 @@ PanelGeom panel_geom(long M, int nb_max) {
 
 }  // namespace
 
+// Slot tables of the blocked row interchanges: one per stream that may run
+// interchanges concurrently (the main and the lookahead stream).
+int* laswp_table(cudaStream_t st) {
+  int* base = (int*)ws_get(WS_PANEL, sizeof(int) * 2 * LASWP_TABLE_INTS + 256);
+  if (!base) return nullptr;
+  return base + (st == ctx().side ? LASWP_TABLE_INTS : 0);
+}
+
+int laswp_blocked(double* A, long ld, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
+                  bool reverse, bool tr, cudaStream_t st) {
+  const int ncols = n0 + n1;
+  int* table = laswp_table(st);
+  if (!table) return FLA_FAILURE;
+  const int ps = prof_begin(st);
+  laswp_compose_kernel<<<1, 256, 0, st>>>(d_piv, npiv, reverse ? 1 : 0, table);
+  const unsigned grid = (unsigned)((ncols + LASWP_NC - 1) / LASWP_NC);
+  if (tr)
+    laswp_apply_kernel<true><<<grid, 256, 0, st>>>(A, ld, row0, table, c0, n0, c1, n1);
+  else
+    laswp_apply_kernel<false><<<grid, 256, 0, st>>>(A, ld, row0, table, c0, n0, c1, n1);
+  prof_end(ps, st, PROF_SWAP, 0.0);
+  count_launch(2);
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
+}
+
 int laswp_dev(double* A, long ld, int row0, const int* d_piv, int npiv, int c0, int n0, int c1,
               int n1, bool reverse, cudaStream_t st) {
   const int ncols = n0 + n1;
   if (ncols <= 0 || npiv <= 0) return FLA_SUCCESS;
+  if (npiv <= LASWP_MAXP) return laswp_blocked(A, ld, row0, d_piv, npiv, c0, n0, c1, n1, reverse, false, st);
+  const int threads = 128;
   const int ps = prof_begin(st);
-  if (npiv <= LASWP_MAXP) {
-    laswp_block_kernel<false><<<(ncols + LASWP_NC - 1) / LASWP_NC, 256, 0, st>>>(A, ld, row0, d_piv, npiv, c0, n0,
-                                                                          c1, n1, reverse ? 1 : 0);
-  } else {
-    const int threads = 128;
-    laswp_kernel<<<(ncols + threads - 1) / threads, threads, npiv * sizeof(int), st>>>(
-        A, ld, row0, d_piv, npiv, c0, n0, c1, n1, reverse ? 1 : 0);
-  }
+  laswp_kernel<<<(ncols + threads - 1) / threads, threads, npiv * sizeof(int), st>>>(
+      A, ld, row0, d_piv, npiv, c0, n0, c1, n1, reverse ? 1 : 0);
   prof_end(ps, st, PROF_SWAP, 0.0);
   count_launch();
   FB_CK(cudaGetLastError());
   return FLA_SUCCESS;
 }
 
-// Row interchanges on a transposed matrix (see laswp_block_kernel<true>),
-// npiv <= 128 per launch; longer pivot sequences go in chunks of 128.
+// Row interchanges on a transposed matrix (see laswp_apply_kernel<true>),
+// in chunks of at most LASWP_MAXP interchanges.
 int laswp_t_dev(double* AT, long ldt, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
                 cudaStream_t st) {
   const int ncols = n0 + n1;
   if (ncols <= 0 || npiv <= 0) return FLA_SUCCESS;
   for (int i0 = 0; i0 < npiv; i0 += LASWP_MAXP) {
     const int cnt = std::min(LASWP_MAXP, npiv - i0);
-    const int ps = prof_begin(st);
-    laswp_block_kernel<true><<<(ncols + LASWP_NC - 1) / LASWP_NC, 256, 0, st>>>(AT, ldt, row0 + i0, d_piv + i0, cnt,
-                                                                               c0, n0, c1, n1, 0);
-    prof_end(ps, st, PROF_SWAP, 0.0);
-    count_launch();
-    FB_CK(cudaGetLastError());
+    if (laswp_blocked(AT, ldt, row0 + i0, d_piv + i0, cnt, c0, n0, c1, n1, false, true, st) != FLA_SUCCESS)
+      return FLA_FAILURE;
   }
   return FLA_SUCCESS;
 }

@@ -43,7 +43,8 @@ namespace fb {
 
 namespace {
 
-constexpr int LEAF_THREADS = 256;
+constexpr int LEAF_THREADS = 1024;
+constexpr int LEAF_ROWS_TARGET = 256;  // rows per CTA the cluster size aims at
 constexpr int LEAF_MAXC = 16;     // largest cluster
 constexpr int LEAF_MAXW = 128;    // widest leaf
 
@@ -123,13 +124,19 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
     }
     if (lane == 0) { s_rv[warp] = bv; s_ri[warp] = bi; }
     __syncthreads();
-    if (tid == 0) {
-      double v = s_rv[0];
-      int i0 = s_ri[0];
-      for (int q = 1; q < LEAF_THREADS / 32; ++q)
-        if (s_rv[q] > v || (s_rv[q] == v && s_ri[q] < i0)) { v = s_rv[q]; i0 = s_ri[q]; }
-      s_bv = v;
-      s_bi = i0;
+    if (warp == 0) {
+      double v = s_rv[lane];  // LEAF_THREADS / 32 == 32 partial results
+      int i0 = s_ri[lane];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, i0, off);
+        if (ov > v || (ov == v && oi < i0)) { v = ov; i0 = oi; }
+      }
+      if (lane == 0) {
+        s_bv = v;
+        s_bi = i0;
+      }
     }
     __syncthreads();
     // ---- 2. push the candidate (and row j, by its owner) to every CTA
@@ -196,14 +203,32 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
       }
       __syncthreads();
       // ---- 5. scale column j below the pivot (reciprocal multiply, as
-      // bl1_dinvscalv) and apply the rank-1 update to the slab
+      // bl1_dinvscalv), then the rank-1 update of the slab, one element per
+      // thread and pass (rows fastest), four independent elements in flight
       const double rinv = 1.0 / piv;
-      for (int i = tid; i < rows; i += LEAF_THREADS) {
-        if (r0 + i > j) {
-          const double l = slab[i + j * lds] * rinv;
-          slab[i + j * lds] = l;
-          for (int q = j + 1; q < w; ++q) slab[i + q * lds] -= l * u[q];
+      const int i_lo = max(0, j + 1 - r0);  // first local row below the pivot
+      for (int i = i_lo + tid; i < rows; i += LEAF_THREADS) slab[i + j * lds] *= rinv;
+      __syncthreads();
+      const int nrow = rows - i_lo, ncol = w - j - 1;
+      const int total = nrow > 0 ? nrow * ncol : 0;
+      for (int e0 = tid; e0 < total; e0 += 4 * LEAF_THREADS) {
+        int idx[4];
+        double v[4], l[4], uq[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int e = e0 + k * LEAF_THREADS;
+          idx[k] = -1;
+          if (e < total) {
+            const int q = e / nrow, i = i_lo + (e - q * nrow);
+            idx[k] = i + (j + 1 + q) * lds;
+            v[k] = slab[idx[k]];
+            l[k] = slab[i + j * lds];
+            uq[k] = u[j + 1 + q];
+          }
         }
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (idx[k] >= 0) slab[idx[k]] = fma(-l[k], uq[k], v[k]);
       }
     }
     __syncthreads();
@@ -265,9 +290,10 @@ int leaf_setup() {
 // Cluster size and slab geometry for an M x w leaf; false if it does not fit.
 bool leaf_geometry(long M, int w, int* C, int* R, int* lds, size_t* smem) {
   if (w > LEAF_MAXW) return false;
-  // about one row per thread when M is small, the largest cluster otherwise
+  // about LEAF_ROWS_TARGET rows per CTA when M is small, the largest cluster
+  // otherwise
   int cs = 1;
-  while (cs < g_leaf.max_cluster && (M + cs - 1) / cs > LEAF_THREADS) cs <<= 1;
+  while (cs < g_leaf.max_cluster && (M + cs - 1) / cs > LEAF_ROWS_TARGET) cs <<= 1;
   for (; cs <= g_leaf.max_cluster; cs <<= 1) {
     const long r = (M + cs - 1) / cs;
     const int l = (int)(r | 1);

@@ -102,6 +102,60 @@ __global__ void __launch_bounds__(THREADS) trsm_tile_kernel(const double* __rest
   }
 }
 
+// X := inv(T) for a b x b triangular T (b <= 128), one warp per column of X.
+// Column c of inv(T) solves T x = e_c: the warp keeps the running right-hand
+// side in registers (lane l holds rows l, l+32, l+64, l+96), and at each step
+// the owner of the current unknown broadcasts it (multiplied by the
+// reciprocal of the pivot unless UNIT) and every lane updates its rows with
+// one column of T from shared memory.  No block barriers inside the sweep,
+// so the b steps cost only warp-level latency.
+constexpr int INV_WARPS = 16;
+constexpr size_t INV_SMEM = (size_t)(TB * LDT + TB) * sizeof(double);
+template <bool LOWER, bool UNIT>
+__global__ void __launch_bounds__(INV_WARPS * 32) tri_inv_kernel(const double* __restrict__ T, long ldt,
+                                                                 double* __restrict__ X, long ldx, int b) {
+  extern __shared__ double sm[];
+  double* ST = sm;             // stored triangle, ST[r + c*LDT]
+  double* sd = ST + TB * LDT;  // reciprocal diagonal
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int c = warp; c < b; c += INV_WARPS)
+    for (int r = lane; r < b; r += 32)
+      ST[r + c * LDT] = (LOWER ? (r >= c) : (r <= c)) ? T[r + (long)c * ldt] : 0.0;
+  __syncthreads();
+  if (!UNIT)
+    for (int j = tid; j < b; j += INV_WARPS * 32) sd[j] = 1.0 / ST[j + j * LDT];
+  __syncthreads();
+  const int c = blockIdx.x * INV_WARPS + warp;
+  if (c >= b) return;
+  double r[4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) r[m] = (lane + 32 * m == c) ? 1.0 : 0.0;
+  const int j_first = c, j_last = LOWER ? b - 1 : 0;
+  const int nsteps = LOWER ? (b - c) : (c + 1);
+  for (int s = 0; s < nsteps; ++s) {
+    const int j = LOWER ? j_first + s : j_first - s;
+    const int slot = j >> 5;
+    double v = r[0];
+#pragma unroll
+    for (int m = 1; m < 4; ++m)
+      if (slot == m) v = r[m];
+    double xj = __shfl_sync(0xffffffffu, v, j & 31);
+    if (!UNIT) xj *= sd[j];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const int i = lane + 32 * m;
+      if (i == j) r[m] = xj;
+      else if (LOWER ? (i > j && i < b) : (i < j)) r[m] -= ST[i + j * LDT] * xj;
+    }
+  }
+  (void)j_last;
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const int i = lane + 32 * m;
+    if (i < b) X[i + (long)c * ldx] = (LOWER ? i >= c : i <= c) ? r[m] : 0.0;
+  }
+}
+
 template <bool L, bool T, bool U, bool R>
 void set_attr_one() {
   cudaFuncSetAttribute(trsm_tile_kernel<L, T, U, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
@@ -126,6 +180,10 @@ void set_attrs() {
   set_attr_one<false, false, true, true>();
   set_attr_one<false, true, false, true>();
   set_attr_one<false, true, true, true>();
+  cudaFuncSetAttribute(tri_inv_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INV_SMEM);
+  cudaFuncSetAttribute(tri_inv_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INV_SMEM);
+  cudaFuncSetAttribute(tri_inv_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INV_SMEM);
+  cudaFuncSetAttribute(tri_inv_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INV_SMEM);
   g_attr = true;
 }
 
@@ -184,19 +242,7 @@ __global__ void set_identity_kernel(double* X, long ldx, int n) {
 // L X = I (128-row diagonal solves and GEMM updates).  Used to turn the
 // factorizations' panel triangular solves into DMMA GEMMs.
 int tri_inverse_lower(const double* L, long ldl, int b, bool unit, double* X, long ldx, cudaStream_t st) {
-  if (b <= 0) return FLA_SUCCESS;
-  const int blocks = (int)std::min<long>(1024, ((long)b * b + 255) / 256);
-  set_identity_kernel<<<blocks, 256, 0, st>>>(X, ldx, b);
-  count_launch();
-  FB_CK(cudaGetLastError());
-  DMat T, B;
-  T.p = const_cast<double*>(L);
-  T.ld = ldl;
-  T.m = T.n = b;
-  B.p = X;
-  B.ld = ldx;
-  B.m = B.n = b;
-  return trsm_left_dev(T, B, true, false, unit, st);
+  return tri_inverse(L, ldl, b, true, unit, X, ldx, st);
 }
 
 
@@ -224,9 +270,26 @@ int trsm_right_block(const double* T, long ldt, double* X, long ldx, long m, int
   return FLA_SUCCESS;
 }
 
-// X := inv(T) for a b x b triangular T: X := I, then the blocked left solve.
+// X := inv(T) for a b x b triangular T: one warp per column when b <= 128,
+// else X := I and the blocked left solve.
 int tri_inverse(const double* T, long ldt, int b, bool lower, bool unit, double* X, long ldx, cudaStream_t st) {
   if (b <= 0) return FLA_SUCCESS;
+  if (b <= TB) {
+    set_attrs();
+    const unsigned grid = (unsigned)((b + INV_WARPS - 1) / INV_WARPS);
+    const int ps = prof_begin(st);
+    if (lower) {
+      if (unit) tri_inv_kernel<true, true><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, ldx, b);
+      else tri_inv_kernel<true, false><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, ldx, b);
+    } else {
+      if (unit) tri_inv_kernel<false, true><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, ldx, b);
+      else tri_inv_kernel<false, false><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, ldx, b);
+    }
+    prof_end(ps, st, PROF_TRSM, (double)b * b * b / 3.0);
+    count_launch();
+    FB_CK(cudaGetLastError());
+    return FLA_SUCCESS;
+  }
   const int blocks = (int)std::min<long>(1024, ((long)b * b + 255) / 256);
   set_identity_kernel<<<blocks, 256, 0, st>>>(X, ldx, b);
   count_launch();
