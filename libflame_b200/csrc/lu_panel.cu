@@ -92,6 +92,10 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
 
   const int r0 = c * a.R;
   const int rows = max(0, min(a.R, a.M - r0));
+  int rt_log = 5;  // log2 of the slab height rounded up to a power of two (>= 32)
+  while ((1 << rt_log) < rows && rt_log < 10) ++rt_log;
+  const int rt_mask = (1 << rt_log) - 1;
+  const int i_row0 = tid & rt_mask, cg = tid >> rt_log, cgs = LEAF_THREADS >> rt_log;
   if (RM) {
     for (int e = tid; e < rows * w; e += LEAF_THREADS) {
       const int i = e / w, col = e - i * w;
@@ -209,26 +213,23 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
       const int i_lo = max(0, j + 1 - r0);  // first local row below the pivot
       for (int i = i_lo + tid; i < rows; i += LEAF_THREADS) slab[i + j * lds] *= rinv;
       __syncthreads();
-      const int nrow = rows - i_lo, ncol = w - j - 1;
-      const int total = nrow > 0 ? nrow * ncol : 0;
-      for (int e0 = tid; e0 < total; e0 += 4 * LEAF_THREADS) {
-        int idx[4];
-        double v[4], l[4], uq[4];
+      // thread -> (row i = tid mod RT, column group cg = tid / RT); RT is the
+      // slab height rounded up to a power of two, so no divisions
+      for (int i_row = i_row0 + max(0, ((i_lo - i_row0) + rt_mask) >> rt_log << rt_log); i_row < rows;
+           i_row += rt_mask + 1) {
+        const double l = slab[i_row + j * lds];
+        int q = j + 1 + cg;
+        for (; q + 3 * cgs < w; q += 4 * cgs) {
+          double v[4], uq[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const int e = e0 + k * LEAF_THREADS;
-          idx[k] = -1;
-          if (e < total) {
-            const int q = e / nrow, i = i_lo + (e - q * nrow);
-            idx[k] = i + (j + 1 + q) * lds;
-            v[k] = slab[idx[k]];
-            l[k] = slab[i + j * lds];
-            uq[k] = u[j + 1 + q];
+          for (int k = 0; k < 4; ++k) {
+            v[k] = slab[i_row + (q + k * cgs) * lds];
+            uq[k] = u[q + k * cgs];
           }
-        }
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
-          if (idx[k] >= 0) slab[idx[k]] = fma(-l[k], uq[k], v[k]);
+          for (int k = 0; k < 4; ++k) slab[i_row + (q + k * cgs) * lds] = fma(-l, uq[k], v[k]);
+        }
+        for (; q < w; q += cgs) slab[i_row + q * lds] = fma(-l, u[q], slab[i_row + q * lds]);
       }
     }
     __syncthreads();
