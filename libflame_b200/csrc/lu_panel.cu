@@ -12,14 +12,14 @@
 //
 // Leaf (lu_leaf_cluster_kernel): the M x w leaf is split in row slabs, one
 // per CTA of a cluster of up to 16 CTAs, each slab held in shared memory for
-// the whole leaf.  Per column j: every CTA pushes its best candidate row
-// (magnitude, row, the whole w-wide row) and, if it owns it, the current row
-// j into every CTA's shared memory (DSMEM stores); one hardware cluster
-// barrier; every warp picks the same winner from the local copies; then one
-// pass over (row, column group) exchanges rows j and p(j), scales column j
-// below the pivot, applies the rank-1 update and finds the candidates of
-// column j + 1; one block barrier.  Exchange buffers alternate between two
-// halves by column parity, so these two barriers per column suffice.  Cluster CTAs are co-scheduled by the
+// the whole leaf.  Per column: every CTA finds its best candidate row and
+// pushes the candidate (magnitude, row, the whole w-wide row) and, if it owns
+// it, the current row j into every CTA's shared memory (DSMEM stores); one
+// hardware cluster barrier; then every CTA picks the same winner from its
+// local copy, the owners of rows j and p(j) exchange them, and each CTA
+// scales its part of column j and applies the rank-1 update to its slab.
+// Exchange buffers alternate between two halves by column parity, so one
+// barrier per column suffices.  Cluster CTAs are co-scheduled by the
 // hardware, so the leaf can run on a second stream beside the trailing
 // update without any co-residency assumption, and the barrier is not a spin.
 //
@@ -45,7 +45,6 @@ namespace {
 
 constexpr int LEAF_THREADS = 1024;
 constexpr int LEAF_ROWS_TARGET = 256;  // rows per CTA the cluster size aims at
-constexpr int LEAF_RAWN = 4;           // rows per thread: slabs of up to 4096 rows
 constexpr int LEAF_MAXC = 16;     // largest cluster
 constexpr int LEAF_MAXW = 128;    // widest leaf
 
@@ -78,6 +77,8 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
   extern __shared__ double S[];
   __shared__ double s_rv[LEAF_THREADS / 32];
   __shared__ int s_ri[LEAF_THREADS / 32];
+  __shared__ double s_bv;
+  __shared__ int s_bi, s_wc, s_r;
   cg::cluster_group cluster = cg::this_cluster();
   const int C = (int)cluster.num_blocks();
   const int c = (int)cluster.block_rank();
@@ -96,9 +97,26 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
   const int rt_mask = (1 << rt_log) - 1;
   const int i_row0 = tid & rt_mask, cg = tid >> rt_log, cgs = LEAF_THREADS >> rt_log;
   if (RM) {
-    for (int e = tid; e < rows * w; e += LEAF_THREADS) {
-      const int i = e / w, col = e - i * w;
-      slab[i + col * lds] = a.P[(long)(r0 + i) * a.ld + col];
+    // eight independent loads in flight per thread
+    const int tot = rows * w;
+    for (int e0 = tid; e0 < tot; e0 += 8 * LEAF_THREADS) {
+      double v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int e = e0 + k * LEAF_THREADS;
+        if (e < tot) {
+          const int i = e / w, col = e - i * w;
+          v[k] = a.P[(long)(r0 + i) * a.ld + col];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int e = e0 + k * LEAF_THREADS;
+        if (e < tot) {
+          const int i = e / w, col = e - i * w;
+          slab[i + col * lds] = v[k];
+        }
+      }
     }
   } else {
     for (int col = 0; col < w; ++col)
@@ -106,34 +124,19 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
   }
   __syncthreads();
 
-  // Thread -> (row i_row0 + k * RT, column group cg): RT is the slab height
-  // rounded up to a power of two (at most 1024), the cgs = 1024 / RT groups
-  // take columns cg, cg + cgs, ...  raw[k] holds the current value of the
-  // pivot column in the thread's rows, read before the cluster barrier, so
-  // that the column can be overwritten with the multipliers in the same pass
-  // that the other column groups read it.
-  const int RT = rt_mask + 1;
-  double raw[LEAF_RAWN];
-  auto read_raw = [&](int col) {
-#pragma unroll
-    for (int k = 0; k < LEAF_RAWN; ++k) {
-      const int i = i_row0 + k * RT;
-      raw[k] = (i < rows && col < w) ? slab[i + col * lds] : 0.0;
+  int first_null = -1;
+  for (int j = 0; j < w; ++j) {
+    const int par = j & 1;
+    // ---- 1. local candidate: max |a(i,j)| over rows i >= j, smallest row on ties
+    double bv = -1.0;
+    int bi = INT_MAX;
+    for (int i = tid; i < rows; i += LEAF_THREADS) {
+      const int gi = r0 + i;
+      if (gi >= j) {
+        const double v = fabs(slab[i + j * lds]);
+        if (v > bv || (v == bv && gi < bi)) { bv = v; bi = gi; }
+      }
     }
-  };
-  // Block-wide best candidate from per-warp partials; every warp reduces
-  // the same 32 partials in the same order, so all agree without a barrier.
-  auto reduce_partials = [&](double& bv, int& bi) {
-    bv = s_rv[lane];
-    bi = s_ri[lane];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
-    }
-  };
-  auto warp_partial = [&](double bv, int bi) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
       const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
@@ -141,58 +144,53 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
       if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
     }
     if (lane == 0) { s_rv[warp] = bv; s_ri[warp] = bi; }
-  };
-
-  // candidate of column 0
-  {
-    double bv = -1.0;
-    int bi = INT_MAX;
-    for (int i = tid; i < rows; i += LEAF_THREADS) {
-      const double v = fabs(slab[i]);
-      if (v > bv || (v == bv && r0 + i < bi)) { bv = v; bi = r0 + i; }
+    __syncthreads();
+    if (warp == 0) {
+      double v = s_rv[lane];  // LEAF_THREADS / 32 == 32 partial results
+      int i0 = s_ri[lane];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, i0, off);
+        if (ov > v || (ov == v && oi < i0)) { v = ov; i0 = oi; }
+      }
+      if (lane == 0) {
+        s_bv = v;
+        s_bi = i0;
+      }
     }
-    warp_partial(bv, bi);
-  }
-  read_raw(0);
-  __syncthreads();
-
-  int first_null = -1;
-  for (int j = 0; j < w; ++j) {
-    const int par = j & 1;
-    double cbv;
-    int cbi;
-    reduce_partials(cbv, cbi);
-    // ---- push the candidate (magnitude, row, its whole leaf row) and, by
-    // its owner, row j to every CTA of the cluster
+    __syncthreads();
+    // ---- 2. push the candidate (and row j, by its owner) to every CTA
     {
-      const int li = cbi - r0;
-      const bool have = cbi != INT_MAX;
+      const int li = s_bi - r0;  // local row of the candidate (if any)
+      const bool have = s_bi != INT_MAX;
+      const bool own_j = (j >= r0) && (j < r0 + rows);
       const int per = w + 1;
       for (int e = tid; e < C * per; e += LEAF_THREADS) {
         const int d = e / per, q = e - d * per;
         if (q < w) {
-          *cluster.map_shared_rank(xrow + ((size_t)par * C + c) * w + q, d) = have ? slab[li + q * lds] : 0.0;
+          double* dst = cluster.map_shared_rank(xrow + ((size_t)par * C + c) * w + q, d);
+          *dst = have ? slab[li + q * lds] : 0.0;
         } else {
-          *cluster.map_shared_rank(xval + par * C + c, d) = cbv;
-          *cluster.map_shared_rank(xidx + par * C + c, d) = cbi;
+          *cluster.map_shared_rank(xval + par * C + c, d) = s_bv;
+          *cluster.map_shared_rank(xidx + par * C + c, d) = s_bi;
         }
       }
-      if (j >= r0 && j < r0 + rows)
+      if (own_j)
         for (int e = tid; e < C * w; e += LEAF_THREADS) {
           const int d = e / w, q = e - d * w;
           *cluster.map_shared_rank(rowj + par * w + q, d) = slab[(j - r0) + q * lds];
         }
     }
     cluster.sync();
-    // ---- winner: every warp reads the C candidates (lane q < C) and reduces
-    int r, wc;
-    {
+    // ---- 3. winner (identical on every CTA: same data, same order)
+    if (warp == 0) {
       double v = -2.0;
       int i0 = INT_MAX, w0 = 0;
-      if (lane < C) {
-        const double cv = xval[par * C + lane];
-        const int ci = xidx[par * C + lane];
-        if (ci != INT_MAX) { v = cv; i0 = ci; w0 = lane; }
+      for (int q = lane; q < C; q += 32) {
+        const double cv = xval[par * C + q];
+        const int ci = xidx[par * C + q];
+        if (ci != INT_MAX && (cv > v || (cv == v && ci < i0))) { v = cv; i0 = ci; w0 = q; }
       }
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
@@ -201,73 +199,58 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
         const int ow = __shfl_xor_sync(0xffffffffu, w0, off);
         if (ov > v || (ov == v && oi < i0)) { v = ov; i0 = oi; w0 = ow; }
       }
-      r = i0;
-      wc = w0;
+      if (lane == 0) { s_wc = w0; s_r = i0; }
     }
-    const double* u = xrow + ((size_t)par * C + wc) * w;  // the pivot row
-    const double* rj = rowj + par * w;                     // row j before the exchange
+    __syncthreads();
+    int r = s_r;
+    const double* u = xrow + ((size_t)par * C + s_wc) * w;  // the pivot row
     if (r == INT_MAX) {
       // no orderable candidate (every magnitude NaN): keep row j, as idamax
       // does when no later entry compares greater than the first
       r = j;
-      u = rj;
+      u = rowj + par * w;
     }
     const double piv = u[j];
     if (c == 0 && tid == 0) a.piv[j] = r - j;
-    // ---- exchange rows j and r, scale column j below the pivot (reciprocal
-    // multiply, as bl1_dinvscalv), rank-1 update, and the candidates of
-    // column j + 1, in one pass over (row, column group)
-    const bool zero = (piv == 0.0);
-    if (zero && first_null < 0) first_null = j;
-    const double rinv = zero ? 0.0 : 1.0 / piv;
-    const int nj = j + 1;
-    const bool track = (nj < w) && (cg == nj % cgs);
-    double bv = -1.0;
-    int bi = INT_MAX;
-#pragma unroll
-    for (int k = 0; k < LEAF_RAWN; ++k) {
-      const int i = i_row0 + k * RT;
-      if (i >= rows) break;
-      const int gi = r0 + i;
-      if (!zero && gi >= j) {
-        if (gi == j) {
-          if (r != j)  // row j becomes the pivot row
-            for (int q = cg; q < w; q += cgs) slab[i + q * lds] = u[q];
-        } else if (gi == r) {  // row r receives row j, then is updated
-          const double l = rj[j] * rinv;
-          for (int q = cg; q < w; q += cgs)
-            slab[i + q * lds] = (q < j) ? rj[q] : (q == j ? l : fma(-l, u[q], rj[q]));
-        } else {
-          const double l = raw[k] * rinv;
-          int q = j + ((cg - j % cgs + cgs) % cgs);  // first column >= j of this group
-          if (q == j) {
-            slab[i + q * lds] = l;
-            q += cgs;
-          }
-          for (; q + 3 * cgs < w; q += 4 * cgs) {
-            double v[4], uq[4];
-#pragma unroll
-            for (int t = 0; t < 4; ++t) {
-              v[t] = slab[i + (q + t * cgs) * lds];
-              uq[t] = u[q + t * cgs];
-            }
-#pragma unroll
-            for (int t = 0; t < 4; ++t) slab[i + (q + t * cgs) * lds] = fma(-l, uq[t], v[t]);
-          }
-          for (; q < w; q += cgs) slab[i + q * lds] = fma(-l, u[q], slab[i + q * lds]);
-        }
+    if (piv == 0.0) {
+      if (first_null < 0) first_null = j;
+    } else {
+      if (r != j) {
+        // ---- 4. exchange rows j and r (whole leaf row)
+        if (j >= r0 && j < r0 + rows)
+          for (int q = tid; q < w; q += LEAF_THREADS) slab[(j - r0) + q * lds] = u[q];
+        if (r >= r0 && r < r0 + rows)
+          for (int q = tid; q < w; q += LEAF_THREADS) slab[(r - r0) + q * lds] = rowj[par * w + q];
       }
-      if (track && gi >= nj) {
-        // value of column j + 1 after this step (this thread wrote it)
-        const double v = fabs(slab[i + nj * lds]);
-        if (v > bv || (v == bv && gi < bi)) { bv = v; bi = gi; }
+      __syncthreads();
+      // ---- 5. scale column j below the pivot (reciprocal multiply, as
+      // bl1_dinvscalv), then the rank-1 update of the slab, one element per
+      // thread and pass (rows fastest), four independent elements in flight
+      const double rinv = 1.0 / piv;
+      const int i_lo = max(0, j + 1 - r0);  // first local row below the pivot
+      for (int i = i_lo + tid; i < rows; i += LEAF_THREADS) slab[i + j * lds] *= rinv;
+      __syncthreads();
+      // thread -> (row i = tid mod RT, column group cg = tid / RT); RT is the
+      // slab height rounded up to a power of two, so no divisions
+      for (int i_row = i_row0 + max(0, ((i_lo - i_row0) + rt_mask) >> rt_log << rt_log); i_row < rows;
+           i_row += rt_mask + 1) {
+        const double l = slab[i_row + j * lds];
+        int q = j + 1 + cg;
+        for (; q + 3 * cgs < w; q += 4 * cgs) {
+          double v[4], uq[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            v[k] = slab[i_row + (q + k * cgs) * lds];
+            uq[k] = u[q + k * cgs];
+          }
+#pragma unroll
+          for (int k = 0; k < 4; ++k) slab[i_row + (q + k * cgs) * lds] = fma(-l, uq[k], v[k]);
+        }
+        for (; q < w; q += cgs) slab[i_row + q * lds] = fma(-l, u[q], slab[i_row + q * lds]);
       }
     }
-    warp_partial(bv, bi);
     __syncthreads();
-    read_raw(nj);
   }
-
   if (RM) {
     for (int e = tid; e < rows * w; e += LEAF_THREADS) {
       const int i = e / w, col = e - i * w;
@@ -323,15 +306,29 @@ int leaf_setup() {
 }
 
 // Cluster size and slab geometry for an M x w leaf; false if it does not fit.
+// Widest leaf: the leaf's rank-1 updates re-read the whole slab every
+// column, so wide leaves are split and their halves joined by DMMA GEMMs;
+// FLA_B200_LU_LEAF_MAXW (8..128) overrides the default for tuning.
+int leaf_maxw() {
+  static int mw = 0;
+  if (mw == 0) {
+    mw = 64;
+    if (const char* e = std::getenv("FLA_B200_LU_LEAF_MAXW")) {
+      const int v = std::atoi(e);
+      if (v >= 8 && v <= LEAF_MAXW) mw = v;
+    }
+  }
+  return mw;
+}
+
 bool leaf_geometry(long M, int w, int* C, int* R, int* lds, size_t* smem) {
-  if (w > LEAF_MAXW) return false;
+  if (w > leaf_maxw()) return false;
   // about LEAF_ROWS_TARGET rows per CTA when M is small, the largest cluster
   // otherwise
   int cs = 1;
   while (cs < g_leaf.max_cluster && (M + cs - 1) / cs > LEAF_ROWS_TARGET) cs <<= 1;
   for (; cs <= g_leaf.max_cluster; cs <<= 1) {
     const long r = (M + cs - 1) / cs;
-    if (r > (long)LEAF_RAWN * 1024) continue;  // rows per thread of the kernel
     const int l = (int)(r | 1);
     const size_t need = leaf_smem_bytes(l, w, cs);
     if (need <= g_leaf.smem_cap) {
