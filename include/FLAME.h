@@ -250,6 +250,14 @@ int dgetrs_( char* trans, int* n, int* nrhs, double* a, int* lda, int* ipiv, dou
 /* src/map/common/lapacksrc/f2c/dposv.c:120-190, dgesv.c:113-175 */
 int dposv_( char* uplo, int* n, int* nrhs, double* a, int* lda, double* b, int* ldb, int* info );
 int dgesv_( int* n, int* nrhs, double* a, int* lda, int* ipiv, double* b, int* ldb, int* info );
+/* src/map/common/lapacksrc/f2c/dsgesv.c:189-412, dsposv.c:250-413: mixed
+ * precision with FP64 refinement; iter >= 0 refinement steps, -3 / -31 when
+ * the FP64 factorization took over (A then holds its factors).  work and
+ * swork are accepted and not referenced. */
+int dsgesv_( int* n, int* nrhs, double* a, int* lda, int* ipiv, double* b, int* ldb, double* x, int* ldx,
+             double* work, float* swork, int* iter, int* info );
+int dsposv_( char* uplo, int* n, int* nrhs, double* a, int* lda, double* b, int* ldb, double* x, int* ldx,
+             double* work, float* swork, int* iter, int* info );
 
 #ifdef __cplusplus
 }

@@ -58,6 +58,33 @@ int           FLA_B200_dgemm( int transa, int transb, long m, long n, long k, do
 int           FLA_B200_LU_piv_panel_noalloc( int m, int n, double* A, int lda, int* piv,
                                              void* stream );
 
+/* ---- Mixed precision (no counterpart in the reference beyond dsgesv_ /
+ * dsposv_, whose conventions they follow) ----
+ * X := A^-1 B for a square FLA_DOUBLE A (device or host buffers): the
+ * factorization runs in low precision (FP32 storage, 16-bit tensor-core
+ * trailing updates with FP32 accumulation, panels in FP64) and FP64
+ * iterative refinement restores FP64 accuracy; A is left unchanged.
+ * prec: 0 BF16, 1 FP16 with power-of-two equilibration, -1 the library
+ * default (FLA_B200_IR_PREC, else FP16).  solver: 0 classic refinement
+ * (dsgesv_'s), 1 GMRES-IR (GMRES in FP64 preconditioned by the
+ * low-precision factors, for ill-conditioned A), -1 the default
+ * (FLA_B200_IR_SOLVER, else GMRES-IR).  iter (optional) receives the
+ * number of refinement steps, or -3 (low-precision factorization failed)
+ * / -31 (no convergence in 30 steps) when the FP64 factorization of a copy
+ * produced X; inner (optional) the GMRES iterations.  Returns FLA_SUCCESS,
+ * the zero-based failing column of the FP64 fallback, or FLA_FAILURE. */
+FLA_Error     FLA_B200_LU_piv_solve_mixed( FLA_Obj A, FLA_Obj B, FLA_Obj X, int prec, int solver,
+                                           int* iter, int* inner );
+FLA_Error     FLA_B200_Chol_solve_mixed( FLA_Uplo uplo, FLA_Obj A, FLA_Obj B, FLA_Obj X, int prec,
+                                         int solver, int* iter, int* inner );
+
+/* The 16-bit tensor-core GEMM of the mixed-precision factorizations on
+ * device buffers: C (FP32, column-major) := alpha A B^T + beta C, A m x k
+ * and B n x k FP32 column-major, rounded to prec (0 BF16, 1 FP16),
+ * accumulated in FP32. */
+int           FLA_B200_lp_gemm( int prec, long m, long n, long k, float alpha, const float* A, long lda,
+                                const float* B, long ldb, float beta, float* C, long ldc );
+
 #ifdef __cplusplus
 }
 #endif

@@ -74,6 +74,12 @@ _SIGS = {
     "FLA_B200_dgemm": (C.c_int, [C.c_int, C.c_int, C.c_long, C.c_long, C.c_long, C.c_double,
                                  C.c_void_p, C.c_long, C.c_void_p, C.c_long, C.c_double,
                                  C.c_void_p, C.c_long, C.c_int]),
+    "FLA_B200_LU_piv_solve_mixed": (C.c_int, [FLA_Obj, FLA_Obj, FLA_Obj, C.c_int, C.c_int,
+                                              C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "FLA_B200_Chol_solve_mixed": (C.c_int, [C.c_int, FLA_Obj, FLA_Obj, FLA_Obj, C.c_int, C.c_int,
+                                            C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "FLA_B200_lp_gemm": (C.c_int, [C.c_int, C.c_long, C.c_long, C.c_long, C.c_float, C.c_void_p, C.c_long,
+                                   C.c_void_p, C.c_long, C.c_float, C.c_void_p, C.c_long]),
 }
 
 _OPTIONAL = set()
@@ -234,3 +240,20 @@ def qr_ut_recover_tau(T, t):
 def shift_pivots_to(ptype, p):
     vp = View(p)
     return lib().FLA_Shift_pivots_to(ptype, vp.obj)
+
+
+def lu_piv_solve_mixed(A, B, X, prec=-1, solver=-1):
+    """X := A^-1 B, low-precision LU + FP64 refinement (A unchanged).
+    Returns (FLA error code, refinement steps, GMRES iterations)."""
+    vA, vB, vX = View(A), View(B), View(X)
+    it, inner = C.c_int(0), C.c_int(0)
+    r = lib().FLA_B200_LU_piv_solve_mixed(vA.obj, vB.obj, vX.obj, prec, solver, C.byref(it), C.byref(inner))
+    return r, it.value, inner.value
+
+
+def chol_solve_mixed(A, B, X, uplo=FLA_LOWER_TRIANGULAR, prec=-1, solver=-1):
+    """X := A^-1 B for SPD A, low-precision Cholesky + FP64 refinement."""
+    vA, vB, vX = View(A), View(B), View(X)
+    it, inner = C.c_int(0), C.c_int(0)
+    r = lib().FLA_B200_Chol_solve_mixed(uplo, vA.obj, vB.obj, vX.obj, prec, solver, C.byref(it), C.byref(inner))
+    return r, it.value, inner.value

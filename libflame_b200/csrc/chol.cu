@@ -190,6 +190,18 @@ int chol_lower_enqueue(DMat A, cudaStream_t st) {
   return FLA_SUCCESS;
 }
 
+// Factor one b x b (b <= 128) lower diagonal block in place (FP64); gcol is
+// the global index of its first column for the info word.
+int potrf_diag_dev(double* A, long ld, int b, int gcol, cudaStream_t st) {
+  set_attrs();
+  int ps = prof_begin(st);
+  potrf_diag_kernel<<<1, POTRF_THREADS, POTRF_SMEM, st>>>(A, ld, b, gcol, ctx().d_status + ST_INFO);
+  prof_end(ps, st, PROF_DIAG, (double)b * b * b / 3.0);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
+}
+
 int chol_lower_dev(DMat A, int* info) {
   if (A.m == 0) {
     *info = -1;

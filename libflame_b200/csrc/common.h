@@ -50,6 +50,7 @@ inline void count_launch(unsigned n = 1) { ctx().launches += n; }
 enum ProfClass : int { PROF_GEMM = 0, PROF_PANEL, PROF_TRSM, PROF_SWAP, PROF_DIAG, PROF_OTHER, PROF_NCLASS };
 void op_begin(cudaStream_t st);
 void op_end(cudaStream_t st);
+void op_hold(bool on);  // keep the current op window open across nested drivers
 bool prof_on();
 int prof_begin(cudaStream_t st);                       // returns a slot or -1
 void prof_end(int slot, cudaStream_t st, int cls, double flops);
@@ -86,6 +87,16 @@ enum WsSlot : int {
   WS_REPACK,        // aligned repack of an operand
   WS_MISC,
   WS_MISC2,
+  WS_LP0,           // mixed-precision solvers: low-precision factor
+  WS_LP1,           //   packed 16-bit operands
+  WS_LP2,
+  WS_LP3,           //   FP64 panel / inverses
+  WS_LP4,           //   inverse blocks kept for the correction solves
+  WS_IR0,           //   refinement vectors (FP64 / FP32)
+  WS_IR1,
+  WS_IR2,
+  WS_STAGE_X,       // staging of a third operand (solution X)
+  WS_FB,            // FP64 copy for the fallback factorization / symmetric residual
   WS_NSLOTS
 };
 void* ws_get(int slot, size_t bytes);  // nullptr on allocation failure
@@ -206,6 +217,10 @@ int transpose_dev(const double* src, long lds, double* dst, long ldd, long m, lo
 // order, over the A-columns [c0, c0+n0) and [c1, c1+n1) (rows of AT).
 int laswp_t_dev(double* AT, long ldt, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
                 cudaStream_t st);
+int laswp_t_f32(float* AT, long ldt, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
+                cudaStream_t st);
+// Cholesky of one b x b (b <= 128) lower diagonal block in place (FP64).
+int potrf_diag_dev(double* A, long ld, int b, int gcol, cudaStream_t st);
 // LU panel on the transposed matrix: the M x w panel of A whose element
 // (i, j) is at P[i * ld + j] (rows of A are the columns of AT).
 int lu_panel_factor_t(double* P, long ld, long M, int w, int* d_piv, int gcol, cudaStream_t st);

@@ -239,12 +239,12 @@ __global__ void __launch_bounds__(256) laswp_compose_kernel(const int* __restric
   }
 }
 
-template <bool TR>
-__global__ void __launch_bounds__(256) laswp_apply_kernel(double* A, long ld, int row0, const int* __restrict__ table,
+template <typename T, bool TR>
+__global__ void __launch_bounds__(256) laswp_apply_kernel(T* A, long ld, int row0, const int* __restrict__ table,
                                                           int c0, int n0, int c1, int n1) {
   __shared__ int s_row[2 * LASWP_MAXP];
   __shared__ int s_src[2 * LASWP_MAXP];
-  __shared__ double s_val[LASWP_NC][2 * LASWP_MAXP + 1];
+  __shared__ T s_val[LASWP_NC][2 * LASWP_MAXP + 1];
   const int tid = threadIdx.x;
   const int nslot = table[0];
   for (int s = tid; s < nslot; s += blockDim.x) {
@@ -343,7 +343,8 @@ int* laswp_table(cudaStream_t st) {
   return base + (st == ctx().side ? LASWP_TABLE_INTS : 0);
 }
 
-int laswp_blocked(double* A, long ld, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
+template <typename T>
+int laswp_blocked(T* A, long ld, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
                   bool reverse, bool tr, cudaStream_t st) {
   const int ncols = n0 + n1;
   int* table = laswp_table(st);
@@ -352,9 +353,9 @@ int laswp_blocked(double* A, long ld, int row0, const int* d_piv, int npiv, int 
   laswp_compose_kernel<<<1, 256, 0, st>>>(d_piv, npiv, reverse ? 1 : 0, table);
   const unsigned grid = (unsigned)((ncols + LASWP_NC - 1) / LASWP_NC);
   if (tr)
-    laswp_apply_kernel<true><<<grid, 256, 0, st>>>(A, ld, row0, table, c0, n0, c1, n1);
+    laswp_apply_kernel<T, true><<<grid, 256, 0, st>>>(A, ld, row0, table, c0, n0, c1, n1);
   else
-    laswp_apply_kernel<false><<<grid, 256, 0, st>>>(A, ld, row0, table, c0, n0, c1, n1);
+    laswp_apply_kernel<T, false><<<grid, 256, 0, st>>>(A, ld, row0, table, c0, n0, c1, n1);
   prof_end(ps, st, PROF_SWAP, 0.0);
   count_launch(2);
   FB_CK(cudaGetLastError());
@@ -365,7 +366,7 @@ int laswp_dev(double* A, long ld, int row0, const int* d_piv, int npiv, int c0, 
               int n1, bool reverse, cudaStream_t st) {
   const int ncols = n0 + n1;
   if (ncols <= 0 || npiv <= 0) return FLA_SUCCESS;
-  if (npiv <= LASWP_MAXP) return laswp_blocked(A, ld, row0, d_piv, npiv, c0, n0, c1, n1, reverse, false, st);
+  if (npiv <= LASWP_MAXP) return laswp_blocked<double>(A, ld, row0, d_piv, npiv, c0, n0, c1, n1, reverse, false, st);
   const int threads = 128;
   const int ps = prof_begin(st);
   laswp_kernel<<<(ncols + threads - 1) / threads, threads, npiv * sizeof(int), st>>>(
@@ -376,18 +377,27 @@ int laswp_dev(double* A, long ld, int row0, const int* d_piv, int npiv, int c0, 
   return FLA_SUCCESS;
 }
 
-// Row interchanges on a transposed matrix (see laswp_apply_kernel<true>),
+// Row interchanges on a transposed matrix (see laswp_apply_kernel<T, true>),
 // in chunks of at most LASWP_MAXP interchanges.
-int laswp_t_dev(double* AT, long ldt, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
+template <typename T>
+int laswp_t_any(T* AT, long ldt, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
                 cudaStream_t st) {
   const int ncols = n0 + n1;
   if (ncols <= 0 || npiv <= 0) return FLA_SUCCESS;
   for (int i0 = 0; i0 < npiv; i0 += LASWP_MAXP) {
     const int cnt = std::min(LASWP_MAXP, npiv - i0);
-    if (laswp_blocked(AT, ldt, row0 + i0, d_piv + i0, cnt, c0, n0, c1, n1, false, true, st) != FLA_SUCCESS)
+    if (laswp_blocked<T>(AT, ldt, row0 + i0, d_piv + i0, cnt, c0, n0, c1, n1, false, true, st) != FLA_SUCCESS)
       return FLA_FAILURE;
   }
   return FLA_SUCCESS;
+}
+int laswp_t_dev(double* AT, long ldt, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
+                cudaStream_t st) {
+  return laswp_t_any<double>(AT, ldt, row0, d_piv, npiv, c0, n0, c1, n1, st);
+}
+int laswp_t_f32(float* AT, long ldt, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
+                cudaStream_t st) {
+  return laswp_t_any<float>(AT, ldt, row0, d_piv, npiv, c0, n0, c1, n1, st);
 }
 
 int apply_pivots_dev(DMat A, const int* d_piv, int k1, int k2, bool reverse, cudaStream_t st) {

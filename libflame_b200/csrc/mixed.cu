@@ -1,0 +1,761 @@
+// Mixed-precision solvers: factor in low precision on the tensor cores,
+// refine in FP64.
+//
+// Reference behaviour: dsgesv_ / dsposv_ (src/map/common/lapacksrc/f2c/
+// dsgesv.c:189-412, dsposv.c:250-413): factor a single-precision copy,
+// x = solve(b), then up to ITERMAX = 30 refinement steps r = b - A x (FP64),
+// x += solve(r), stopping when every column has ||r||_inf <= ||x||_inf * cte
+// with cte = ||A||_inf * eps * sqrt(n) (eps = DBL_EPSILON / 2, dlamch 'E');
+// on failure fall back to the FP64 factorization (iter = -2 overflow, -3
+// factorization failure, -31 no convergence).
+//
+// B200 form:
+//   * the working copy of A is FP32; the panels are factored in FP64 by the
+//     same kernels as the plain FP64 path (cluster LU leaves, diagonal-block
+//     Cholesky) and rounded back, while every trailing update and panel
+//     solve is a 16-bit (BF16 or FP16) tensor-core GEMM with FP32
+//     accumulation (lp_gemm.cu), with the same one-panel lookahead on a
+//     second stream;
+//   * optional power-of-two equilibration (rows and columns for LU, the
+//     symmetric diag(a_ii)^-1/2 for Cholesky) keeps the 16-bit operands in
+//     range (required for FP16);
+//   * the correction solves run in FP32 with the inverted diagonal blocks
+//     formed during the factorization (two GEMMs per block);
+//   * FP64 is used only for r = b - A x (DMMA GEMM), the update of x and the
+//     norms;
+//   * GMRES-IR: the correction equation A d = r is solved by GMRES(m) left-
+//     preconditioned with the low-precision factors, in FP64, all right-hand
+//     sides in lockstep (one GEMM per matrix-vector product), which carries
+//     the refinement to condition numbers beyond 1/u of the factorization.
+#include <algorithm>
+#include <cfloat>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.h"
+#include "lowprec.h"
+#include "mixed.h"
+
+namespace fb {
+
+namespace {
+
+constexpr int MB = 128;  // block size of the low-precision factorizations
+
+// AT[j + i * ldt] = (float)(A[i + j * lda] * sr[i] * sc[j])   (A m x n)
+__global__ void transpose_scale_kernel(const double* __restrict__ A, long lda, float* __restrict__ AT, long ldt,
+                                       int m, int n, const double* __restrict__ sr, const double* __restrict__ sc) {
+  __shared__ float tile[32][33];
+  const int bi = blockIdx.x * 32, bj = blockIdx.y * 32;
+  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+    const int i = bi + threadIdx.x, j = bj + y;
+    float v = 0.f;
+    if (i < m && j < n) {
+      double a = A[i + (long)j * lda];
+      if (sr) a *= sr[i];
+      if (sc) a *= sc[j];
+      v = (float)a;
+    }
+    tile[y][threadIdx.x] = v;
+  }
+  __syncthreads();
+  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+    const int j = bj + threadIdx.x, i = bi + y;
+    if (i < m && j < n) AT[j + (long)i * ldt] = tile[threadIdx.x][y];
+  }
+}
+
+// F[i + j * ldf] = (float)(a(i, j) * d[i] * d[j]) for i >= j, a(i, j) from the
+// stored triangle (upper: a(i, j) = A[j + i * lda]).
+__global__ void lower_scale_kernel(const double* __restrict__ A, long lda, float* __restrict__ F, long ldf, int n,
+                                   const double* __restrict__ d, int upper) {
+  const long total = (long)n * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long i = e % n, j = e / n;
+    if (i < j) continue;
+    double a = upper ? A[j + i * lda] : A[i + j * lda];
+    if (d) a *= d[i] * d[j];
+    F[i + j * ldf] = (float)a;
+  }
+}
+
+// Full symmetric copy S from the stored triangle of A.
+__global__ void symmetrize_kernel(const double* __restrict__ A, long lda, double* __restrict__ S, long lds, int n,
+                                  int upper) {
+  const long total = (long)n * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long i = e % n, j = e / n;
+    const bool stored = upper ? (i <= j) : (i >= j);
+    S[i + j * lds] = stored ? A[i + j * lda] : A[j + i * lda];
+  }
+}
+
+// out[i] = max_j |A(i, j)| * (cs ? cs[j] : 1), one thread per row (the warp
+// reads 32 consecutive rows of a column: coalesced).
+__global__ void row_absmax_kernel(const double* __restrict__ A, long lda, int m, int n, const double* __restrict__ cs,
+                                  double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double v = 0.0;
+  for (int j = 0; j < n; ++j) v = fmax(v, fabs(A[i + (long)j * lda]) * (cs ? cs[j] : 1.0));
+  out[i] = v;
+}
+// out[j] = max_i |A(i, j)| * rs[i], one block per column.
+__global__ void col_absmax_kernel(const double* __restrict__ A, long lda, int m, const double* __restrict__ rs,
+                                  double* __restrict__ out) {
+  __shared__ double red[256];
+  const int j = blockIdx.x;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) v = fmax(v, fabs(A[i + (long)j * lda]) * (rs ? rs[i] : 1.0));
+  red[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[j] = red[0];
+}
+// v[i] := 2^-e with v[i] = f 2^e, f in [0.5, 1): an exact power-of-two
+// reciprocal (1 where v[i] is 0 or not finite).
+__global__ void pow2_recip_kernel(double* v, int n, int sqrt_of) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double x = v[i];
+  if (!(x > 0.0) || !isfinite(x)) {
+    v[i] = 1.0;
+    return;
+  }
+  int e;
+  frexp(x, &e);
+  v[i] = ldexp(1.0, sqrt_of ? -(e / 2) : -e);
+}
+// diagonal of A into v
+__global__ void diag_kernel(const double* __restrict__ A, long lda, int n, double* __restrict__ v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = fabs(A[i + (long)i * lda]);
+}
+// ||A||_inf = max_i sum_j |a_ij|, one thread per row; the maximum is taken
+// with an integer atomicMax on the (non-negative) double's bits
+__global__ void inf_norm_kernel(const double* __restrict__ A, long lda, int n, unsigned long long* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int j = 0; j < n; ++j) s += fabs(A[i + (long)j * lda]);
+  atomicMax(out, (unsigned long long)__double_as_longlong(s));
+}
+// out[c] = max_i |X(i, c)|, one block per column
+__global__ void colmax_kernel(const double* __restrict__ X, long ldx, int n, double* __restrict__ out) {
+  __shared__ double red[256];
+  const int c = blockIdx.x;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v = fmax(v, fabs(X[i + (long)c * ldx]));
+  red[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[c] = red[0];
+}
+// Y(i, c) = (TO)(X(i, c) * (s ? s[i] : 1))
+template <typename TO, typename TI>
+__global__ void scale_copy_kernel(const TI* __restrict__ X, long ldx, TO* __restrict__ Y, long ldy, int n, int nrhs,
+                                  const double* __restrict__ s) {
+  const long total = (long)n * nrhs;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long i = e % n, c = e / n;
+    double v = (double)X[i + c * ldx];
+    if (s) v *= s[i];
+    Y[i + c * ldy] = (TO)v;
+  }
+}
+// X(i, c) += D(i, c)
+__global__ void add_kernel(double* __restrict__ X, long ldx, const double* __restrict__ D, long ldd, int n,
+                           int nrhs) {
+  const long total = (long)n * nrhs;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long i = e % n, c = e / n;
+    X[i + c * ldx] += D[i + c * ldd];
+  }
+}
+// out[q + c * nv] = sum_i V_q(i, c) W(i, c), V_q = V + q * vstride; grid (nrhs, nv)
+__global__ void coldots_kernel(const double* __restrict__ V, long vstride, const double* __restrict__ W, long ld,
+                               int n, int nv, double* __restrict__ out) {
+  __shared__ double red[256];
+  const int c = blockIdx.x, q = blockIdx.y;
+  const double* v = V + q * vstride + (long)c * ld;
+  const double* w = W + (long)c * ld;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s = fma(v[i], w[i], s);
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[q + (long)c * nv] = red[0];
+}
+// W(i, c) += sign * sum_q coef[q + c * nv] V_q(i, c)
+__global__ void col_combine_kernel(double* __restrict__ W, const double* __restrict__ V, long vstride, long ld,
+                                   int n, int nrhs, int nv, const double* __restrict__ coef, double sign) {
+  const long total = (long)n * nrhs;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long i = e % n, c = e / n;
+    double s = 0.0;
+    for (int q = 0; q < nv; ++q) s = fma(coef[q + c * nv], V[q * vstride + i + c * ld], s);
+    W[i + c * ld] += sign * s;
+  }
+}
+// Y(i, c) = X(i, c) * f[c]
+__global__ void colscale_kernel(const double* __restrict__ X, double* __restrict__ Y, long ld, int n, int nrhs,
+                                const double* __restrict__ f) {
+  const long total = (long)n * nrhs;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long i = e % n, c = e / n;
+    Y[i + c * ld] = X[i + c * ld] * f[c];
+  }
+}
+
+// perm[i] = source row of row i of P b: the pivot interchanges applied in
+// order to the identity (one thread; the vector in shared memory when it
+// fits, else in perm itself)
+__global__ void perm_from_pivots_kernel(const int* __restrict__ piv, int n, int* __restrict__ perm, int use_smem) {
+  extern __shared__ int sp[];
+  int* v = use_smem ? sp : perm;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v[i] = i;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int i = 0; i < n; ++i) {
+      const int t = i + piv[i];
+      const int x = v[i];
+      v[i] = v[t];
+      v[t] = x;
+    }
+  __syncthreads();
+  if (use_smem)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = v[i];
+}
+// T(i, c) = (float)(R(perm[i], c) * s[perm[i]])
+__global__ void gather_rows_kernel(const double* __restrict__ R, long ldr, const int* __restrict__ perm,
+                                   const double* __restrict__ s, float* __restrict__ T, long ldt, int n, int nrhs) {
+  const long total = (long)n * nrhs;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long i = e % n, c = e / n;
+    const int src = perm[i];
+    double v = R[src + c * ldr];
+    if (s) v *= s[src];
+    T[i + c * ldt] = (float)v;
+  }
+}
+
+inline int grid_for(long total) { return (int)std::min<long>(8192, (total + 255) / 256); }
+
+}  // namespace
+
+// ===========================================================================
+// Low-precision factorizations
+// ===========================================================================
+namespace {
+
+struct LpWork {
+  uint16_t* PA = nullptr;   // packed A-operand (n x MB)
+  uint16_t* PB = nullptr;   // packed B-operand (n x MB)
+  uint16_t* PC = nullptr;   // packed operand of the side stream (n x MB)
+  uint16_t* PX = nullptr;   // packed inverse block (MB x MB)
+  double* P64 = nullptr;    // FP64 panel (MB x n)
+  double* X64 = nullptr;    // FP64 inverse blocks (2 x MB x MB)
+};
+
+int lp_workspace(long n, LpFactor* f, LpWork* w) {
+  const size_t np = (size_t)std::max<long>(n, 1);
+  f->ldf = (n + 3) & ~3L;
+  f->F = (float*)ws_get(WS_LP0, sizeof(float) * (size_t)f->ldf * np);
+  char* p16 = (char*)ws_get(WS_LP1, sizeof(uint16_t) * (3 * (size_t)MB * np + (size_t)MB * MB) + 1024);
+  char* p64 = (char*)ws_get(WS_LP3, sizeof(double) * ((size_t)MB * np + 2 * (size_t)MB * MB) + 1024);
+  const long nblk = (n + MB - 1) / MB;
+  char* pinv = (char*)ws_get(WS_LP4, sizeof(float) * 2 * (size_t)nblk * MB * MB + sizeof(double) * 2 * np +
+                                         sizeof(int) * 2 * np + 1024);
+  if (!f->F || !p16 || !p64 || !pinv) return FLA_FAILURE;
+  w->PA = (uint16_t*)p16;
+  w->PB = w->PA + (size_t)MB * np;
+  w->PC = w->PB + (size_t)MB * np;
+  w->PX = w->PC + (size_t)MB * np;
+  w->P64 = (double*)p64;
+  w->X64 = w->P64 + (size_t)MB * np;
+  f->inv1 = (float*)pinv;
+  f->inv2 = f->inv1 + (size_t)nblk * MB * MB;
+  f->sr = (double*)(f->inv2 + (size_t)nblk * MB * MB);
+  f->sc = f->sr + np;
+  f->piv = (int*)(f->sc + np);
+  f->perm = f->piv + np;
+  f->n = n;
+  return FLA_SUCCESS;
+}
+
+}  // namespace
+
+// LU with partial pivoting of (diag(sr) A diag(sc)) in low precision, on the
+// transposed FP32 copy F = (scaled A)^T (n x n, ld ldf): the layout and the
+// step structure of the FP64 driver (lu_piv_dev), with every trailing update
+// and panel solve a 16-bit tensor-core GEMM.
+int lp_lu_factor(DMat A, LowPrec prec, bool scale, LpFactor* f) {
+  Context& cx = ctx();
+  cudaStream_t st = cx.stream, sd = cx.side;
+  const long n = A.m;
+  LpWork w;
+  if (lp_workspace(n, f, &w) != FLA_SUCCESS) return FLA_FAILURE;
+  f->chol = false;
+  f->prec = prec;
+  f->scaled = scale;
+  if (status_reset() != FLA_SUCCESS) return FLA_FAILURE;
+  if (scale) {
+    row_absmax_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(A.p, A.ld, (int)n, (int)n, nullptr, f->sr);
+    pow2_recip_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(f->sr, (int)n, 0);
+    col_absmax_kernel<<<(unsigned)n, 256, 0, st>>>(A.p, A.ld, (int)n, f->sr, f->sc);
+    pow2_recip_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(f->sc, (int)n, 0);
+    count_launch(4);
+  }
+  {
+    dim3 grid((unsigned)((n + 31) / 32), (unsigned)((n + 31) / 32)), block(32, 8);
+    transpose_scale_kernel<<<grid, block, 0, st>>>(A.p, A.ld, f->F, f->ldf, (int)n, (int)n, scale ? f->sr : nullptr,
+                                                   scale ? f->sc : nullptr);
+    count_launch();
+    FB_CK(cudaGetLastError());
+  }
+  float* F = f->F;
+  const long ldf = f->ldf;
+  auto at = [&](long i, long j) { return F + j + i * ldf; };  // element (i, j) of the scaled A
+  const long ldp = MB;
+  double* X64 = w.X64;                  // inv(L11^T)
+  double* Y64 = w.X64 + (size_t)MB * MB;  // inv(U11^T)
+
+  // panel k: FP64 copy, factor, round back, the two inverse triangles
+  auto panel = [&](long k, cudaStream_t s) -> int {
+    const int b = (int)std::min<long>(MB, n - k);
+    const long M = n - k;
+    const long kb = k / MB;
+    if (convert2d<double, float>(s, at(k, k), ldf, w.P64, ldp, b, M) != FLA_SUCCESS) return FLA_FAILURE;
+    if (lu_panel_factor_t(w.P64, ldp, M, b, f->piv + k, (int)k, s) != FLA_SUCCESS) return FLA_FAILURE;
+    if (convert2d<float, double>(s, w.P64, ldp, at(k, k), ldf, b, M) != FLA_SUCCESS) return FLA_FAILURE;
+    if (tri_inverse(w.P64, ldp, b, false, true, X64, MB, s) != FLA_SUCCESS) return FLA_FAILURE;
+    if (tri_inverse(w.P64, ldp, b, true, false, Y64, MB, s) != FLA_SUCCESS) return FLA_FAILURE;
+    if (convert2d<float, double>(s, X64, MB, f->inv1 + kb * MB * MB, MB, b, b) != FLA_SUCCESS) return FLA_FAILURE;
+    if (convert2d<float, double>(s, Y64, MB, f->inv2 + kb * MB * MB, MB, b, b) != FLA_SUCCESS) return FLA_FAILURE;
+    // B operand of U12^T := A12^T inv(L11^T): B(j, kk) = X64(kk, j)
+    return pack16<double>(s, prec, X64, MB, 1, w.PX, MB, b, b, 1.f);
+  };
+
+  cudaEvent_t ev_look = cx.ev[0], ev_panel = cx.ev[1];
+  if (panel(0, st) != FLA_SUCCESS) return FLA_FAILURE;
+  for (long k = 0; k < n; k += MB) {
+    const int b = (int)std::min<long>(MB, n - k);
+    const long nr = n - k - b;
+    if (laswp_t_f32(F, ldf, (int)k, f->piv + k, b, 0, (int)k, (int)(k + b), (int)nr, st) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    if (nr <= 0) continue;
+    // U12^T := A12^T inv(L11^T); A12^T(i, kk) = at(k + kk, k + b + i)
+    if (pack16<float>(st, prec, at(k, k + b), 1, ldf, w.PA, MB, nr, b, 1.f) != FLA_SUCCESS) return FLA_FAILURE;
+    if (lp_gemm(st, prec, nr, b, b, 1.f, w.PA, MB, w.PX, MB, 0.f, at(k, k + b), ldf) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    // trailing update  A22^T -= U12^T A21^T
+    if (pack16<float>(st, prec, at(k, k + b), 1, ldf, w.PA, MB, nr, b, 1.f) != FLA_SUCCESS) return FLA_FAILURE;
+    if (pack16<float>(st, prec, at(k + b, k), ldf, 1, w.PB, MB, nr, b, 1.f) != FLA_SUCCESS) return FLA_FAILURE;
+    const int nb2 = (int)std::min<long>(MB, nr);
+    if (lp_gemm(st, prec, nb2, nr, b, -1.f, w.PA, MB, w.PB, MB, 1.f, at(k + b, k + b), ldf) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    FB_CK(cudaEventRecord(ev_look, st));
+    FB_CK(cudaStreamWaitEvent(sd, ev_look, 0));
+    if (panel(k + b, sd) != FLA_SUCCESS) return FLA_FAILURE;
+    FB_CK(cudaEventRecord(ev_panel, sd));
+    if (nr > nb2 && lp_gemm(st, prec, nr - nb2, nr, b, -1.f, w.PA + (size_t)nb2 * MB, MB, w.PB, MB, 1.f,
+                            at(k + b, k + b + nb2), ldf) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    FB_CK(cudaStreamWaitEvent(st, ev_panel, 0));
+  }
+  {
+    const size_t sbytes = sizeof(int) * (size_t)n;
+    const bool smem = sbytes <= 200 * 1024;
+    if (smem) cudaFuncSetAttribute(perm_from_pivots_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    perm_from_pivots_kernel<<<1, 1024, smem ? sbytes : 0, st>>>(f->piv, (int)n, f->perm, smem ? 1 : 0);
+    count_launch();
+    FB_CK(cudaGetLastError());
+  }
+  int info = -1;
+  if (status_read(&info) != FLA_SUCCESS) return FLA_FAILURE;
+  f->info = info;
+  return FLA_SUCCESS;
+}
+
+// Cholesky of diag(d) A diag(d) in low precision; F holds L (lower, FP32).
+int lp_chol_factor(DMat A, bool upper, LowPrec prec, bool scale, LpFactor* f) {
+  Context& cx = ctx();
+  cudaStream_t st = cx.stream, sd = cx.side;
+  const long n = A.m;
+  LpWork w;
+  if (lp_workspace(n, f, &w) != FLA_SUCCESS) return FLA_FAILURE;
+  f->chol = true;
+  f->prec = prec;
+  f->scaled = scale;
+  if (status_reset() != FLA_SUCCESS) return FLA_FAILURE;
+  if (scale) {
+    diag_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(A.p, A.ld, (int)n, f->sr);
+    pow2_recip_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(f->sr, (int)n, 1);
+    count_launch(2);
+    FB_CK(cudaMemcpyAsync(f->sc, f->sr, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  }
+  lower_scale_kernel<<<grid_for(n * n), 256, 0, st>>>(A.p, A.ld, f->F, f->ldf, (int)n, scale ? f->sr : nullptr,
+                                                      upper ? 1 : 0);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  float* F = f->F;
+  const long ldf = f->ldf;
+  int* info = cx.d_status + ST_INFO;
+  auto at = [&](long i, long j) { return F + i + j * ldf; };
+
+  auto panel = [&](long k, cudaStream_t s) -> int {
+    const int b = (int)std::min<long>(MB, n - k);
+    const long kb = k / MB;
+    if (convert2d<double, float>(s, at(k, k), ldf, w.P64, MB, b, b) != FLA_SUCCESS) return FLA_FAILURE;
+    if (potrf_diag_dev(w.P64, MB, b, (int)k, s) != FLA_SUCCESS) return FLA_FAILURE;
+    if (tri_inverse(w.P64, MB, b, true, false, w.X64, MB, s) != FLA_SUCCESS) return FLA_FAILURE;
+    if (convert2d<float, double>(s, w.P64, MB, at(k, k), ldf, b, b) != FLA_SUCCESS) return FLA_FAILURE;
+    if (convert2d<float, double>(s, w.X64, MB, f->inv1 + kb * MB * MB, MB, b, b) != FLA_SUCCESS) return FLA_FAILURE;
+    const long m2 = n - k - b;
+    if (m2 <= 0) return FLA_SUCCESS;
+    // A21 := A21 inv(L11)^T: B(j, kk) = inv(L11)(j, kk)
+    if (pack16<double>(s, prec, w.X64, 1, MB, w.PX, MB, b, b, 1.f) != FLA_SUCCESS) return FLA_FAILURE;
+    if (pack16<float>(s, prec, at(k + b, k), 1, ldf, w.PC, MB, m2, b, 1.f) != FLA_SUCCESS) return FLA_FAILURE;
+    return lp_gemm(s, prec, m2, b, b, 1.f, w.PC, MB, w.PX, MB, 0.f, at(k + b, k), ldf, GEMM_FULL, 0, info,
+                   (int)(k + b));
+  };
+
+  cudaEvent_t ev_look = cx.ev[2], ev_panel = cx.ev[3];
+  if (panel(0, st) != FLA_SUCCESS) return FLA_FAILURE;
+  for (long k = 0; k < n; k += MB) {
+    const int b = (int)std::min<long>(MB, n - k);
+    const long m2 = n - k - b;
+    if (m2 <= 0) break;
+    const int lim = (int)(k + b);
+    const int nb2 = (int)std::min<long>(MB, m2);
+    if (pack16<float>(st, prec, at(k + b, k), 1, ldf, w.PA, MB, m2, b, 1.f) != FLA_SUCCESS) return FLA_FAILURE;
+    if (lp_gemm(st, prec, m2, nb2, b, -1.f, w.PA, MB, w.PA, MB, 1.f, at(k + b, k + b), ldf, GEMM_LOWER, 0, info,
+                lim) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    FB_CK(cudaEventRecord(ev_look, st));
+    FB_CK(cudaStreamWaitEvent(sd, ev_look, 0));
+    if (panel(k + b, sd) != FLA_SUCCESS) return FLA_FAILURE;
+    FB_CK(cudaEventRecord(ev_panel, sd));
+    if (m2 > nb2 && lp_gemm(st, prec, m2 - nb2, m2 - nb2, b, -1.f, w.PA + (size_t)nb2 * MB, MB,
+                            w.PA + (size_t)nb2 * MB, MB, 1.f, at(k + b + nb2, k + b + nb2), ldf, GEMM_LOWER, 0, info,
+                            lim) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    FB_CK(cudaStreamWaitEvent(st, ev_panel, 0));
+  }
+  int inf = -1;
+  if (status_read(&inf) != FLA_SUCCESS) return FLA_FAILURE;
+  f->info = inf;
+  return FLA_SUCCESS;
+}
+
+// ===========================================================================
+// Correction solve with the low-precision factors: D := M^-1 R (FP64 in and
+// out, FP32 inside).  T is an FP32 n x nrhs workspace, ld n.
+// ===========================================================================
+int lp_solve(const LpFactor& f, const double* R, long ldr, double* D, long ldd, long nrhs, float* T, float* Tb,
+             cudaStream_t st) {
+  const long n = f.n;
+  const long nblk = (n + MB - 1) / MB;
+  const float* F = f.F;
+  const long ldf = f.ldf;
+  // T := scale * R, rows permuted (LU)
+  if (!f.chol) {
+    gather_rows_kernel<<<grid_for(n * nrhs), 256, 0, st>>>(R, ldr, f.perm, f.scaled ? f.sr : nullptr, T, n, (int)n,
+                                                           (int)nrhs);
+  } else {
+    scale_copy_kernel<float, double><<<grid_for(n * nrhs), 256, 0, st>>>(R, ldr, T, n, (int)n, (int)nrhs,
+                                                                        f.scaled ? f.sr : nullptr);
+  }
+  count_launch();
+  // forward: L y = T
+  for (long kb = 0; kb < nblk; ++kb) {
+    const long k = kb * MB;
+    const int b = (int)std::min<long>(MB, n - k);
+    const long rest = n - k - b;
+    const float* inv = f.inv1 + kb * MB * MB;
+    // LU: inv(L11) = inv(L11^T)^T; Cholesky: inv(L11)
+    if (sgemm(st, !f.chol, false, b, nrhs, b, 1.f, inv, MB, T + k, n, 0.f, Tb, MB) != FLA_SUCCESS) return FLA_FAILURE;
+    FB_CK(cudaMemcpy2DAsync(T + k, sizeof(float) * n, Tb, sizeof(float) * MB, sizeof(float) * b, nrhs,
+                            cudaMemcpyDeviceToDevice, st));
+    if (rest > 0) {
+      if (!f.chol) {
+        // L(k+b+i, k+j) = F[(k + j) + (k + b + i) * ldf]
+        if (sgemm(st, true, false, rest, nrhs, b, -1.f, F + k + (k + b) * ldf, ldf, Tb, MB, 1.f, T + k + b, n) !=
+            FLA_SUCCESS)
+          return FLA_FAILURE;
+      } else {
+        if (sgemm(st, false, false, rest, nrhs, b, -1.f, F + (k + b) + k * ldf, ldf, Tb, MB, 1.f, T + k + b, n) !=
+            FLA_SUCCESS)
+          return FLA_FAILURE;
+      }
+    }
+  }
+  // backward: U x = y (LU) or L^T x = y (Cholesky)
+  for (long kb = nblk - 1; kb >= 0; --kb) {
+    const long k = kb * MB;
+    const int b = (int)std::min<long>(MB, n - k);
+    const float* inv = f.chol ? f.inv1 + kb * MB * MB : f.inv2 + kb * MB * MB;
+    // LU: inv(U11) = inv(U11^T)^T; Cholesky: inv(L11^T) = inv(L11)^T
+    if (sgemm(st, true, false, b, nrhs, b, 1.f, inv, MB, T + k, n, 0.f, Tb, MB) != FLA_SUCCESS) return FLA_FAILURE;
+    FB_CK(cudaMemcpy2DAsync(T + k, sizeof(float) * n, Tb, sizeof(float) * MB, sizeof(float) * b, nrhs,
+                            cudaMemcpyDeviceToDevice, st));
+    if (k > 0) {
+      // LU: U(i, k + j) = F[(k + j) + i * ldf];  Cholesky: L^T(i, k + j) = F[(k + j) + i * ldf]
+      if (sgemm(st, true, false, k, nrhs, b, -1.f, F + k, ldf, Tb, MB, 1.f, T, n) != FLA_SUCCESS) return FLA_FAILURE;
+    }
+  }
+  scale_copy_kernel<double, float><<<grid_for(n * nrhs), 256, 0, st>>>(T, n, D, ldd, (int)n, (int)nrhs,
+                                                                      f.scaled ? f.sc : nullptr);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
+}
+
+// ===========================================================================
+// Refinement
+// ===========================================================================
+namespace {
+
+struct IrBuffers {
+  double* R = nullptr;    // residual n x nrhs
+  double* D = nullptr;    // correction
+  double* R64 = nullptr;  // A V_j in GMRES
+  float* T = nullptr;     // FP32 right-hand sides
+  float* Tb = nullptr;    // FP32 block scratch (MB x nrhs)
+  double* V = nullptr;    // GMRES basis (m + 1) x n x nrhs
+  double* W = nullptr;    // GMRES work vector block
+  double* small = nullptr;  // device: dots and norms
+  double* h_small = nullptr;
+};
+
+// R := B - A X (FP64 DMMA GEMM)
+int residual(const DMat& A, const DMat& B, const double* X, long ldx, double* R, long ldr, long nrhs,
+             cudaStream_t st) {
+  const long n = A.m;
+  FB_CK(cudaMemcpy2DAsync(R, sizeof(double) * ldr, B.p, sizeof(double) * B.ld, sizeof(double) * n, nrhs,
+                          cudaMemcpyDeviceToDevice, st));
+  return gemm_f64(st, false, false, n, nrhs, n, -1.0, A.p, A.ld, X, ldx, 1.0, R, ldr);
+}
+
+// max-abs per column of X and R on the host; true when every column has
+// ||r||_inf <= ||x||_inf * cte (dsgesv.c:330-334)
+int converged(const double* X, long ldx, const double* R, long ldr, long n, long nrhs, double cte, IrBuffers& b,
+              cudaStream_t st, bool* ok) {
+  colmax_kernel<<<(unsigned)nrhs, 256, 0, st>>>(X, ldx, (int)n, b.small);
+  colmax_kernel<<<(unsigned)nrhs, 256, 0, st>>>(R, ldr, (int)n, b.small + nrhs);
+  count_launch(2);
+  FB_CK(cudaMemcpyAsync(b.h_small, b.small, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, st));
+  FB_CK(cudaStreamSynchronize(st));
+  *ok = true;
+  for (long c = 0; c < nrhs; ++c)
+    if (!(b.h_small[nrhs + c] <= b.h_small[c] * cte)) *ok = false;
+  return FLA_SUCCESS;
+}
+
+// GMRES(m), left-preconditioned by the low-precision factors, all columns in
+// lockstep: D ~= A^-1 R.  Classical Gram-Schmidt applied twice per step.
+int gmres(const DMat& A, const LpFactor& f, const double* R, double* D, long nrhs, int m, double tol, IrBuffers& b,
+          cudaStream_t st, int* iters) {
+  const long n = A.m;
+  const long ld = (n + 1) & ~1L;  // 16-byte leading dimensions for the GEMM engine
+  const long vstride = ld * nrhs;
+  double* V = b.V;
+  double* W = b.W;
+  double* dev = b.small;         // device scratch: (m + 1) x nrhs dots, nrhs norms
+  double* host = b.h_small;
+  // V0 = M^-1 R, beta = ||V0||
+  if (lp_solve(f, R, ld, V, ld, nrhs, b.T, b.Tb, st) != FLA_SUCCESS) return FLA_FAILURE;
+  coldots_kernel<<<dim3((unsigned)nrhs, 1), 256, 0, st>>>(V, 0, V, ld, (int)n, 1, dev);
+  count_launch();
+  FB_CK(cudaMemcpyAsync(host, dev, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
+  FB_CK(cudaStreamSynchronize(st));
+  std::vector<double> beta(nrhs), inv(nrhs);
+  for (long c = 0; c < nrhs; ++c) {
+    beta[c] = std::sqrt(std::max(0.0, host[c]));
+    inv[c] = beta[c] > 0 ? 1.0 / beta[c] : 0.0;
+  }
+  FB_CK(cudaMemcpyAsync(dev, inv.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, st));
+  colscale_kernel<<<grid_for(n * nrhs), 256, 0, st>>>(V, V, ld, (int)n, (int)nrhs, dev);
+  count_launch();
+  // Hessenberg, Givens rotations and right-hand side per column (host)
+  std::vector<double> H((size_t)(m + 1) * m * nrhs, 0.0), cs((size_t)m * nrhs), sn((size_t)m * nrhs),
+      g((size_t)(m + 1) * nrhs, 0.0);
+  for (long c = 0; c < nrhs; ++c) g[c * (m + 1)] = beta[c];
+  auto Hc = [&](long c, int i, int j) -> double& { return H[(size_t)c * (m + 1) * m + i + (size_t)j * (m + 1)]; };
+  int jdone = 0;
+  std::vector<double> hbuf((size_t)(m + 1) * nrhs), hbuf2((size_t)(m + 1) * nrhs);
+  for (int j = 0; j < m; ++j) {
+    double* Vj = V + j * vstride;
+    // W = M^-1 (A Vj)
+    if (gemm_f64(st, false, false, n, nrhs, n, 1.0, A.p, A.ld, Vj, ld, 0.0, b.R64, ld) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    if (lp_solve(f, b.R64, ld, W, ld, nrhs, b.T, b.Tb, st) != FLA_SUCCESS) return FLA_FAILURE;
+    // two passes of classical Gram-Schmidt against V0..Vj
+    const int nv = j + 1;
+    for (int pass = 0; pass < 2; ++pass) {
+      coldots_kernel<<<dim3((unsigned)nrhs, (unsigned)nv), 256, 0, st>>>(V, vstride, W, ld, (int)n, nv, dev);
+      col_combine_kernel<<<grid_for(n * nrhs), 256, 0, st>>>(W, V, vstride, ld, (int)n, (int)nrhs, nv, dev, -1.0);
+      count_launch(2);
+      FB_CK(cudaMemcpyAsync(pass == 0 ? hbuf.data() : hbuf2.data(), dev, sizeof(double) * nv * nrhs,
+                            cudaMemcpyDeviceToHost, st));
+    }
+    coldots_kernel<<<dim3((unsigned)nrhs, 1), 256, 0, st>>>(W, 0, W, ld, (int)n, 1, dev);
+    count_launch();
+    FB_CK(cudaMemcpyAsync(host, dev, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
+    FB_CK(cudaStreamSynchronize(st));
+    bool all = true;
+    for (long c = 0; c < nrhs; ++c) {
+      for (int i = 0; i < nv; ++i) Hc(c, i, j) = hbuf[i + c * nv] + hbuf2[i + c * nv];
+      const double hn = std::sqrt(std::max(0.0, host[c]));
+      Hc(c, j + 1, j) = hn;
+      inv[c] = hn > 0 ? 1.0 / hn : 0.0;
+      // apply the previous rotations, then a new one zeroing H(j+1, j)
+      for (int i = 0; i < j; ++i) {
+        const double a = Hc(c, i, j), bb = Hc(c, i + 1, j);
+        Hc(c, i, j) = cs[c * m + i] * a + sn[c * m + i] * bb;
+        Hc(c, i + 1, j) = -sn[c * m + i] * a + cs[c * m + i] * bb;
+      }
+      const double a = Hc(c, j, j), bb = Hc(c, j + 1, j);
+      const double r = std::hypot(a, bb);
+      const double cc = r > 0 ? a / r : 1.0, ss = r > 0 ? bb / r : 0.0;
+      cs[c * m + j] = cc;
+      sn[c * m + j] = ss;
+      Hc(c, j, j) = r;
+      Hc(c, j + 1, j) = 0.0;
+      const double gj = g[c * (m + 1) + j];
+      g[c * (m + 1) + j] = cc * gj;
+      g[c * (m + 1) + j + 1] = -ss * gj;
+      if (!(std::fabs(g[c * (m + 1) + j + 1]) <= tol * beta[c])) all = false;
+    }
+    jdone = j + 1;
+    if (all || j + 1 == m) break;
+    FB_CK(cudaMemcpyAsync(dev, inv.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, st));
+    colscale_kernel<<<grid_for(n * nrhs), 256, 0, st>>>(W, V + (j + 1) * vstride, ld, (int)n, (int)nrhs, dev);
+    count_launch();
+  }
+  // y = H^-1 g per column, D = V y
+  std::vector<double> y((size_t)jdone * nrhs, 0.0);
+  for (long c = 0; c < nrhs; ++c)
+    for (int i = jdone - 1; i >= 0; --i) {
+      double s = g[c * (m + 1) + i];
+      for (int q = i + 1; q < jdone; ++q) s -= Hc(c, i, q) * y[q + c * jdone];
+      const double d = Hc(c, i, i);
+      y[i + c * jdone] = d != 0.0 ? s / d : 0.0;
+    }
+  FB_CK(cudaMemsetAsync(D, 0, sizeof(double) * ld * nrhs, st));
+  FB_CK(cudaMemcpyAsync(dev, y.data(), sizeof(double) * jdone * nrhs, cudaMemcpyHostToDevice, st));
+  col_combine_kernel<<<grid_for(n * nrhs), 256, 0, st>>>(D, V, vstride, ld, (int)n, (int)nrhs, jdone, dev, 1.0);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  *iters = jdone;
+  return FLA_SUCCESS;
+}
+
+}  // namespace
+
+// Refine X for A X = B with the low-precision factors f; X (n x nrhs, ld ldx)
+// receives the solution.  Returns FLA_SUCCESS with res->iter >= 0 on
+// convergence, res->iter = -31 (no convergence) otherwise.
+int ir_refine(const DMat& A, const DMat& B, double* X, long ldx, const LpFactor& f, const IrConfig& cfg,
+              IrResult* res) {
+  Context& cx = ctx();
+  cudaStream_t st = cx.stream;
+  const long n = A.m, nrhs = B.n;
+  res->iter = 0;
+  res->inner = 0;
+  IrBuffers b;
+  const int m = std::max(1, cfg.gmres_m);
+  const long ldn = (n + 1) & ~1L;  // 16-byte leading dimensions for the GEMM engine
+  const size_t nb = (size_t)ldn * nrhs;
+  char* w0 = (char*)ws_get(WS_IR0, sizeof(double) * 3 * nb + sizeof(float) * (nb + (size_t)MB * nrhs) + 4096);
+  double* v = cfg.solver == IR_GMRES ? (double*)ws_get(WS_IR1, sizeof(double) * (size_t)(m + 2) * nb) : nullptr;
+  char* w2 = (char*)ws_get(WS_IR2, sizeof(double) * (size_t)(m + 2) * (nrhs + 2) + 4096);
+  if (!w0 || !w2 || (cfg.solver == IR_GMRES && !v)) return FLA_FAILURE;
+  b.R = (double*)w0;
+  b.D = b.R + nb;
+  b.R64 = b.D + nb;
+  b.T = (float*)(b.R64 + nb);
+  b.Tb = b.T + nb;
+  b.V = v;
+  b.W = v ? v + (size_t)(m + 1) * nb : nullptr;
+  b.small = (double*)w2;
+  std::vector<double> hs((size_t)(m + 2) * (nrhs + 2));
+  b.h_small = hs.data();
+
+  // cte = ||A||_inf * eps * sqrt(n)  (dsgesv.c:287-289)
+  unsigned long long* dn = (unsigned long long*)b.small;
+  FB_CK(cudaMemsetAsync(dn, 0, sizeof(unsigned long long), st));
+  inf_norm_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(A.p, A.ld, (int)n, dn);
+  count_launch();
+  unsigned long long bits = 0;
+  FB_CK(cudaMemcpyAsync(&bits, dn, sizeof(bits), cudaMemcpyDeviceToHost, st));
+  FB_CK(cudaStreamSynchronize(st));
+  double anrm;
+  std::memcpy(&anrm, &bits, sizeof(anrm));
+  const double eps = DBL_EPSILON * 0.5;
+  const double cte = anrm * eps * std::sqrt((double)n);
+  res->anorm = anrm;
+
+  // x = M^-1 b
+  if (lp_solve(f, B.p, B.ld, X, ldx, nrhs, b.T, b.Tb, st) != FLA_SUCCESS) return FLA_FAILURE;
+  if (residual(A, B, X, ldx, b.R, ldn, nrhs, st) != FLA_SUCCESS) return FLA_FAILURE;
+  bool ok = false;
+  if (converged(X, ldx, b.R, ldn, n, nrhs, cte, b, st, &ok) != FLA_SUCCESS) return FLA_FAILURE;
+  if (ok) return FLA_SUCCESS;
+  for (int it = 1; it <= cfg.itermax; ++it) {
+    if (cfg.solver == IR_GMRES) {
+      int inner = 0;
+      if (gmres(A, f, b.R, b.D, nrhs, m, cfg.gmres_tol, b, st, &inner) != FLA_SUCCESS) return FLA_FAILURE;
+      res->inner += inner;
+    } else {
+      if (lp_solve(f, b.R, ldn, b.D, ldn, nrhs, b.T, b.Tb, st) != FLA_SUCCESS) return FLA_FAILURE;
+    }
+    add_kernel<<<grid_for(n * nrhs), 256, 0, st>>>(X, ldx, b.D, ldn, (int)n, (int)nrhs);
+    count_launch();
+    if (residual(A, B, X, ldx, b.R, ldn, nrhs, st) != FLA_SUCCESS) return FLA_FAILURE;
+    if (converged(X, ldx, b.R, ldn, n, nrhs, cte, b, st, &ok) != FLA_SUCCESS) return FLA_FAILURE;
+    if (ok) {
+      res->iter = it;
+      return FLA_SUCCESS;
+    }
+  }
+  res->iter = -(cfg.itermax + 1);
+  return FLA_SUCCESS;
+}
+
+// Full symmetric FP64 copy of the stored triangle (residuals of the
+// Cholesky solvers need the whole matrix).
+int symmetrize(const DMat& A, bool upper, double* S, long lds, cudaStream_t st) {
+  symmetrize_kernel<<<grid_for(A.m * A.m), 256, 0, st>>>(A.p, A.ld, S, lds, (int)A.m, upper ? 1 : 0);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
+}
+
+IrConfig ir_default_config() {
+  IrConfig c;
+  if (const char* e = std::getenv("FLA_B200_IR_PREC")) {
+    const std::string s(e);
+    if (s == "bf16") c.prec = LP_BF16;
+    if (s == "fp16") c.prec = LP_FP16;
+  }
+  if (const char* e = std::getenv("FLA_B200_IR_SOLVER")) {
+    const std::string s(e);
+    if (s == "ir") c.solver = IR_CLASSIC;
+    if (s == "gmres") c.solver = IR_GMRES;
+  }
+  return c;
+}
+
+}  // namespace fb

@@ -1,0 +1,53 @@
+// Mixed-precision solvers (mixed.cu): low-precision factors and refinement.
+#pragma once
+#include "common.h"
+#include "lowprec.h"
+
+namespace fb {
+
+enum IrSolver : int { IR_CLASSIC = 0, IR_GMRES = 1 };
+
+struct IrConfig {
+  LowPrec prec = LP_FP16;   // 16-bit format of the tensor-core updates
+  bool scale = true;        // power-of-two equilibration before rounding
+  IrSolver solver = IR_GMRES;
+  int itermax = 30;         // ITERMAX of dsgesv_/dsposv_
+  int gmres_m = 30;         // GMRES restart length (inner iterations per step)
+  double gmres_tol = 1e-8;  // inner relative residual target
+};
+
+struct IrResult {
+  int iter = 0;      // refinement steps (>= 0), or -31 when not converged
+  int inner = 0;     // GMRES iterations in total
+  double anorm = 0;  // ||A||_inf
+};
+
+// Factors of diag(sr) A diag(sc) (LU, transposed layout) or of
+// diag(sr) A diag(sr) (Cholesky, lower) held in FP32.
+struct LpFactor {
+  bool chol = false;
+  bool scaled = false;
+  LowPrec prec = LP_FP16;
+  long n = 0;
+  float* F = nullptr;   // LU: (P D_r A D_c)^T = (L U)^T; Cholesky: L (lower)
+  long ldf = 0;
+  int* piv = nullptr;   // LU: relative pivots
+  int* perm = nullptr;  // LU: row order of P b (perm[i] = source row of row i)
+  float* inv1 = nullptr;  // per 128-block: LU inv(L11^T); Cholesky inv(L11)
+  float* inv2 = nullptr;  // per 128-block: LU inv(U11^T)
+  double* sr = nullptr;   // row scaling (or the symmetric scaling)
+  double* sc = nullptr;   // column scaling
+  int info = -1;          // first failing column of the low-precision factorization
+};
+
+int lp_lu_factor(DMat A, LowPrec prec, bool scale, LpFactor* f);
+int lp_chol_factor(DMat A, bool upper, LowPrec prec, bool scale, LpFactor* f);
+// D := M^-1 R with the low-precision factors (FP64 in and out).
+int lp_solve(const LpFactor& f, const double* R, long ldr, double* D, long ldd, long nrhs, float* T, float* Tb,
+             cudaStream_t st);
+int ir_refine(const DMat& A, const DMat& B, double* X, long ldx, const LpFactor& f, const IrConfig& cfg,
+              IrResult* res);
+int symmetrize(const DMat& A, bool upper, double* S, long lds, cudaStream_t st);
+IrConfig ir_default_config();
+
+}  // namespace fb

@@ -5,6 +5,7 @@
 #include <cstring>
 
 #include "common.h"
+#include "mixed.h"
 
 namespace fb {
 
@@ -531,6 +532,245 @@ int dgesv_(int* n, int* nrhs, double* a, int* lda, int* ipiv, double* b, int* ld
   if (sync_all() != FLA_SUCCESS) return FLA_FAILURE;
   *info = (e >= 0) ? e + 1 : 0;
   return 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Mixed-precision solvers.
+// ---------------------------------------------------------------------------
+namespace {
+
+// Solve A X = B by low-precision LU/Cholesky + refinement, with the FP64
+// factorization as the fallback.  A, B, X: device views (X aligned).  On
+// success with refinement A is untouched; `fact` (if not null) receives the
+// FP64 factors on fallback.  iter: refinement steps (>= 0) or the dsgesv_
+// code of the fallback (-3 low-precision factorization failed, -31 no
+// convergence).  d_piv receives the pivots used (relative, device).
+int mixed_solve_dev(bool chol, bool upper, DMat A, DMat B, DMat X, int* d_piv, const IrConfig& cfg, bool overwrite_a,
+                    int* iter, int* inner, int* info) {
+  cudaStream_t st = ctx().stream;
+  const long n = A.m;
+  *iter = 0;
+  *inner = 0;
+  *info = 0;
+  LpFactor f;
+  int r = chol ? lp_chol_factor(A, upper, cfg.prec, cfg.scale, &f) : lp_lu_factor(A, cfg.prec, cfg.scale, &f);
+  if (r != FLA_SUCCESS) return FLA_FAILURE;
+  bool fallback = false;
+  if (f.info >= 0) {
+    *iter = -3;
+    fallback = true;
+  } else {
+    DMat Ares = A;
+    if (chol) {
+      // the refinement's residual needs the whole symmetric matrix
+      const long ld = (n + 1) & ~1L;
+      double* S = (double*)ws_get(WS_FB, sizeof(double) * (size_t)ld * (size_t)std::max<long>(1, n));
+      if (!S) return FLA_FAILURE;
+      if (symmetrize(A, upper, S, ld, st) != FLA_SUCCESS) return FLA_FAILURE;
+      Ares.p = S;
+      Ares.ld = ld;
+    }
+    IrResult res;
+    if (ir_refine(Ares, B, X.p, X.ld, f, cfg, &res) != FLA_SUCCESS) return FLA_FAILURE;
+    *inner = res.inner;
+    if (res.iter >= 0) {
+      *iter = res.iter;
+      if (!chol) FB_CK(cudaMemcpyAsync(d_piv, f.piv, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
+      return sync_all();
+    }
+    *iter = res.iter;
+    fallback = true;
+  }
+  (void)fallback;
+  // FP64 factorization (in place, or on a copy when A must stay unchanged)
+  DMat Af = A;
+  if (!overwrite_a) {
+    const long ld = (n + 1) & ~1L;
+    double* Cp = (double*)ws_get(WS_FB, sizeof(double) * (size_t)ld * (size_t)std::max<long>(1, n));
+    if (!Cp) return FLA_FAILURE;
+    FB_CK(cudaMemcpy2DAsync(Cp, sizeof(double) * ld, A.p, sizeof(double) * A.ld, sizeof(double) * n, n,
+                            cudaMemcpyDeviceToDevice, st));
+    Af.p = Cp;
+    Af.ld = ld;
+  }
+  int e = -1;
+  if (chol) {
+    if ((upper ? chol_upper_dev(Af, &e) : chol_lower_dev(Af, &e)) != FLA_SUCCESS) return FLA_FAILURE;
+  } else {
+    if (lu_piv_dev(Af, d_piv, &e) != FLA_SUCCESS) return FLA_FAILURE;
+  }
+  if (e >= 0) {
+    *info = e + 1;
+    return sync_all();
+  }
+  FB_CK(cudaMemcpy2DAsync(X.p, sizeof(double) * X.ld, B.p, sizeof(double) * B.ld, sizeof(double) * n, X.n,
+                          cudaMemcpyDeviceToDevice, st));
+  if ((chol ? potrs_dev(upper, Af, X) : getrs_dev(false, Af, d_piv, X)) != FLA_SUCCESS) return FLA_FAILURE;
+  return sync_all();
+}
+
+IrConfig config_from(int prec, int solver) {
+  IrConfig c = ir_default_config();
+  if (prec == 0) c.prec = LP_BF16;
+  if (prec == 1) c.prec = LP_FP16;
+  if (solver == 0) c.solver = IR_CLASSIC;
+  if (solver == 1) c.solver = IR_GMRES;
+  return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+// src/map/common/lapacksrc/f2c/dsgesv.c:189-412: same arguments, checks and
+// ITER/INFO conventions; the single-precision factorization is the 16-bit
+// tensor-core LU (format and refinement from FLA_B200_IR_PREC /
+// FLA_B200_IR_SOLVER, default FP16 with equilibration and GMRES-IR).  work
+// and swork are not referenced (the library keeps its own workspace).
+int dsgesv_(int* n, int* nrhs, double* a, int* lda, int* ipiv, double* b, int* ldb, double* x, int* ldx,
+            double* work, float* swork, int* iter, int* info) {
+  (void)work;
+  (void)swork;
+  *info = 0;
+  *iter = 0;
+  if (*n < 0) return xerbla("DSGESV", 1, info);
+  if (*nrhs < 0) return xerbla("DSGESV", 2, info);
+  if (*lda < std::max(1, *n)) return xerbla("DSGESV", 4, info);
+  if (*ldb < std::max(1, *n)) return xerbla("DSGESV", 7, info);
+  if (*ldx < std::max(1, *n)) return xerbla("DSGESV", 9, info);
+  if (*n == 0) return 0;
+  ensure_init();
+  FLA_Base_obj ba, bb, bx;
+  FLA_Obj A = raw_obj(FLA_DOUBLE, a, *n, *n, *lda, &ba);
+  FLA_Obj B = raw_obj(FLA_DOUBLE, b, *n, *nrhs, *ldb, &bb);
+  FLA_Obj X = raw_obj(FLA_DOUBLE, x, *n, *nrhs, *ldx, &bx);
+  Staged sa, sb, sx;
+  if (stage(A, WS_STAGE_A, &sa) != FLA_SUCCESS || stage(B, WS_STAGE_B, &sb) != FLA_SUCCESS ||
+      stage(X, WS_STAGE_X, &sx, false) != FLA_SUCCESS)
+    return FLA_FAILURE;
+  const int nn = *n;
+  int* dp = (int*)ws_get(WS_STAGE_P, sizeof(int) * (size_t)nn);
+  if (!dp) return FLA_FAILURE;
+  int it = 0, inner = 0, inf = 0;
+  if (mixed_solve_dev(false, false, to_dmat(sa), to_dmat(sb), to_dmat(sx), dp, config_from(-1, -1), true, &it,
+                      &inner, &inf) != FLA_SUCCESS)
+    return FLA_FAILURE;
+  shift_pivots_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, ctx().stream>>>(dp, nn, 1);
+  count_launch();
+  if (it < 0 && unstage(sa) != FLA_SUCCESS) return FLA_FAILURE;  // FP64 factors on fallback
+  if (inf == 0 && unstage(sx) != FLA_SUCCESS) return FLA_FAILURE;
+  FB_CK(cudaMemcpyAsync(ipiv, dp, sizeof(int) * nn, cudaMemcpyDefault, ctx().stream));
+  if (sync_all() != FLA_SUCCESS) return FLA_FAILURE;
+  *iter = it;
+  *info = inf;
+  return 0;
+}
+
+// src/map/common/lapacksrc/f2c/dsposv.c:250-413, as dsgesv_ with the
+// Cholesky factorization of the uplo triangle.
+int dsposv_(char* uplo, int* n, int* nrhs, double* a, int* lda, double* b, int* ldb, double* x, int* ldx,
+            double* work, float* swork, int* iter, int* info) {
+  (void)work;
+  (void)swork;
+  *info = 0;
+  *iter = 0;
+  const bool up = lsame1(uplo, 'U');
+  if (!up && !lsame1(uplo, 'L')) return xerbla("DSPOSV", 1, info);
+  if (*n < 0) return xerbla("DSPOSV", 2, info);
+  if (*nrhs < 0) return xerbla("DSPOSV", 3, info);
+  if (*lda < std::max(1, *n)) return xerbla("DSPOSV", 5, info);
+  if (*ldb < std::max(1, *n)) return xerbla("DSPOSV", 7, info);
+  if (*ldx < std::max(1, *n)) return xerbla("DSPOSV", 9, info);
+  if (*n == 0) return 0;
+  ensure_init();
+  FLA_Base_obj ba, bb, bx;
+  FLA_Obj A = raw_obj(FLA_DOUBLE, a, *n, *n, *lda, &ba);
+  FLA_Obj B = raw_obj(FLA_DOUBLE, b, *n, *nrhs, *ldb, &bb);
+  FLA_Obj X = raw_obj(FLA_DOUBLE, x, *n, *nrhs, *ldx, &bx);
+  Staged sa, sb, sx;
+  if (stage(A, WS_STAGE_A, &sa) != FLA_SUCCESS || stage(B, WS_STAGE_B, &sb) != FLA_SUCCESS ||
+      stage(X, WS_STAGE_X, &sx, false) != FLA_SUCCESS)
+    return FLA_FAILURE;
+  int it = 0, inner = 0, inf = 0;
+  if (mixed_solve_dev(true, up, to_dmat(sa), to_dmat(sb), to_dmat(sx), nullptr, config_from(-1, -1), true, &it,
+                      &inner, &inf) != FLA_SUCCESS)
+    return FLA_FAILURE;
+  if (it < 0 && unstage(sa) != FLA_SUCCESS) return FLA_FAILURE;
+  if (inf == 0 && unstage(sx) != FLA_SUCCESS) return FLA_FAILURE;
+  if (sync_all() != FLA_SUCCESS) return FLA_FAILURE;
+  *iter = it;
+  *info = inf;
+  return 0;
+}
+
+// X := A^-1 B by the mixed-precision LU solver; A is left unchanged.
+// prec: 0 BF16, 1 FP16 (equilibrated), -1 library default; solver: 0
+// classic refinement, 1 GMRES-IR, -1 default.  iter / inner (optional):
+// refinement steps (or -3 / -31 when the FP64 fallback ran) and GMRES
+// iterations.  Returns FLA_SUCCESS, the zero-based index of a zero pivot of
+// the fallback factorization, or FLA_FAILURE.
+FLA_Error FLA_B200_LU_piv_solve_mixed(FLA_Obj A, FLA_Obj B, FLA_Obj X, int prec, int solver, int* iter,
+                                      int* inner) {
+  ensure_init();
+  FB_REQUIRE(A.base && A.base->datatype == FLA_DOUBLE && A.m == A.n, "FLA_B200_LU_piv_solve_mixed",
+             "A must be a square FLA_DOUBLE matrix");
+  FB_REQUIRE(B.base && X.base && B.m == A.m && X.m == A.m && X.n == B.n, "FLA_B200_LU_piv_solve_mixed",
+             "B and X must be n x nrhs");
+  if (A.m == 0 || B.n == 0) return FLA_SUCCESS;
+  Staged sa, sb, sx;
+  if (stage(A, WS_STAGE_A, &sa) != FLA_SUCCESS || stage(B, WS_STAGE_B, &sb) != FLA_SUCCESS ||
+      stage(X, WS_STAGE_X, &sx, false) != FLA_SUCCESS)
+    return FLA_FAILURE;
+  int* dp = (int*)ws_get(WS_STAGE_P, sizeof(int) * (size_t)A.m);
+  if (!dp) return FLA_FAILURE;
+  int it = 0, inn = 0, inf = 0;
+  op_begin(ctx().stream);
+  op_hold(true);
+  const int r = mixed_solve_dev(false, false, to_dmat(sa), to_dmat(sb), to_dmat(sx), dp, config_from(prec, solver),
+                                false, &it, &inn, &inf);
+  op_hold(false);
+  if (r != FLA_SUCCESS) return FLA_FAILURE;
+  if (unstage(sx) != FLA_SUCCESS) return FLA_FAILURE;
+  op_end(ctx().stream);
+  if (sync_all() != FLA_SUCCESS) return FLA_FAILURE;
+  if (iter) *iter = it;
+  if (inner) *inner = inn;
+  return inf > 0 ? inf - 1 : FLA_SUCCESS;
+}
+
+// X := A^-1 B by the mixed-precision Cholesky solver (the uplo triangle of
+// the SPD A is read; A is left unchanged).  Arguments and results as
+// FLA_B200_LU_piv_solve_mixed; a non-positive pivot of the fallback
+// factorization returns its zero-based column.
+FLA_Error FLA_B200_Chol_solve_mixed(FLA_Uplo uplo, FLA_Obj A, FLA_Obj B, FLA_Obj X, int prec, int solver, int* iter,
+                                    int* inner) {
+  ensure_init();
+  FB_REQUIRE(uplo == FLA_LOWER_TRIANGULAR || uplo == FLA_UPPER_TRIANGULAR, "FLA_B200_Chol_solve_mixed",
+             "invalid uplo value");
+  FB_REQUIRE(A.base && A.base->datatype == FLA_DOUBLE && A.m == A.n, "FLA_B200_Chol_solve_mixed",
+             "A must be a square FLA_DOUBLE matrix");
+  FB_REQUIRE(B.base && X.base && B.m == A.m && X.m == A.m && X.n == B.n, "FLA_B200_Chol_solve_mixed",
+             "B and X must be n x nrhs");
+  if (A.m == 0 || B.n == 0) return FLA_SUCCESS;
+  Staged sa, sb, sx;
+  if (stage(A, WS_STAGE_A, &sa) != FLA_SUCCESS || stage(B, WS_STAGE_B, &sb) != FLA_SUCCESS ||
+      stage(X, WS_STAGE_X, &sx, false) != FLA_SUCCESS)
+    return FLA_FAILURE;
+  int it = 0, inn = 0, inf = 0;
+  op_begin(ctx().stream);
+  op_hold(true);
+  const int r = mixed_solve_dev(true, uplo == FLA_UPPER_TRIANGULAR, to_dmat(sa), to_dmat(sb), to_dmat(sx), nullptr,
+                                config_from(prec, solver), false, &it, &inn, &inf);
+  op_hold(false);
+  if (r != FLA_SUCCESS) return FLA_FAILURE;
+  if (unstage(sx) != FLA_SUCCESS) return FLA_FAILURE;
+  op_end(ctx().stream);
+  if (sync_all() != FLA_SUCCESS) return FLA_FAILURE;
+  if (iter) *iter = it;
+  if (inner) *inner = inn;
+  return inf > 0 ? inf - 1 : FLA_SUCCESS;
 }
 
 }  // extern "C"

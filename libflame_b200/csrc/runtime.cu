@@ -99,7 +99,14 @@ static size_t g_prof_used = 0;
 static double g_prof_ms[PROF_NCLASS], g_prof_flops[PROF_NCLASS];
 static unsigned long long g_prof_n[PROF_NCLASS];
 
+// While an enclosing driver holds the op window (op_hold), the op_begin /
+// op_end / collection of the drivers it calls are no-ops, so the window
+// spans the whole enclosing call.
+static bool g_op_hold = false;
+void op_hold(bool on) { g_op_hold = on; }
+
 void op_begin(cudaStream_t st) {
+  if (g_op_hold) return;
   if (!g_op_ev[0]) {
     cudaEventCreate(&g_op_ev[0]);
     cudaEventCreate(&g_op_ev[1]);
@@ -109,12 +116,12 @@ void op_begin(cudaStream_t st) {
 }
 
 void op_end(cudaStream_t st) {
-  if (!g_op_open) return;
+  if (!g_op_open || g_op_hold) return;
   cudaEventRecord(g_op_ev[1], st);
 }
 
 static void prof_collect() {
-  if (g_op_open) {
+  if (g_op_open && !g_op_hold) {
     cudaEventSynchronize(g_op_ev[1]);
     cudaEventElapsedTime(&g_last_op_ms, g_op_ev[0], g_op_ev[1]);
     g_op_open = false;
