@@ -69,14 +69,16 @@ __global__ void transpose_scale_kernel(const double* __restrict__ A, long lda, f
 
 // F[i + j * ldf] = (float)(a(i, j) * d[i] * d[j]) for i >= j, a(i, j) from the
 // stored triangle (upper: a(i, j) = A[j + i * lda]).
+// (plus sigma on the diagonal: the shifted factorization of the retries)
 __global__ void lower_scale_kernel(const double* __restrict__ A, long lda, float* __restrict__ F, long ldf, int n,
-                                   const double* __restrict__ d, int upper) {
+                                   const double* __restrict__ d, int upper, double sigma) {
   const long total = (long)n * n;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
     const long i = e % n, j = e / n;
     if (i < j) continue;
     double a = upper ? A[j + i * lda] : A[i + j * lda];
     if (d) a *= d[i] * d[j];
+    if (i == j) a += sigma;
     F[i + j * ldf] = (float)a;
   }
 }
@@ -171,13 +173,13 @@ __global__ void scale_copy_kernel(const TI* __restrict__ X, long ldx, TO* __rest
     Y[i + c * ldy] = (TO)v;
   }
 }
-// X(i, c) += D(i, c)
+// X(i, c) += sign * D(i, c)
 __global__ void add_kernel(double* __restrict__ X, long ldx, const double* __restrict__ D, long ldd, int n,
-                           int nrhs) {
+                           int nrhs, double sign) {
   const long total = (long)n * nrhs;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
     const long i = e % n, c = e / n;
-    X[i + c * ldx] += D[i + c * ldd];
+    X[i + c * ldx] += sign * D[i + c * ldd];
   }
 }
 // out[q + c * nv] = sum_i V_q(i, c) W(i, c), V_q = V + q * vstride; grid (nrhs, nv)
@@ -264,6 +266,7 @@ struct LpWork {
   uint16_t* PB = nullptr;   // packed B-operand (n x MB)
   uint16_t* PC = nullptr;   // packed operand of the side stream (n x MB)
   uint16_t* PX = nullptr;   // packed inverse block (MB x MB)
+  long plane = 0, planeX = 0;  // LP_TF32X3: float offset of the lo planes
   double* P64 = nullptr;    // FP64 panel (MB x n)
   double* X64 = nullptr;    // FP64 inverse blocks (2 x MB x MB)
 };
@@ -272,16 +275,19 @@ int lp_workspace(long n, LpFactor* f, LpWork* w) {
   const size_t np = (size_t)std::max<long>(n, 1);
   f->ldf = (n + 3) & ~3L;
   f->F = (float*)ws_get(WS_LP0, sizeof(float) * (size_t)f->ldf * np);
-  char* p16 = (char*)ws_get(WS_LP1, sizeof(uint16_t) * (3 * (size_t)MB * np + (size_t)MB * MB) + 1024);
+  const size_t pk = lp_packed_bytes(LP_TF32X3, (long)np, MB), px = lp_packed_bytes(LP_TF32X3, MB, MB);
+  char* p16 = (char*)ws_get(WS_LP1, 3 * pk + px + 1024);
   char* p64 = (char*)ws_get(WS_LP3, sizeof(double) * ((size_t)MB * np + 2 * (size_t)MB * MB) + 1024);
   const long nblk = (n + MB - 1) / MB;
   char* pinv = (char*)ws_get(WS_LP4, sizeof(float) * 2 * (size_t)nblk * MB * MB + sizeof(double) * 2 * np +
                                          sizeof(int) * 2 * np + 1024);
   if (!f->F || !p16 || !p64 || !pinv) return FLA_FAILURE;
   w->PA = (uint16_t*)p16;
-  w->PB = w->PA + (size_t)MB * np;
-  w->PC = w->PB + (size_t)MB * np;
-  w->PX = w->PC + (size_t)MB * np;
+  w->PB = (uint16_t*)(p16 + pk);
+  w->PC = (uint16_t*)(p16 + 2 * pk);
+  w->PX = (uint16_t*)(p16 + 3 * pk);
+  w->plane = (long)MB * (long)np;
+  w->planeX = (long)MB * MB;
   w->P64 = (double*)p64;
   w->X64 = w->P64 + (size_t)MB * np;
   f->inv1 = (float*)pinv;
@@ -344,7 +350,7 @@ int lp_lu_factor(DMat A, LowPrec prec, bool scale, LpFactor* f) {
     if (convert2d<float, double>(s, X64, MB, f->inv1 + kb * MB * MB, MB, b, b) != FLA_SUCCESS) return FLA_FAILURE;
     if (convert2d<float, double>(s, Y64, MB, f->inv2 + kb * MB * MB, MB, b, b) != FLA_SUCCESS) return FLA_FAILURE;
     // B operand of U12^T := A12^T inv(L11^T): B(j, kk) = X64(kk, j)
-    return pack16<double>(s, prec, X64, MB, 1, w.PX, MB, b, b, 1.f);
+    return pack16<double>(s, prec, X64, MB, 1, w.PX, MB, b, b, 1.f, w.planeX);
   };
 
   cudaEvent_t ev_look = cx.ev[0], ev_panel = cx.ev[1];
@@ -356,21 +362,27 @@ int lp_lu_factor(DMat A, LowPrec prec, bool scale, LpFactor* f) {
       return FLA_FAILURE;
     if (nr <= 0) continue;
     // U12^T := A12^T inv(L11^T); A12^T(i, kk) = at(k + kk, k + b + i)
-    if (pack16<float>(st, prec, at(k, k + b), 1, ldf, w.PA, MB, nr, b, 1.f) != FLA_SUCCESS) return FLA_FAILURE;
-    if (lp_gemm(st, prec, nr, b, b, 1.f, w.PA, MB, w.PX, MB, 0.f, at(k, k + b), ldf) != FLA_SUCCESS)
+    if (pack16<float>(st, prec, at(k, k + b), 1, ldf, w.PA, MB, nr, b, 1.f, w.plane) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    if (lp_gemm(st, prec, nr, b, b, 1.f, w.PA, MB, w.PX, MB, 0.f, at(k, k + b), ldf, GEMM_FULL, 0, nullptr, INT_MAX,
+                w.plane, w.planeX) != FLA_SUCCESS)
       return FLA_FAILURE;
     // trailing update  A22^T -= U12^T A21^T
-    if (pack16<float>(st, prec, at(k, k + b), 1, ldf, w.PA, MB, nr, b, 1.f) != FLA_SUCCESS) return FLA_FAILURE;
-    if (pack16<float>(st, prec, at(k + b, k), ldf, 1, w.PB, MB, nr, b, 1.f) != FLA_SUCCESS) return FLA_FAILURE;
+    if (pack16<float>(st, prec, at(k, k + b), 1, ldf, w.PA, MB, nr, b, 1.f, w.plane) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    if (pack16<float>(st, prec, at(k + b, k), ldf, 1, w.PB, MB, nr, b, 1.f, w.plane) != FLA_SUCCESS)
+      return FLA_FAILURE;
     const int nb2 = (int)std::min<long>(MB, nr);
-    if (lp_gemm(st, prec, nb2, nr, b, -1.f, w.PA, MB, w.PB, MB, 1.f, at(k + b, k + b), ldf) != FLA_SUCCESS)
+    if (lp_gemm(st, prec, nb2, nr, b, -1.f, w.PA, MB, w.PB, MB, 1.f, at(k + b, k + b), ldf, GEMM_FULL, 0, nullptr,
+                INT_MAX, w.plane, w.plane) != FLA_SUCCESS)
       return FLA_FAILURE;
     FB_CK(cudaEventRecord(ev_look, st));
     FB_CK(cudaStreamWaitEvent(sd, ev_look, 0));
     if (panel(k + b, sd) != FLA_SUCCESS) return FLA_FAILURE;
     FB_CK(cudaEventRecord(ev_panel, sd));
-    if (nr > nb2 && lp_gemm(st, prec, nr - nb2, nr, b, -1.f, w.PA + (size_t)nb2 * MB, MB, w.PB, MB, 1.f,
-                            at(k + b, k + b + nb2), ldf) != FLA_SUCCESS)
+    if (nr > nb2 && lp_gemm(st, prec, nr - nb2, nr, b, -1.f, lp_off(w.PA, prec, (size_t)nb2 * MB), MB, w.PB, MB,
+                            1.f, at(k + b, k + b + nb2), ldf, GEMM_FULL, 0, nullptr, INT_MAX, w.plane,
+                            w.plane) != FLA_SUCCESS)
       return FLA_FAILURE;
     FB_CK(cudaStreamWaitEvent(st, ev_panel, 0));
   }
@@ -389,7 +401,7 @@ int lp_lu_factor(DMat A, LowPrec prec, bool scale, LpFactor* f) {
 }
 
 // Cholesky of diag(d) A diag(d) in low precision; F holds L (lower, FP32).
-int lp_chol_factor(DMat A, bool upper, LowPrec prec, bool scale, LpFactor* f) {
+int lp_chol_factor_shift(DMat A, bool upper, LowPrec prec, bool scale, double sigma, LpFactor* f) {
   Context& cx = ctx();
   cudaStream_t st = cx.stream, sd = cx.side;
   const long n = A.m;
@@ -406,7 +418,7 @@ int lp_chol_factor(DMat A, bool upper, LowPrec prec, bool scale, LpFactor* f) {
     FB_CK(cudaMemcpyAsync(f->sc, f->sr, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   }
   lower_scale_kernel<<<grid_for(n * n), 256, 0, st>>>(A.p, A.ld, f->F, f->ldf, (int)n, scale ? f->sr : nullptr,
-                                                      upper ? 1 : 0);
+                                                      upper ? 1 : 0, sigma);
   count_launch();
   FB_CK(cudaGetLastError());
   float* F = f->F;
@@ -425,10 +437,11 @@ int lp_chol_factor(DMat A, bool upper, LowPrec prec, bool scale, LpFactor* f) {
     const long m2 = n - k - b;
     if (m2 <= 0) return FLA_SUCCESS;
     // A21 := A21 inv(L11)^T: B(j, kk) = inv(L11)(j, kk)
-    if (pack16<double>(s, prec, w.X64, 1, MB, w.PX, MB, b, b, 1.f) != FLA_SUCCESS) return FLA_FAILURE;
-    if (pack16<float>(s, prec, at(k + b, k), 1, ldf, w.PC, MB, m2, b, 1.f) != FLA_SUCCESS) return FLA_FAILURE;
+    if (pack16<double>(s, prec, w.X64, 1, MB, w.PX, MB, b, b, 1.f, w.planeX) != FLA_SUCCESS) return FLA_FAILURE;
+    if (pack16<float>(s, prec, at(k + b, k), 1, ldf, w.PC, MB, m2, b, 1.f, w.plane) != FLA_SUCCESS)
+      return FLA_FAILURE;
     return lp_gemm(s, prec, m2, b, b, 1.f, w.PC, MB, w.PX, MB, 0.f, at(k + b, k), ldf, GEMM_FULL, 0, info,
-                   (int)(k + b));
+                   (int)(k + b), w.plane, w.planeX);
   };
 
   cudaEvent_t ev_look = cx.ev[2], ev_panel = cx.ev[3];
@@ -439,23 +452,40 @@ int lp_chol_factor(DMat A, bool upper, LowPrec prec, bool scale, LpFactor* f) {
     if (m2 <= 0) break;
     const int lim = (int)(k + b);
     const int nb2 = (int)std::min<long>(MB, m2);
-    if (pack16<float>(st, prec, at(k + b, k), 1, ldf, w.PA, MB, m2, b, 1.f) != FLA_SUCCESS) return FLA_FAILURE;
+    if (pack16<float>(st, prec, at(k + b, k), 1, ldf, w.PA, MB, m2, b, 1.f, w.plane) != FLA_SUCCESS)
+      return FLA_FAILURE;
     if (lp_gemm(st, prec, m2, nb2, b, -1.f, w.PA, MB, w.PA, MB, 1.f, at(k + b, k + b), ldf, GEMM_LOWER, 0, info,
-                lim) != FLA_SUCCESS)
+                lim, w.plane, w.plane) != FLA_SUCCESS)
       return FLA_FAILURE;
     FB_CK(cudaEventRecord(ev_look, st));
     FB_CK(cudaStreamWaitEvent(sd, ev_look, 0));
     if (panel(k + b, sd) != FLA_SUCCESS) return FLA_FAILURE;
     FB_CK(cudaEventRecord(ev_panel, sd));
-    if (m2 > nb2 && lp_gemm(st, prec, m2 - nb2, m2 - nb2, b, -1.f, w.PA + (size_t)nb2 * MB, MB,
-                            w.PA + (size_t)nb2 * MB, MB, 1.f, at(k + b + nb2, k + b + nb2), ldf, GEMM_LOWER, 0, info,
-                            lim) != FLA_SUCCESS)
+    if (m2 > nb2 && lp_gemm(st, prec, m2 - nb2, m2 - nb2, b, -1.f, lp_off(w.PA, prec, (size_t)nb2 * MB), MB,
+                            lp_off(w.PA, prec, (size_t)nb2 * MB), MB, 1.f, at(k + b + nb2, k + b + nb2), ldf,
+                            GEMM_LOWER, 0, info, lim, w.plane, w.plane) != FLA_SUCCESS)
       return FLA_FAILURE;
     FB_CK(cudaStreamWaitEvent(st, ev_panel, 0));
   }
   int inf = -1;
   if (status_read(&inf) != FLA_SUCCESS) return FLA_FAILURE;
   f->info = inf;
+  return FLA_SUCCESS;
+}
+
+// Cholesky in low precision; when the 16-bit factorization breaks down
+// (the rounding perturbs an ill-conditioned matrix out of the SPD cone),
+// retry on the shifted diag(d) A diag(d) + sigma I with sigma = 2u, 8u, 32u,
+// 128u (u the unit roundoff of the 16-bit format): the factors then
+// precondition a nearby matrix and GMRES-IR restores the solution of A.
+int lp_chol_factor(DMat A, bool upper, LowPrec prec, bool scale, LpFactor* f) {
+  if (lp_chol_factor_shift(A, upper, prec, scale, 0.0, f) != FLA_SUCCESS) return FLA_FAILURE;
+  const double u = prec == LP_FP16 ? std::ldexp(1.0, -11) : prec == LP_BF16 ? std::ldexp(1.0, -8) : std::ldexp(1.0, -21);
+  for (int t = 0; t < 4 && f->info >= 0 && scale; ++t) {
+    const double sigma = u * std::ldexp(1.0, 2 * t + 1);
+    if (lp_chol_factor_shift(A, upper, prec, scale, sigma, f) != FLA_SUCCESS) return FLA_FAILURE;
+    f->shift = sigma;
+  }
   return FLA_SUCCESS;
 }
 
@@ -711,8 +741,25 @@ int ir_refine(const DMat& A, const DMat& B, double* X, long ldx, const LpFactor&
   if (lp_solve(f, B.p, B.ld, X, ldx, nrhs, b.T, b.Tb, st) != FLA_SUCCESS) return FLA_FAILURE;
   if (residual(A, B, X, ldx, b.R, ldn, nrhs, st) != FLA_SUCCESS) return FLA_FAILURE;
   bool ok = false;
+  static const bool trace = std::getenv("FLA_B200_IR_TRACE") != nullptr;
+  // worst column's ||r||_inf / (||A||_inf ||x||_inf), from the last converged() call
+  auto ratio = [&]() {
+    double w = 0.0;
+    for (long c = 0; c < nrhs; ++c) {
+      const double den = anrm * b.h_small[c];
+      w = std::max(w, den > 0 ? b.h_small[nrhs + c] / den : (b.h_small[nrhs + c] > 0 ? INFINITY : 0.0));
+    }
+    return w;
+  };
   if (converged(X, ldx, b.R, ldn, n, nrhs, cte, b, st, &ok) != FLA_SUCCESS) return FLA_FAILURE;
-  if (ok) return FLA_SUCCESS;
+  double last = ratio();
+  if (trace) std::fprintf(stderr, "libflame_b200 ir: step 0  r/(|A||x|) %.3e\n", last);
+  // After the dsgesv_ criterion holds, refinement goes on while each step
+  // still halves the backward error, so that X reaches the backward error
+  // of the FP64 factorization rather than the criterion's eps * sqrt(n).
+  bool met = ok;
+  int stall = 0;
+  if (met && !cfg.polish) return FLA_SUCCESS;
   for (int it = 1; it <= cfg.itermax; ++it) {
     if (cfg.solver == IR_GMRES) {
       int inner = 0;
@@ -721,14 +768,38 @@ int ir_refine(const DMat& A, const DMat& B, double* X, long ldx, const LpFactor&
     } else {
       if (lp_solve(f, b.R, ldn, b.D, ldn, nrhs, b.T, b.Tb, st) != FLA_SUCCESS) return FLA_FAILURE;
     }
-    add_kernel<<<grid_for(n * nrhs), 256, 0, st>>>(X, ldx, b.D, ldn, (int)n, (int)nrhs);
+    add_kernel<<<grid_for(n * nrhs), 256, 0, st>>>(X, ldx, b.D, ldn, (int)n, (int)nrhs, 1.0);
     count_launch();
     if (residual(A, B, X, ldx, b.R, ldn, nrhs, st) != FLA_SUCCESS) return FLA_FAILURE;
     if (converged(X, ldx, b.R, ldn, n, nrhs, cte, b, st, &ok) != FLA_SUCCESS) return FLA_FAILURE;
-    if (ok) {
+    const double now = ratio();
+    if (trace) std::fprintf(stderr, "libflame_b200 ir: step %d  r/(|A||x|) %.3e  gmres %d\n", it, now, res->inner);
+    if (met && !(now < 0.5 * last)) {
+      // no longer improving: keep the better of the last two iterates
+      if (now > last) {
+        add_kernel<<<grid_for(n * nrhs), 256, 0, st>>>(X, ldx, b.D, ldn, (int)n, (int)nrhs, -1.0);
+        count_launch();
+      }
       res->iter = it;
       return FLA_SUCCESS;
     }
+    if (ok && (!cfg.polish || met)) {
+      res->iter = it;
+      return FLA_SUCCESS;
+    }
+    if (ok) met = true;
+    // stagnation: three steps in a row without halving the backward error
+    stall = (now < 0.5 * last) ? 0 : stall + 1;
+    if (!met && stall >= 3) {
+      res->iter = -(cfg.itermax + 1);
+      res->stalled = true;
+      return FLA_SUCCESS;
+    }
+    last = std::min(last, now);
+  }
+  if (met) {
+    res->iter = cfg.itermax;
+    return FLA_SUCCESS;
   }
   res->iter = -(cfg.itermax + 1);
   return FLA_SUCCESS;
@@ -749,6 +820,7 @@ IrConfig ir_default_config() {
     const std::string s(e);
     if (s == "bf16") c.prec = LP_BF16;
     if (s == "fp16") c.prec = LP_FP16;
+    if (s == "tf32x3") c.prec = LP_TF32X3;
   }
   if (const char* e = std::getenv("FLA_B200_IR_SOLVER")) {
     const std::string s(e);

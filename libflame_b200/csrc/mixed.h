@@ -8,18 +8,20 @@ namespace fb {
 enum IrSolver : int { IR_CLASSIC = 0, IR_GMRES = 1 };
 
 struct IrConfig {
-  LowPrec prec = LP_FP16;   // 16-bit format of the tensor-core updates
+  LowPrec prec = LP_FP16;   // format of the tensor-core updates (escalates to LP_TF32X3)
   bool scale = true;        // power-of-two equilibration before rounding
   IrSolver solver = IR_GMRES;
   int itermax = 30;         // ITERMAX of dsgesv_/dsposv_
   int gmres_m = 30;         // GMRES restart length (inner iterations per step)
   double gmres_tol = 1e-8;  // inner relative residual target
+  bool polish = true;       // refine on while the backward error still halves
 };
 
 struct IrResult {
   int iter = 0;      // refinement steps (>= 0), or -31 when not converged
   int inner = 0;     // GMRES iterations in total
   double anorm = 0;  // ||A||_inf
+  bool stalled = false;  // stopped early: the backward error stopped decreasing
 };
 
 // Factors of diag(sr) A diag(sc) (LU, transposed layout) or of
@@ -38,6 +40,7 @@ struct LpFactor {
   double* sr = nullptr;   // row scaling (or the symmetric scaling)
   double* sc = nullptr;   // column scaling
   int info = -1;          // first failing column of the low-precision factorization
+  double shift = 0.0;     // Cholesky: diagonal shift of the factored matrix
 };
 
 int lp_lu_factor(DMat A, LowPrec prec, bool scale, LpFactor* f);

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstring>
+#include <vector>
 
 #include "common.h"
 #include "mixed.h"
@@ -554,35 +555,45 @@ int mixed_solve_dev(bool chol, bool upper, DMat A, DMat B, DMat X, int* d_piv, c
   *iter = 0;
   *inner = 0;
   *info = 0;
-  LpFactor f;
-  int r = chol ? lp_chol_factor(A, upper, cfg.prec, cfg.scale, &f) : lp_lu_factor(A, cfg.prec, cfg.scale, &f);
-  if (r != FLA_SUCCESS) return FLA_FAILURE;
-  bool fallback = false;
-  if (f.info >= 0) {
-    *iter = -3;
-    fallback = true;
-  } else {
-    DMat Ares = A;
-    if (chol) {
-      // the refinement's residual needs the whole symmetric matrix
-      const long ld = (n + 1) & ~1L;
-      double* S = (double*)ws_get(WS_FB, sizeof(double) * (size_t)ld * (size_t)std::max<long>(1, n));
-      if (!S) return FLA_FAILURE;
-      if (symmetrize(A, upper, S, ld, st) != FLA_SUCCESS) return FLA_FAILURE;
-      Ares.p = S;
-      Ares.ld = ld;
+  DMat Ares = A;
+  if (chol) {
+    // the refinement's residual needs the whole symmetric matrix
+    const long ld = (n + 1) & ~1L;
+    double* S = (double*)ws_get(WS_FB, sizeof(double) * (size_t)ld * (size_t)std::max<long>(1, n));
+    if (!S) return FLA_FAILURE;
+    if (symmetrize(A, upper, S, ld, st) != FLA_SUCCESS) return FLA_FAILURE;
+    Ares.p = S;
+    Ares.ld = ld;
+  }
+  // Escalation: the requested format first; if its factorization breaks
+  // down or the refinement stalls, the FP32-accurate tensor-core format
+  // (3xTF32); then the FP64 factorization.
+  int steps = 0, code = -31;
+  std::vector<LowPrec> ladder{cfg.prec};
+  if (cfg.prec != LP_TF32X3) ladder.push_back(LP_TF32X3);
+  for (LowPrec p : ladder) {
+    LpFactor f;
+    int r = chol ? lp_chol_factor(A, upper, p, cfg.scale, &f) : lp_lu_factor(A, p, cfg.scale, &f);
+    if (r != FLA_SUCCESS) return FLA_FAILURE;
+    if (f.info >= 0) {
+      code = -3;
+      continue;
     }
+    IrConfig c2 = cfg;
+    c2.prec = p;
     IrResult res;
-    if (ir_refine(Ares, B, X.p, X.ld, f, cfg, &res) != FLA_SUCCESS) return FLA_FAILURE;
-    *inner = res.inner;
+    if (ir_refine(Ares, B, X.p, X.ld, f, c2, &res) != FLA_SUCCESS) return FLA_FAILURE;
+    *inner += res.inner;
     if (res.iter >= 0) {
-      *iter = res.iter;
+      *iter = steps + res.iter;
       if (!chol) FB_CK(cudaMemcpyAsync(d_piv, f.piv, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
       return sync_all();
     }
-    *iter = res.iter;
-    fallback = true;
+    steps += cfg.itermax;
+    code = -(cfg.itermax + 1);
   }
+  *iter = code;
+  bool fallback = true;
   (void)fallback;
   // FP64 factorization (in place, or on a copy when A must stay unchanged)
   DMat Af = A;
@@ -615,6 +626,7 @@ IrConfig config_from(int prec, int solver) {
   IrConfig c = ir_default_config();
   if (prec == 0) c.prec = LP_BF16;
   if (prec == 1) c.prec = LP_FP16;
+  if (prec == 2) c.prec = LP_TF32X3;
   if (solver == 0) c.solver = IR_CLASSIC;
   if (solver == 1) c.solver = IR_GMRES;
   return c;

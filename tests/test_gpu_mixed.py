@@ -36,7 +36,7 @@ def backward_error(A, X, B):
                for c in range(B.shape[1]))
 
 
-@pytest.mark.parametrize("prec,name", [(0, "bfloat16"), (1, "float16")])
+@pytest.mark.parametrize("prec,name", [(0, "bfloat16"), (1, "float16"), (2, None)])
 @pytest.mark.parametrize("m,n,k", [(300, 200, 128), (1000, 700, 256), (64, 64, 40)])
 def test_lp_gemm_matches_rounded_product(cuda, flame, prec, name, m, n, k):
     torch = cuda
@@ -45,11 +45,14 @@ def test_lp_gemm_matches_rounded_product(cuda, flame, prec, name, m, n, k):
     B = torch.randn((k, n), dtype=torch.float32, device="cuda", generator=g).t()
     Cm = torch.randn((n, m), dtype=torch.float32, device="cuda", generator=g).t()
     C0 = Cm.clone()
-    dt = getattr(torch, name)
     rc = flame.lib().FLA_B200_lp_gemm(prec, m, n, k, -1.0, C.c_void_p(A.data_ptr()), m, C.c_void_p(B.data_ptr()), n,
                                       1.0, C.c_void_p(Cm.data_ptr()), m)
     assert rc == flame.FLA_SUCCESS, flame.last_error()
-    ref = C0.double() - A.to(dt).double() @ B.to(dt).double().t()
+    if name is None:  # 3xTF32: FP32-accurate products of the FP32 operands
+        ref = C0.double() - A.double() @ B.double().t()
+    else:
+        dt = getattr(torch, name)
+        ref = C0.double() - A.to(dt).double() @ B.to(dt).double().t()
     err = ((Cm.double() - ref).abs().max() / ref.abs().max()).item()
     assert err < 1e-5, err
 
@@ -61,7 +64,7 @@ def _oracle_lu_solution(oracle, A, B):
 
 
 @pytest.mark.parametrize("n,kappa", [(300, 1e2), (1000, 1e5)])
-@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("prec", [0, 1, 2])
 @pytest.mark.parametrize("solver", [0, 1])
 def test_lu_solve_mixed_matches_oracle(cuda, flame, oracle, n, kappa, prec, solver):
     rng = seeded(n + int(np.log10(kappa)) + 10 * prec + 100 * solver)
@@ -77,8 +80,8 @@ def test_lu_solve_mixed_matches_oracle(cuda, flame, oracle, n, kappa, prec, solv
     be, be_o = backward_error(A, X, B), backward_error(A, Xo, B)
     assert be <= max(4 * be_o, 1e-15), (be, be_o, it)
     assert rel_fro(X, Xo) <= kappa * 1e-14, (rel_fro(X, Xo), it)
-    if solver == 1 or kappa <= 1e2:
-        assert it >= 0, "refinement should converge here (iter=%d)" % it
+    # converges (after escalating to 3xTF32 when the 16-bit factors stall)
+    assert it >= 0, "refinement should converge here (iter=%d)" % it
 
 
 @pytest.mark.parametrize("n,kappa", [(300, 1e2), (1000, 1e5), (1000, 1e8)])
@@ -102,8 +105,7 @@ def test_chol_solve_mixed_matches_oracle(cuda, flame, oracle, n, kappa, uplo):
     be, be_o = backward_error(A, X, B), backward_error(A, Xo, B)
     assert be <= max(4 * be_o, 1e-15), (be, be_o, it, inner)
     assert rel_fro(X, Xo) <= kappa * 1e-14, (rel_fro(X, Xo), it)
-    if kappa <= 1e5:
-        assert it >= 0
+    assert it >= 0, (it, inner)
 
 
 def test_chol_solve_mixed_falls_back(cuda, flame, oracle):
