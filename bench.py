@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--no-ir", action="store_true")
+    ap.add_argument("--ir-n", type=int, default=16384)
     return ap.parse_args()
 
 
@@ -176,6 +178,79 @@ def measure_fp64_peak(torch, dev):
         best = min(best, e0.elapsed_time(e1))
     del a, b
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def mixed_ir_section(torch, dev, F, n, nrhs):
+    """Time-to-solution of the mixed-precision solvers (16-bit/3xTF32
+    tensor-core factorization + FP64 refinement) against the FP64 form
+    (FLA_LU_piv + FLA_LU_piv_solve, FLA_Chol + FLA_Chol_solve) on
+    A = Q diag(s) Q^T (SPD) and U diag(s) V^T (general), s log-spaced so that
+    kappa = 1e2, 1e5, 1e8; nrhs N(0,1) right-hand sides.  Both times are
+    device times of the library's own calls (CUDA events on its stream);
+    errors are normwise backward errors max_c |b - A x|_inf /
+    (|A|_inf |x|_inf + |b|_inf) and the forward difference to the FP64 form."""
+    g = torch.Generator(device=dev).manual_seed(4242)
+    Q = torch.linalg.qr(torch.randn((n, n), dtype=torch.float64, device=dev, generator=g))[0]
+    V = torch.linalg.qr(torch.randn((n, n), dtype=torch.float64, device=dev, generator=g))[0]
+    B = torch.randn((nrhs, n), dtype=torch.float64, device=dev, generator=g).t()  # column-major n x nrhs
+    X64 = torch.empty((nrhs, n), dtype=torch.float64, device=dev).t()
+    Xmx = torch.empty((nrhs, n), dtype=torch.float64, device=dev).t()
+    work = torch.empty((n, n), dtype=torch.float64, device=dev).t()
+    piv = torch.empty(n, dtype=torch.int32, device=dev)
+    vW, vp, vB, v64, vmx = F.View(work), F.View(piv), F.View(B), F.View(X64), F.View(Xmx)
+    L = F.lib()
+
+    def berr(A, X):
+        R = B - A @ X
+        an = A.abs().sum(dim=1).max()
+        return (R.abs().amax(dim=0) / (an * X.abs().amax(dim=0) + B.abs().amax(dim=0))).max().item()
+
+    out = {}
+    for kind in ("spd", "general"):
+        for kappa in (1e2, 1e5, 1e8):
+            s = torch.logspace(0, -float(np.log10(kappa)), n, dtype=torch.float64, device=dev)
+            A = (Q * s) @ (Q.t() if kind == "spd" else V.t())
+            if kind == "spd":
+                A = (A + A.t()) / 2
+            A = A.t().contiguous().t()  # column-major
+            vA = F.View(A)
+            t64 = []
+            tmx = []
+            rec = {}
+            for rep in range(2):
+                work.copy_(A)
+                torch.cuda.synchronize()
+                if kind == "spd":
+                    r1 = L.FLA_Chol(F.FLA_LOWER_TRIANGULAR, vW.obj)
+                    m1 = F.last_op_ms()
+                    r2 = L.FLA_Chol_solve(F.FLA_LOWER_TRIANGULAR, vW.obj, vB.obj, v64.obj)
+                else:
+                    r1 = L.FLA_LU_piv(vW.obj, vp.obj)
+                    m1 = F.last_op_ms()
+                    r2 = L.FLA_LU_piv_solve(vW.obj, vp.obj, vB.obj, v64.obj)
+                m2 = F.last_op_ms()
+                if r1 != F.FLA_SUCCESS or r2 != F.FLA_SUCCESS:
+                    raise RuntimeError("FP64 form failed: %d %d %s" % (r1, r2, F.last_error()))
+                t64.append(m1 + m2)
+                if kind == "spd":
+                    r, it, inner = F.chol_solve_mixed(A, B, Xmx, F.FLA_LOWER_TRIANGULAR)
+                else:
+                    r, it, inner = F.lu_piv_solve_mixed(A, B, Xmx)
+                if r != F.FLA_SUCCESS:
+                    raise RuntimeError("mixed solver failed: %d %s" % (r, F.last_error()))
+                tmx.append(F.last_op_ms())
+                rec = {"iter": it, "gmres_iters": inner}
+            f64, fmx = min(t64), min(tmx)
+            rec.update({"fp64_ms": f64, "mixed_ms": fmx, "speedup": f64 / fmx,
+                        "backward_error_fp64": berr(A, X64), "backward_error_mixed": berr(A, Xmx),
+                        "forward_diff_vs_fp64": ((Xmx - X64).norm() / X64.norm()).item()})
+            out["%s_kappa_%.0e" % (kind, kappa)] = rec
+            del A, vA
+    del Q, V, work
+    torch.cuda.empty_cache()
+    return {"workload": "n=%d, nrhs=%d, A = Q diag(s) Q^T / U diag(s) V^T, s log-spaced to kappa" % (n, nrhs),
+            "solver": "default: FP16 tensor-core factors (3xTF32 when refinement stalls) + GMRES-IR in FP64",
+            "cases": out}
 
 
 def run_ours(args, rank, world):
@@ -308,6 +383,10 @@ def run_ours(args, rank, world):
         result["secondary"] = {"FLA_Chol_n16384_fp64": {"tflops": n ** 3 / 3.0 / (cms * 1e-3) / 1e12,
                                                         "ms": cms,
                                                         "frac_of_peak": n ** 3 / 3.0 / (cms * 1e-3) / 1e12 / result["roofline"]["peak"]}}
+
+    # ---- mixed-precision refinement against the FP64 form at equal error
+    if rank == 0 and not args.no_ir:
+        result["mixed_ir"] = mixed_ir_section(torch, dev, F, args.ir_n, 32)
 
     # ---- CPU baseline: the reference's multithreaded path, bounded sample
     if rank == 0 and not args.no_cpu_baseline:

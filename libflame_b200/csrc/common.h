@@ -97,6 +97,8 @@ enum WsSlot : int {
   WS_IR2,
   WS_STAGE_X,       // staging of a third operand (solution X)
   WS_FB,            // FP64 copy for the fallback factorization / symmetric residual
+  WS_PERM,          // composed row orders of long pivot sequences
+  WS_PERM_T,        // gathered rows
   WS_NSLOTS
 };
 void* ws_get(int slot, size_t bytes);  // nullptr on allocation failure

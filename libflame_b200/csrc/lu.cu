@@ -400,11 +400,67 @@ int laswp_t_f32(float* AT, long ldt, int row0, const int* d_piv, int npiv, int c
   return laswp_t_any<float>(AT, ldt, row0, d_piv, npiv, c0, n0, c1, n1, st);
 }
 
+// Row order produced by the interchanges i <-> i + p[i], i = 0..npiv-1 (in
+// reverse order when `reverse`), on rows 0..mrows-1 of a block: src[r] is
+// the original row that ends in row r.  One thread applies the sequence to
+// the identity, in shared memory when it fits.
+__global__ void pivot_perm_kernel(const int* __restrict__ piv, int npiv, int mrows, int reverse,
+                                  int* __restrict__ src, int use_smem) {
+  extern __shared__ int sv[];
+  int* v = use_smem ? sv : src;
+  for (int i = threadIdx.x; i < mrows; i += blockDim.x) v[i] = i;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < npiv; ++q) {
+      const int i = reverse ? npiv - 1 - q : q;
+      const int t = i + piv[i];
+      const int x = v[i];
+      v[i] = v[t];
+      v[t] = x;
+    }
+  }
+  __syncthreads();
+  if (use_smem)
+    for (int i = threadIdx.x; i < mrows; i += blockDim.x) src[i] = v[i];
+}
+// T(r, c) = A(src[r], c) for the mrows x ncols block; then copied back
+__global__ void gather_rows_f64_kernel(const double* __restrict__ A, long lda, const int* __restrict__ src,
+                                       double* __restrict__ T, long ldt, int mrows, int ncols) {
+  const long total = (long)mrows * ncols;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long r = e % mrows, c = e / mrows;
+    T[r + c * ldt] = A[src[r] + c * lda];
+  }
+}
+
 int apply_pivots_dev(DMat A, const int* d_piv, int k1, int k2, bool reverse, cudaStream_t st) {
   // FLA_Apply_pivots_ln_opd_var1 (src/lapack/util/app/piv/ln/flamec/
   // FLA_Apply_pivots_ln_opt_var1.c:274-340): swap rows i and i + p[i].
-  // Pivot blocks of up to 4096 entries per launch (kernel SMEM).
-  const int chunk = 4096;
+  const int npiv = k2 - k1 + 1;
+  if (npiv <= 0 || A.n <= 0) return FLA_SUCCESS;
+  const long mrows = A.m - k1;
+  if (A.n <= 64 && npiv > LASWP_MAXP && mrows <= INT_MAX) {
+    // few columns, many interchanges (the solves): compose the whole
+    // sequence into one row order, gather the block, copy it back
+    int* src = (int*)ws_get(WS_PERM, sizeof(int) * ((size_t)mrows + 64));
+    double* T = (double*)ws_get(WS_PERM_T, sizeof(double) * (size_t)mrows * (size_t)A.n);
+    if (!src || !T) return FLA_FAILURE;
+    const size_t sb = sizeof(int) * (size_t)mrows;
+    const bool smem = sb <= 200 * 1024;
+    if (smem) cudaFuncSetAttribute(pivot_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    pivot_perm_kernel<<<1, 1024, smem ? sb : 0, st>>>(d_piv + k1, npiv, (int)mrows, reverse ? 1 : 0, src,
+                                                       smem ? 1 : 0);
+    const long total = mrows * A.n;
+    gather_rows_f64_kernel<<<(unsigned)std::min<long>(8192, (total + 255) / 256), 256, 0, st>>>(
+        A.p + k1, A.ld, src, T, mrows, (int)mrows, (int)A.n);
+    count_launch(2);
+    FB_CK(cudaGetLastError());
+    FB_CK(cudaMemcpy2DAsync(A.p + k1, sizeof(double) * A.ld, T, sizeof(double) * mrows, sizeof(double) * mrows,
+                            A.n, cudaMemcpyDeviceToDevice, st));
+    return FLA_SUCCESS;
+  }
+  // otherwise blocks of LASWP_MAXP interchanges (composed per block)
+  const int chunk = LASWP_MAXP;
   if (!reverse) {
     for (int i0 = k1; i0 <= k2; i0 += chunk) {
       int cnt = std::min(chunk, k2 - i0 + 1);
