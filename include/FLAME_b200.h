@@ -85,6 +85,33 @@ FLA_Error     FLA_B200_Chol_solve_mixed( FLA_Uplo uplo, FLA_Obj A, FLA_Obj B, FL
 int           FLA_B200_lp_gemm( int prec, long m, long n, long k, float alpha, const float* A, long lda,
                                 const float* B, long ldb, float beta, float* C, long ldc );
 
+/* ---- Batched factorizations (no counterpart in the reference) ----
+ * `count` independent matrices A[i] (device pointers, column-major, order
+ * n[i] <= 512, leading dimension lda[i]; the arrays n, A, lda, piv, B, ldb
+ * and info are host arrays) in one persistent launch, largest first.  Each
+ * matrix gets the single-matrix semantics: info[i] = FLA_SUCCESS, or the
+ * zero-based failing column (Cholesky) / first zero-pivot column (LU).
+ * nrhs in 0..8: with nrhs > 0 every B[i] (n[i] x nrhs, ldb[i], device) is
+ * overwritten in the same launch by the solution of A[i] X = B[i] (skipped
+ * for matrices that failed).  LU pivots go to piv[i] (device, n[i] ints,
+ * relative as FLA_LU_piv).  Only the lower Cholesky is provided. */
+FLA_Error     FLA_Chol_batched( FLA_Uplo uplo, int count, const int* n, double** A, const int* lda,
+                                int nrhs, double** B, const int* ldb, int* info );
+FLA_Error     FLA_LU_piv_batched( int count, const int* n, double** A, const int* lda, int** piv,
+                                  int nrhs, double** B, const int* ldb, int* info );
+FLA_Error     FLA_B200_Chol_batched_f32( int count, const int* n, float** A, const int* lda, int nrhs,
+                                         float** B, const int* ldb, int* info );
+FLA_Error     FLA_B200_LU_piv_batched_f32( int count, const int* n, float** A, const int* lda, int** piv,
+                                           int nrhs, float** B, const int* ldb, int* info );
+/* Autotuner of the batched kernels: per size bin (orders 1-32, 33-64,
+ * 65-128, 129-256, 257-512) times the panel widths 8, 16, 24, 32 on
+ * `samples` scratch matrices and keeps the fastest for later calls on this
+ * device (lu: 0 Cholesky, 1 LU; f64: 0 FP32, 1 FP64).  times (optional, 20
+ * doubles) receives the bin x width timings in ms. */
+int           FLA_B200_batched_tune( int lu, int f64, int samples, double* times );
+/* Panel width the batched kernels use for order n. */
+int           FLA_B200_batched_nb( int lu, int f64, int n );
+
 #ifdef __cplusplus
 }
 #endif

@@ -78,6 +78,16 @@ _SIGS = {
                                               C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "FLA_B200_Chol_solve_mixed": (C.c_int, [C.c_int, FLA_Obj, FLA_Obj, FLA_Obj, C.c_int, C.c_int,
                                             C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "FLA_Chol_batched": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                   C.c_void_p, C.c_void_p]),
+    "FLA_LU_piv_batched": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                     C.c_void_p, C.c_void_p]),
+    "FLA_B200_Chol_batched_f32": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                            C.c_void_p, C.c_void_p]),
+    "FLA_B200_LU_piv_batched_f32": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                              C.c_void_p, C.c_void_p, C.c_void_p]),
+    "FLA_B200_batched_tune": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "FLA_B200_batched_nb": (C.c_int, [C.c_int, C.c_int, C.c_int]),
     "FLA_B200_lp_gemm": (C.c_int, [C.c_int, C.c_long, C.c_long, C.c_long, C.c_float, C.c_void_p, C.c_long,
                                    C.c_void_p, C.c_long, C.c_float, C.c_void_p, C.c_long]),
 }
@@ -257,3 +267,37 @@ def chol_solve_mixed(A, B, X, uplo=FLA_LOWER_TRIANGULAR, prec=-1, solver=-1):
     it, inner = C.c_int(0), C.c_int(0)
     r = lib().FLA_B200_Chol_solve_mixed(uplo, vA.obj, vB.obj, vX.obj, prec, solver, C.byref(it), C.byref(inner))
     return r, it.value, inner.value
+
+
+def _ptr_array(tensors):
+    return (C.c_void_p * len(tensors))(*[t.data_ptr() for t in tensors])
+
+
+def batched(kind, mats, pivs=None, rhs=None, f32=False):
+    """Batched factorization (+ solve) of column-major CUDA tensors.
+    kind: "chol" or "lu".  mats: list of n x n tensors (column-major views);
+    pivs: list of int32 CUDA tensors (LU); rhs: list of n x nrhs tensors
+    overwritten with the solutions.  Returns (error code, info list)."""
+    import numpy as _np
+    cnt = len(mats)
+    n = _np.array([m.shape[0] for m in mats], dtype=_np.int32)
+    lda = _np.array([max(1, m.stride(1)) for m in mats], dtype=_np.int32)
+    A = _ptr_array(mats)
+    nrhs = 0 if rhs is None else rhs[0].shape[1]
+    B = _ptr_array(rhs) if rhs is not None else None
+    ldb = _np.array([max(1, b.stride(1)) for b in rhs], dtype=_np.int32) if rhs is not None else None
+    info = _np.zeros(cnt, dtype=_np.int32)
+    P = (lambda a: a.ctypes.data_as(C.c_void_p) if a is not None else None)
+    L = lib()
+    if kind == "chol":
+        if f32:
+            r = L.FLA_B200_Chol_batched_f32(cnt, P(n), A, P(lda), nrhs, B, P(ldb), P(info))
+        else:
+            r = L.FLA_Chol_batched(FLA_LOWER_TRIANGULAR, cnt, P(n), A, P(lda), nrhs, B, P(ldb), P(info))
+    else:
+        pv = _ptr_array(pivs)
+        if f32:
+            r = L.FLA_B200_LU_piv_batched_f32(cnt, P(n), A, P(lda), pv, nrhs, B, P(ldb), P(info))
+        else:
+            r = L.FLA_LU_piv_batched(cnt, P(n), A, P(lda), pv, nrhs, B, P(ldb), P(info))
+    return r, info.tolist()
