@@ -644,7 +644,8 @@ int batched_entry(bool lu, int count, const int* n, T** A, const int* lda, int**
   cudaStream_t st = ctx().stream;
   // device copies of the argument arrays
   const size_t c = (size_t)count;
-  char* m = (char*)ws_get(WS_MISC2, c * (8 * 4 + 4 * 2) + 1024);
+  // layout: A, B, piv pointers, ld, ldb (8 bytes each), n, info (4 bytes each)
+  char* m = (char*)ws_get(WS_MISC2, c * (8 * 5 + 4 * 2) + 1024);
   if (!m) return FLA_FAILURE;
   T** dA = (T**)m;
   T** dB = (T**)(m + c * 8);
