@@ -539,7 +539,8 @@ int batched_tune(bool lu, bool f64, int samples_per_bin, double* times_out) {
     cudaEventCreate(&e1);
     float best = 1e30f;
     int bestnb = t.host[hi];
-    for (int c : cands) {
+    for (int ci = 0; ci < 4; ++ci) {
+      const int c = cands[ci];
       for (int nn = lo; nn <= hi; ++nn) t.host[nn] = c;
       FB_CK(cudaMemcpy(t.dev, t.host.data(), sizeof(int) * (BMAXN + 1), cudaMemcpyHostToDevice));
       float ms = 1e30f;
@@ -557,7 +558,7 @@ int batched_tune(bool lu, bool f64, int samples_per_bin, double* times_out) {
         cudaEventElapsedTime(&x, e0, e1);
         ms = std::min(ms, x);
       }
-      if (times_out) times_out[b * 4 + (&c - cands)] = ms;
+      if (times_out) times_out[b * 4 + ci] = ms;
       if (ms < best) {
         best = ms;
         bestnb = c;
