@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--no-ir", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batch-count", type=int, default=10000)
     ap.add_argument("--ir-n", type=int, default=16384)
     return ap.parse_args()
 
@@ -253,6 +255,77 @@ def mixed_ir_section(torch, dev, F, n, nrhs):
             "cases": out}
 
 
+def batched_section(torch, dev, F, count):
+    """count matrices, orders uniform in [8, 512] (seeded): SPD A = G G^T/n + I
+    through FLA_Chol_batched + 4-RHS solve (FP64 and FP32), and U(-1,1)
+    matrices through FLA_LU_piv_batched + 4-RHS solve (FP64), each a single
+    persistent launch.  Inputs are restored from a pristine copy (one copy of
+    the flat buffer) before every timed call; time = the library's device
+    time of the call.  flops: n^3/3 + 4 n^2 * 2 (Cholesky), 2n^3/3 + 4 n^2 * 2
+    (LU) per matrix."""
+    import ctypes as C
+    rng = np.random.default_rng(2027)
+    sizes = rng.integers(8, 513, size=count).astype(np.int32)
+    nrhs = 4
+    offs = np.zeros(count + 1, dtype=np.int64)
+    offs[1:] = np.cumsum(sizes.astype(np.int64) ** 2)
+    boffs = np.zeros(count + 1, dtype=np.int64)
+    boffs[1:] = np.cumsum(sizes.astype(np.int64) * nrhs)
+    g = torch.Generator(device=dev).manual_seed(2027)
+    L = F.lib()
+    out = {"workload": "%d matrices, n ~ U{8..512} (seed 2027), 4 right-hand sides" % count}
+    flop_chol = float(np.sum(sizes.astype(np.float64) ** 3 / 3 + 8.0 * sizes.astype(np.float64) ** 2))
+    flop_lu = float(np.sum(2 * sizes.astype(np.float64) ** 3 / 3 + 8.0 * sizes.astype(np.float64) ** 2))
+    lda = sizes.copy()
+    info = np.zeros(count, dtype=np.int32)
+    P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    for kind, dt in (("chol", torch.float64), ("chol", torch.float32), ("lu", torch.float64)):
+        src = torch.empty(int(offs[-1]), dtype=dt, device=dev)
+        for nval in np.unique(sizes):
+            idx = np.nonzero(sizes == nval)[0]
+            nv = int(nval)
+            if kind == "chol":
+                G = torch.randn((len(idx), nv, nv), dtype=torch.float64, device=dev, generator=g)
+                M = G @ G.transpose(1, 2) / nv + torch.eye(nv, dtype=torch.float64, device=dev)
+            else:
+                M = torch.rand((len(idx), nv, nv), dtype=torch.float64, device=dev, generator=g) * 2 - 1
+            for q, i in enumerate(idx):
+                src[int(offs[i]):int(offs[i + 1])] = M[q].t().reshape(-1).to(dt)  # column-major
+        work = src.clone()
+        bsrc = torch.randn(int(boffs[-1]), dtype=dt, device=dev, generator=g)
+        bwork = bsrc.clone()
+        es = work.element_size()
+        A = (C.c_void_p * count)(*[work.data_ptr() + int(offs[i]) * es for i in range(count)])
+        B = (C.c_void_p * count)(*[bwork.data_ptr() + int(boffs[i]) * es for i in range(count)])
+        pivbuf = torch.empty(int(sizes.sum()), dtype=torch.int32, device=dev)
+        poffs = np.concatenate([[0], np.cumsum(sizes)])
+        PV = (C.c_void_p * count)(*[pivbuf.data_ptr() + int(poffs[i]) * 4 for i in range(count)])
+        times = []
+        for rep in range(4):
+            work.copy_(src)
+            bwork.copy_(bsrc)
+            torch.cuda.synchronize()
+            if kind == "chol" and dt == torch.float64:
+                r = L.FLA_Chol_batched(F.FLA_LOWER_TRIANGULAR, count, P(sizes), A, P(lda), nrhs, B, P(lda), P(info))
+            elif kind == "chol":
+                r = L.FLA_B200_Chol_batched_f32(count, P(sizes), A, P(lda), nrhs, B, P(lda), P(info))
+            else:
+                r = L.FLA_LU_piv_batched(count, P(sizes), A, P(lda), PV, nrhs, B, P(lda), P(info))
+            if r != F.FLA_SUCCESS:
+                raise RuntimeError("batched %s failed: %s" % (kind, F.last_error()))
+            if rep > 0:
+                times.append(F.last_op_ms())
+        ms = statistics.median(times)
+        fl = flop_chol if kind == "chol" else flop_lu
+        key = "%s_%s" % (kind, "fp64" if dt == torch.float64 else "fp32")
+        out[key] = {"ms": ms, "tflops": fl / (ms * 1e-3) / 1e12, "matrices_per_s": count / (ms * 1e-3),
+                    "failed": int((info != -1).sum())}
+        del src, work, bsrc, bwork, pivbuf
+        torch.cuda.empty_cache()
+    out["note"] = "SIMT FP64/FP32 FMA kernels (one CTA per matrix, persistent grid); tflops includes the solves"
+    return out
+
+
 def run_ours(args, rank, world):
     import ctypes as C
     import torch
@@ -387,6 +460,10 @@ def run_ours(args, rank, world):
     # ---- mixed-precision refinement against the FP64 form at equal error
     if rank == 0 and not args.no_ir:
         result["mixed_ir"] = mixed_ir_section(torch, dev, F, args.ir_n, 32)
+
+    # ---- batched factorizations + solves of many uneven matrices
+    if rank == 0 and not args.no_batched:
+        result["batched"] = batched_section(torch, dev, F, args.batch_count)
 
     # ---- CPU baseline: the reference's multithreaded path, bounded sample
     if rank == 0 and not args.no_cpu_baseline:

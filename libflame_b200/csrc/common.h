@@ -99,6 +99,8 @@ enum WsSlot : int {
   WS_FB,            // FP64 copy for the fallback factorization / symmetric residual
   WS_PERM,          // composed row orders of long pivot sequences
   WS_PERM_T,        // gathered rows
+  WS_TRINV,         // inverted diagonal blocks of the solves
+  WS_SOLVE_W,       // block of solved unknowns
   WS_NSLOTS
 };
 void* ws_get(int slot, size_t bytes);  // nullptr on allocation failure
@@ -205,6 +207,9 @@ int trsm_block(const double* T, long ldt, double* B, long ldb, int b, long n, bo
                bool trans, bool unit, cudaStream_t st);
 // X := inv(L), L b x b lower triangular (unit diagonal if unit), X ld ldx.
 int tri_inverse_lower(const double* L, long ldl, int b, bool unit, double* X, long ldx, cudaStream_t st);
+// Inverses of the 128 x 128 diagonal blocks of an n x n triangle, one
+// launch: block q into X + q*128*128 (ld 128).
+int tri_inverse_blocks(const double* T, long ldt, long n, bool lower, bool unit, double* X, cudaStream_t st);
 // X := inv(T), T b x b triangular (lower or upper; unit diagonal if unit).
 int tri_inverse(const double* T, long ldt, int b, bool lower, bool unit, double* X, long ldx, cudaStream_t st);
 // X := X inv(op(T)) ^T row by row: every row x of the m x b block X is

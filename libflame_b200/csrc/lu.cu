@@ -489,6 +489,41 @@ int trsm_left_dev(DMat T, DMat B, bool lower, bool trans, bool unit, cudaStream_
   if (n == 0 || nr == 0) return FLA_SUCCESS;
   const bool fwd = (lower != trans);
   const long nblk = (n + NBMAX - 1) / NBMAX;
+  if (nr <= 256 && n > NBMAX && tma_ok(T.p, T.ld) && tma_ok(B.p, B.ld)) {
+    // Few right-hand sides: every diagonal block's inverse in one launch,
+    // then per block X_b := op(inv(T_bb)) B_b and the update of the rows
+    // still to solve, both DMMA GEMMs (no 128-step substitution chain).
+    double* Inv = (double*)ws_get(WS_TRINV, sizeof(double) * (size_t)nblk * NBMAX * NBMAX);
+    const long ldw = NBMAX;
+    double* W = (double*)ws_get(WS_SOLVE_W, sizeof(double) * (size_t)ldw * (size_t)nr);
+    if (!Inv || !W) return FLA_FAILURE;
+    if (tri_inverse_blocks(T.p, T.ld, n, lower, unit, Inv, st) != FLA_SUCCESS) return FLA_FAILURE;
+    for (long bi = 0; bi < nblk; ++bi) {
+      const long jb = fwd ? bi * NBMAX : (nblk - 1 - bi) * NBMAX;
+      const int b = (int)std::min<long>(NBMAX, n - jb);
+      double* Bj = B.p + jb;
+      const double* Ij = Inv + (jb / NBMAX) * NBMAX * NBMAX;
+      // op(inv(T_bb)) = inv(op(T_bb))
+      if (gemm_f64(st, trans, false, b, nr, b, 1.0, Ij, NBMAX, Bj, B.ld, 0.0, W, ldw) != FLA_SUCCESS)
+        return FLA_FAILURE;
+      FB_CK(cudaMemcpy2DAsync(Bj, sizeof(double) * B.ld, W, sizeof(double) * ldw, sizeof(double) * b, nr,
+                              cudaMemcpyDeviceToDevice, st));
+      if (fwd) {
+        const long rest = n - jb - b;
+        if (rest <= 0) continue;
+        const double* Tblk = trans ? (T.p + jb + (jb + b) * T.ld) : (T.p + (jb + b) + jb * T.ld);
+        if (gemm_f64(st, trans, false, rest, nr, b, -1.0, Tblk, T.ld, W, ldw, 1.0, B.p + jb + b, B.ld) !=
+            FLA_SUCCESS)
+          return FLA_FAILURE;
+      } else {
+        if (jb == 0) continue;
+        const double* Tblk = trans ? (T.p + jb) : (T.p + jb * T.ld);
+        if (gemm_f64(st, trans, false, jb, nr, b, -1.0, Tblk, T.ld, W, ldw, 1.0, B.p, B.ld) != FLA_SUCCESS)
+          return FLA_FAILURE;
+      }
+    }
+    return FLA_SUCCESS;
+  }
   for (long bi = 0; bi < nblk; ++bi) {
     const long jb = fwd ? bi * NBMAX : (nblk - 1 - bi) * NBMAX;
     const int b = (int)std::min<long>(NBMAX, n - jb);

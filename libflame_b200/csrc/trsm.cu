@@ -111,13 +111,21 @@ __global__ void __launch_bounds__(THREADS) trsm_tile_kernel(const double* __rest
 // so the b steps cost only warp-level latency.
 constexpr int INV_WARPS = 16;
 constexpr size_t INV_SMEM = (size_t)(TB * LDT + TB) * sizeof(double);
+// Batched over the diagonal blocks of an n x n triangle: blockIdx.y = block
+// index q, T_q = T + q*TB*(1 + ldt), X_q = X + q * xstride; with gridDim.y
+// = 1 and n = b, the single b x b block.
 template <bool LOWER, bool UNIT>
 __global__ void __launch_bounds__(INV_WARPS * 32) tri_inv_kernel(const double* __restrict__ T, long ldt,
-                                                                 double* __restrict__ X, long ldx, int b) {
+                                                                 double* __restrict__ X, long ldx, int n,
+                                                                 long xstride) {
   extern __shared__ double sm[];
   double* ST = sm;             // stored triangle, ST[r + c*LDT]
   double* sd = ST + TB * LDT;  // reciprocal diagonal
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int q = blockIdx.y;
+  const int b = min(TB, n - q * TB);
+  T += (long)q * TB * (1 + ldt);
+  X += (long)q * xstride;
   for (int c = warp; c < b; c += INV_WARPS)
     for (int r = lane; r < b; r += 32)
       ST[r + c * LDT] = (LOWER ? (r >= c) : (r <= c)) ? T[r + (long)c * ldt] : 0.0;
@@ -279,11 +287,11 @@ int tri_inverse(const double* T, long ldt, int b, bool lower, bool unit, double*
     const unsigned grid = (unsigned)((b + INV_WARPS - 1) / INV_WARPS);
     const int ps = prof_begin(st);
     if (lower) {
-      if (unit) tri_inv_kernel<true, true><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, ldx, b);
-      else tri_inv_kernel<true, false><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, ldx, b);
+      if (unit) tri_inv_kernel<true, true><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, ldx, b, 0);
+      else tri_inv_kernel<true, false><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, ldx, b, 0);
     } else {
-      if (unit) tri_inv_kernel<false, true><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, ldx, b);
-      else tri_inv_kernel<false, false><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, ldx, b);
+      if (unit) tri_inv_kernel<false, true><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, ldx, b, 0);
+      else tri_inv_kernel<false, false><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, ldx, b, 0);
     }
     prof_end(ps, st, PROF_TRSM, (double)b * b * b / 3.0);
     count_launch();
@@ -302,6 +310,29 @@ int tri_inverse(const double* T, long ldt, int b, bool lower, bool unit, double*
   B.ld = ldx;
   B.m = B.n = b;
   return trsm_left_dev(Tm, B, lower, false, unit, st);
+}
+
+
+// Inverses of all 128 x 128 diagonal blocks of the n x n triangle T in one
+// launch: block q (order min(128, n - 128 q)) into X + q * 128 * 128, ld 128.
+int tri_inverse_blocks(const double* T, long ldt, long n, bool lower, bool unit, double* X, cudaStream_t st) {
+  if (n <= 0) return FLA_SUCCESS;
+  set_attrs();
+  const long nblk = (n + TB - 1) / TB;
+  dim3 grid((unsigned)((TB + INV_WARPS - 1) / INV_WARPS), (unsigned)nblk);
+  const long xs = (long)TB * TB;
+  const int ps = prof_begin(st);
+  if (lower) {
+    if (unit) tri_inv_kernel<true, true><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, TB, (int)n, xs);
+    else tri_inv_kernel<true, false><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, TB, (int)n, xs);
+  } else {
+    if (unit) tri_inv_kernel<false, true><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, TB, (int)n, xs);
+    else tri_inv_kernel<false, false><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, TB, (int)n, xs);
+  }
+  prof_end(ps, st, PROF_TRSM, (double)n * TB * TB / 3.0);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
 }
 
 }  // namespace fb
