@@ -262,8 +262,9 @@ FLA_Error FLA_Chol_solve(FLA_Uplo uplo, FLA_Obj A, FLA_Obj B, FLA_Obj X) {
   if (stage(A, WS_STAGE_A, &sa) != FLA_SUCCESS) return FLA_FAILURE;
   bool ident = same_view(B, X);
   if (stage(X, WS_STAGE_B, &sx, ident) != FLA_SUCCESS) return FLA_FAILURE;
-  if (!ident && copy_into(B, sx) != FLA_SUCCESS) return FLA_FAILURE;
   cudaStream_t st = ctx().stream;
+  op_begin(st);
+  if (!ident && copy_into(B, sx) != FLA_SUCCESS) return FLA_FAILURE;
   DMat a = to_dmat(sa), x = to_dmat(sx);
   int r;
   if (uplo == FLA_LOWER_TRIANGULAR) {
@@ -274,6 +275,7 @@ FLA_Error FLA_Chol_solve(FLA_Uplo uplo, FLA_Obj A, FLA_Obj B, FLA_Obj X) {
     if (r == FLA_SUCCESS) r = trsm_left_dev(a, x, false, false, false, st);
   }
   if (r != FLA_SUCCESS) return FLA_FAILURE;
+  op_end(st);
   if (unstage(sx) != FLA_SUCCESS || sync_all() != FLA_SUCCESS) return FLA_FAILURE;
   return FLA_SUCCESS;
 }
@@ -292,14 +294,16 @@ FLA_Error FLA_LU_piv_solve(FLA_Obj A, FLA_Obj p, FLA_Obj B, FLA_Obj X) {
   if (stage(A, WS_STAGE_A, &sa) != FLA_SUCCESS) return FLA_FAILURE;
   bool ident = same_view(B, X);
   if (stage(X, WS_STAGE_B, &sx, ident) != FLA_SUCCESS) return FLA_FAILURE;
-  if (!ident && copy_into(B, sx) != FLA_SUCCESS) return FLA_FAILURE;
   PivStage ps;
   if (piv_stage(p, (long)A.m, true, &ps) != FLA_SUCCESS) return FLA_FAILURE;
   cudaStream_t st = ctx().stream;
+  op_begin(st);
+  if (!ident && copy_into(B, sx) != FLA_SUCCESS) return FLA_FAILURE;
   DMat a = to_dmat(sa), x = to_dmat(sx);
   if (apply_pivots_dev(x, ps.dev, 0, (int)A.m - 1, false, st) != FLA_SUCCESS) return FLA_FAILURE;
   if (trsm_left_dev(a, x, true, false, true, st) != FLA_SUCCESS) return FLA_FAILURE;
   if (trsm_left_dev(a, x, false, false, false, st) != FLA_SUCCESS) return FLA_FAILURE;
+  op_end(st);
   if (unstage(sx) != FLA_SUCCESS || sync_all() != FLA_SUCCESS) return FLA_FAILURE;
   return FLA_SUCCESS;
 }
