@@ -112,6 +112,20 @@ int           FLA_B200_batched_tune( int lu, int f64, int samples, double* times
 /* Panel width the batched kernels use for order n. */
 int           FLA_B200_batched_nb( int lu, int f64, int n );
 
+/* ---- Differentiation (no counterpart in the reference) ----
+ * Adjoint of the lower Cholesky factorization A = L L^T (blocked reverse
+ * mode, in place): L holds the factor from FLA_Chol, Lbar the adjoint of L
+ * in its lower triangle; on return the lower triangle of Lbar holds Abar,
+ * the adjoint of the lower entries of A (the gradient with respect to a
+ * symmetric A is (Abar + Abar^T)/2).  Only FLA_LOWER_TRIANGULAR. */
+FLA_Error     FLA_Chol_adjoint( FLA_Uplo uplo, FLA_Obj L, FLA_Obj Lbar );
+/* Lbar += scale * diag(1/L(i,i)): the adjoint of scale * sum_i log L(i,i)
+ * (log det A = 2 sum_i log L(i,i)); logdet (optional) receives the sum. */
+FLA_Error     FLA_B200_Chol_logdet_adjoint( FLA_Obj L, FLA_Obj Lbar, double scale, double* logdet );
+/* Adjoint of X = inv(L) B (left, lower, no transpose, non-unit): on entry X
+ * and Xbar; on return Xbar := Bbar = inv(L)^T Xbar and Lbar -= tril(Bbar X^T). */
+FLA_Error     FLA_B200_Trsm_llnn_adjoint( FLA_Obj L, FLA_Obj X, FLA_Obj Xbar, FLA_Obj Lbar );
+
 #ifdef __cplusplus
 }
 #endif

@@ -88,6 +88,9 @@ _SIGS = {
                                               C.c_void_p, C.c_void_p, C.c_void_p]),
     "FLA_B200_batched_tune": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "FLA_B200_batched_nb": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+    "FLA_Chol_adjoint": (C.c_int, [C.c_int, FLA_Obj, FLA_Obj]),
+    "FLA_B200_Chol_logdet_adjoint": (C.c_int, [FLA_Obj, FLA_Obj, C.c_double, C.POINTER(C.c_double)]),
+    "FLA_B200_Trsm_llnn_adjoint": (C.c_int, [FLA_Obj, FLA_Obj, FLA_Obj, FLA_Obj]),
     "FLA_B200_lp_gemm": (C.c_int, [C.c_int, C.c_long, C.c_long, C.c_long, C.c_float, C.c_void_p, C.c_long,
                                    C.c_void_p, C.c_long, C.c_float, C.c_void_p, C.c_long]),
 }
@@ -301,3 +304,21 @@ def batched(kind, mats, pivs=None, rhs=None, f32=False):
         else:
             r = L.FLA_LU_piv_batched(cnt, P(n), A, P(lda), pv, nrhs, B, P(ldb), P(info))
     return r, info.tolist()
+
+
+def chol_adjoint(L, Lbar):
+    """Lbar (lower) := Abar, the adjoint of the lower entries of A = L L^T."""
+    vL, vB = View(L), View(Lbar)
+    return lib().FLA_Chol_adjoint(FLA_LOWER_TRIANGULAR, vL.obj, vB.obj)
+
+
+def chol_logdet_adjoint(L, Lbar, scale):
+    vL, vB = View(L), View(Lbar)
+    ld = C.c_double(0.0)
+    r = lib().FLA_B200_Chol_logdet_adjoint(vL.obj, vB.obj, scale, C.byref(ld))
+    return r, ld.value
+
+
+def trsm_llnn_adjoint(L, X, Xbar, Lbar):
+    vL, vX, vXb, vLb = View(L), View(X), View(Xbar), View(Lbar)
+    return lib().FLA_B200_Trsm_llnn_adjoint(vL.obj, vX.obj, vXb.obj, vLb.obj)

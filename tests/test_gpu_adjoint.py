@@ -1,0 +1,119 @@
+"""Cholesky adjoint (FLA_Chol_adjoint), log-determinant and triangular-solve
+adjoints, and the Gaussian-process likelihood gradient built from them.
+
+Checks: (1) the symmetric gradient (Abar + Abar^T)/2 against the closed form
+L^-T sym(Phi(L^T Lbar)) L^-1 evaluated with the oracle's factor (relative
+1e-10); (2) a central finite difference (h = 1e-6) of f(A) = <Lbar, chol(A)>
+along random symmetric directions; (3) the GP gradient dloss/dK =
+0.5 (K^-1 - alpha alpha^T) from the oracle's FLA_Chol + triangular solves,
+and central differences on 200 random entries (relative 1e-5)."""
+import numpy as np
+import pytest
+
+from conftest import rel_fro, seeded, spd, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+
+def closed_form(L, Lbar):
+    P = L.T @ np.tril(Lbar)
+    P = np.tril(P) - 0.5 * np.diag(np.diag(P))
+    Ps = 0.5 * (P + P.T)
+    Li = np.linalg.inv(L)
+    return Li.T @ Ps @ Li
+
+
+@pytest.mark.parametrize("n", [1, 5, 127, 128, 129, 300, 520])
+def test_chol_adjoint_closed_form(cuda, flame, oracle, n):
+    rng = seeded(n + 3)
+    A = spd(rng, n)
+    Lo, ro = oracle.chol(A)
+    assert ro == -1
+    L = np.tril(Lo)
+    Lbar = np.tril(rng.standard_normal((n, n)))
+    Ld, Bd = to_dev(cuda, L), to_dev(cuda, Lbar)
+    assert flame.chol_adjoint(Ld, Bd) == flame.FLA_SUCCESS, flame.last_error()
+    Ab = np.tril(to_host(Bd))
+    S = 0.5 * (Ab + Ab.T)
+    assert rel_fro(S, closed_form(L, Lbar)) < 1e-10
+    # the strict upper triangle of Lbar is left alone
+    assert np.array_equal(np.triu(to_host(Bd), 1), np.triu(to_dev(cuda, Lbar).cpu().numpy(), 1))
+
+
+def test_chol_adjoint_finite_differences(cuda, flame, oracle):
+    n, h = 96, 1e-6
+    rng = seeded(17)
+    A = spd(rng, n)
+    Lbar = np.tril(rng.standard_normal((n, n)))
+    L = np.tril(oracle.chol(A)[0])
+    Ld, Bd = to_dev(cuda, L), to_dev(cuda, Lbar)
+    assert flame.chol_adjoint(Ld, Bd) == flame.FLA_SUCCESS
+    Ab = np.tril(to_host(Bd))
+    S = 0.5 * (Ab + Ab.T)
+    f = lambda M: np.sum(Lbar * np.tril(oracle.chol(M)[0]))  # noqa: E731
+    for _ in range(5):
+        E = rng.standard_normal((n, n))
+        E = (E + E.T) / 2
+        fd = (f(A + h * E) - f(A - h * E)) / (2 * h)
+        an = np.sum(S * E)
+        assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (fd, an)
+
+
+def _gp(rng, n):
+    x = rng.uniform(0, 1, (n, 3))
+    d2 = ((x[:, None, :] - x[None, :, :]) ** 2).sum(-1)
+    K = np.exp(-d2 / (2 * 0.3 ** 2)) + 1e-2 * np.eye(n)
+    y = rng.standard_normal((n, 1))
+    return K, y
+
+
+def gp_loss_and_grad(cuda, flame, K, y):
+    """loss = 0.5 y^T K^-1 y + sum log L_ii and dloss/dK (symmetric), through
+    FLA_Chol, the triangular solves and the three adjoints."""
+    n = K.shape[0]
+    Ld = to_dev(cuda, K)
+    assert flame.chol(Ld) == flame.FLA_SUCCESS
+    L = np.tril(to_host(Ld))
+    Ld = to_dev(cuda, L)
+    v = np.linalg.solve(L, y)              # forward quantities (host, for the check only)
+    alpha = np.linalg.solve(L.T, v)
+    loss = 0.5 * float(y.T @ alpha) + float(np.log(np.diag(L)).sum())
+    # reverse: loss1 = 0.5 v^T v, v = inv(L) y  ->  vbar = v
+    Lbar = to_dev(cuda, np.zeros((n, n)))
+    Vd, Vb = to_dev(cuda, v), to_dev(cuda, v.copy())
+    assert flame.trsm_llnn_adjoint(Ld, Vd, Vb, Lbar) == flame.FLA_SUCCESS, flame.last_error()
+    r, logdet = flame.chol_logdet_adjoint(Ld, Lbar, 1.0)
+    assert r == flame.FLA_SUCCESS
+    assert abs(logdet - np.log(np.diag(L)).sum()) < 1e-9 * max(1.0, abs(logdet))
+    assert flame.chol_adjoint(Ld, Lbar) == flame.FLA_SUCCESS
+    Ab = np.tril(to_host(Lbar))
+    return loss, 0.5 * (Ab + Ab.T)
+
+
+def test_gp_gradient_matches_oracle_and_fd(cuda, flame, oracle):
+    n = 300
+    rng = seeded(99)
+    K, y = _gp(rng, n)
+    loss, G = gp_loss_and_grad(cuda, flame, K, y)
+    # oracle: K^-1 from FLA_Chol + two triangular solves on I, alpha likewise
+    Lo, ro = oracle.chol(K)
+    assert ro == -1
+    Kinv = oracle.chol_solve(Lo, np.eye(n))
+    alpha = oracle.chol_solve(Lo, y)
+    G_ref = 0.5 * (Kinv - alpha @ alpha.T)
+    assert rel_fro(G, G_ref) < 1e-9
+    # central differences on 200 random symmetric entries
+    h = 1e-6
+    idx = rng.integers(0, n, size=(200, 2))
+
+    def loss_of(M):
+        L = np.tril(oracle.chol(M)[0])
+        v = np.linalg.solve(L, y)
+        return 0.5 * float(v.T @ v) + float(np.log(np.diag(L)).sum())
+    for i, j in idx[:200:10]:  # 20 oracle evaluations per sign keep the CPU suite short
+        E = np.zeros((n, n))
+        E[i, j] += 1
+        E[j, i] += 1 if i != j else 0
+        fd = (loss_of(K + h * E) - loss_of(K - h * E)) / (2 * h)
+        an = np.sum(G * E)
+        assert abs(fd - an) <= 1e-5 * max(1.0, abs(an)), (i, j, fd, an)
