@@ -29,6 +29,7 @@
 //     the refinement to condition numbers beyond 1/u of the factorization.
 #include <algorithm>
 #include <cfloat>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -751,6 +752,7 @@ int ir_refine(const DMat& A, const DMat& B, double* X, long ldx, const LpFactor&
     }
     return w;
   };
+  auto tlast = std::chrono::steady_clock::now();
   if (converged(X, ldx, b.R, ldn, n, nrhs, cte, b, st, &ok) != FLA_SUCCESS) return FLA_FAILURE;
   double last = ratio();
   if (trace) std::fprintf(stderr, "libflame_b200 ir: step 0  r/(|A||x|) %.3e\n", last);
@@ -773,7 +775,12 @@ int ir_refine(const DMat& A, const DMat& B, double* X, long ldx, const LpFactor&
     if (residual(A, B, X, ldx, b.R, ldn, nrhs, st) != FLA_SUCCESS) return FLA_FAILURE;
     if (converged(X, ldx, b.R, ldn, n, nrhs, cte, b, st, &ok) != FLA_SUCCESS) return FLA_FAILURE;
     const double now = ratio();
-    if (trace) std::fprintf(stderr, "libflame_b200 ir: step %d  r/(|A||x|) %.3e  gmres %d\n", it, now, res->inner);
+    if (trace) {
+      const auto tnow = std::chrono::steady_clock::now();
+      std::fprintf(stderr, "libflame_b200 ir: step %d  r/(|A||x|) %.3e  gmres %d  %.3f ms\n", it, now, res->inner,
+                   std::chrono::duration<double, std::milli>(tnow - tlast).count());
+      tlast = tnow;
+    }
     if (met && !(now < 0.5 * last)) {
       // no longer improving: keep the better of the last two iterates
       if (now > last) {

@@ -575,10 +575,27 @@ int mixed_solve_dev(bool chol, bool upper, DMat A, DMat B, DMat X, int* d_piv, c
   int steps = 0, code = -31;
   std::vector<LowPrec> ladder{cfg.prec};
   if (cfg.prec != LP_TF32X3) ladder.push_back(LP_TF32X3);
+  static const bool trace = std::getenv("FLA_B200_IR_TRACE") != nullptr;
   for (LowPrec p : ladder) {
     LpFactor f;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    if (trace) {
+      cudaEventCreate(&t0);
+      cudaEventCreate(&t1);
+      cudaEventRecord(t0, st);
+    }
     int r = chol ? lp_chol_factor(A, upper, p, cfg.scale, &f) : lp_lu_factor(A, p, cfg.scale, &f);
     if (r != FLA_SUCCESS) return FLA_FAILURE;
+    if (trace) {
+      cudaEventRecord(t1, st);
+      cudaEventSynchronize(t1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, t0, t1);
+      std::fprintf(stderr, "libflame_b200 ir: %s factorization in format %d: %.3f ms (info %d)\n",
+                   chol ? "Cholesky" : "LU", (int)p, ms, f.info);
+      cudaEventDestroy(t0);
+      cudaEventDestroy(t1);
+    }
     if (f.info >= 0) {
       code = -3;
       continue;

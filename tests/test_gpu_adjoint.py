@@ -77,7 +77,7 @@ def gp_loss_and_grad(cuda, flame, K, y):
     Ld = to_dev(cuda, L)
     v = np.linalg.solve(L, y)              # forward quantities (host, for the check only)
     alpha = np.linalg.solve(L.T, v)
-    loss = 0.5 * float(y.T @ alpha) + float(np.log(np.diag(L)).sum())
+    loss = 0.5 * (y.T @ alpha).item() + float(np.log(np.diag(L)).sum())
     # reverse: loss1 = 0.5 v^T v, v = inv(L) y  ->  vbar = v
     Lbar = to_dev(cuda, np.zeros((n, n)))
     Vd, Vb = to_dev(cuda, v), to_dev(cuda, v.copy())
@@ -109,7 +109,7 @@ def test_gp_gradient_matches_oracle_and_fd(cuda, flame, oracle):
     def loss_of(M):
         L = np.tril(oracle.chol(M)[0])
         v = np.linalg.solve(L, y)
-        return 0.5 * float(v.T @ v) + float(np.log(np.diag(L)).sum())
+        return 0.5 * (v.T @ v).item() + float(np.log(np.diag(L)).sum())
     for i, j in idx[:200:10]:  # 20 oracle evaluations per sign keep the CPU suite short
         E = np.zeros((n, n))
         E[i, j] += 1
