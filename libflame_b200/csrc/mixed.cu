@@ -253,6 +253,56 @@ __global__ void gather_rows_kernel(const double* __restrict__ R, long ldr, const
   }
 }
 
+// One block step of a blocked triangular sweep with the inverted diagonal
+// block (FP32, nr <= 32 right-hand sides):
+//   Xb := op(Inv) Yin(b0 : b0+w, :)         (every CTA forms it; CTA 0 stores it
+//                                            into Xout(b0 : b0+w, :))
+//   Yin(r, :) -= op(F)(r, b0 : b0+w) Xb      for r in [r_lo, r_hi), 64 rows per CTA
+// op(Inv)(i, k) = Inv[k + i * 128] when TI (else Inv[i + k * 128]);
+// op(F)(r, b0 + k) = F[(b0 + k) + r * ldf] when TF (else F[r + (b0 + k) * ldf]).
+// The solved block goes to a second buffer, so no CTA reads rows another
+// CTA of the same launch writes.
+template <bool TI, bool TF>
+__global__ void __launch_bounds__(256) solve_step_kernel(const float* __restrict__ F, long ldf,
+                                                         const float* __restrict__ Inv, float* __restrict__ Yin,
+                                                         float* __restrict__ Xout, long ldy, int nr, int b0, int w,
+                                                         int r_lo, int r_hi) {
+  __shared__ float sY[128][33];
+  __shared__ float sX[128][33];
+  const int tid = threadIdx.x;
+  for (int e = tid; e < w * nr; e += 256) {
+    const int i = e % w, c = e / w;
+    sY[i][c] = Yin[(long)(b0 + i) + (long)c * ldy];
+  }
+  __syncthreads();
+  for (int e = tid; e < w * nr; e += 256) {
+    const int i = e % w, c = e / w;
+    float s = 0.f;
+    for (int k = 0; k < w; ++k) s = fmaf(TI ? Inv[k + i * 128] : Inv[i + k * 128], sY[k][c], s);
+    sX[i][c] = s;
+  }
+  __syncthreads();
+  if (blockIdx.x == 0)
+    for (int e = tid; e < w * nr; e += 256) {
+      const int i = e % w, c = e / w;
+      Xout[(long)(b0 + i) + (long)c * ldy] = sX[i][c];
+    }
+  const int r = r_lo + blockIdx.x * 64 + (tid & 63);
+  const int cg = tid >> 6;  // 4 groups of 8 right-hand sides
+  if (r >= r_hi || cg * 8 >= nr) return;
+  float acc[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) acc[q] = 0.f;
+  for (int k = 0; k < w; ++k) {
+    const float f = TF ? F[(long)(b0 + k) + (long)r * ldf] : F[(long)r + (long)(b0 + k) * ldf];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc[q] = fmaf(f, sX[k][cg * 8 + q], acc[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q)
+    if (cg * 8 + q < nr) Yin[(long)r + (long)(cg * 8 + q) * ldy] -= acc[q];
+}
+
 inline int grid_for(long total) { return (int)std::min<long>(8192, (total + 255) / 256); }
 
 }  // namespace
@@ -509,41 +559,65 @@ int lp_solve(const LpFactor& f, const double* R, long ldr, double* D, long ldd, 
                                                                         f.scaled ? f.sr : nullptr);
   }
   count_launch();
-  // forward: L y = T
-  for (long kb = 0; kb < nblk; ++kb) {
-    const long k = kb * MB;
-    const int b = (int)std::min<long>(MB, n - k);
-    const long rest = n - k - b;
-    const float* inv = f.inv1 + kb * MB * MB;
-    // LU: inv(L11) = inv(L11^T)^T; Cholesky: inv(L11)
-    if (sgemm(st, !f.chol, false, b, nrhs, b, 1.f, inv, MB, T + k, n, 0.f, Tb, MB) != FLA_SUCCESS) return FLA_FAILURE;
-    FB_CK(cudaMemcpy2DAsync(T + k, sizeof(float) * n, Tb, sizeof(float) * MB, sizeof(float) * b, nrhs,
-                            cudaMemcpyDeviceToDevice, st));
-    if (rest > 0) {
-      if (!f.chol) {
-        // L(k+b+i, k+j) = F[(k + j) + (k + b + i) * ldf]
-        if (sgemm(st, true, false, rest, nrhs, b, -1.f, F + k + (k + b) * ldf, ldf, Tb, MB, 1.f, T + k + b, n) !=
-            FLA_SUCCESS)
-          return FLA_FAILURE;
-      } else {
-        if (sgemm(st, false, false, rest, nrhs, b, -1.f, F + (k + b) + k * ldf, ldf, Tb, MB, 1.f, T + k + b, n) !=
-            FLA_SUCCESS)
-          return FLA_FAILURE;
+  // Forward sweep L y = T (T -> Tb), backward sweep U x = y or L^T x = y
+  // (Tb -> T), one fused launch per 128-row block while nrhs <= 32.
+  if (nrhs <= 32) {
+    for (long kb = 0; kb < nblk; ++kb) {
+      const long k = kb * MB;
+      const int b = (int)std::min<long>(MB, n - k);
+      const long rest = n - k - b;
+      const unsigned g = (unsigned)std::max<long>(1, (rest + 63) / 64);
+      const float* inv = f.inv1 + kb * MB * MB;
+      // LU: inv(L11) = inv(L11^T)^T, L(r, c) = F[c + r * ldf]; Cholesky: inv(L11), L(r, c) = F[r + c * ldf]
+      if (!f.chol)
+        solve_step_kernel<true, true><<<g, 256, 0, st>>>(F, ldf, inv, T, Tb, n, (int)nrhs, (int)k, b, (int)(k + b),
+                                                         (int)n);
+      else
+        solve_step_kernel<false, false><<<g, 256, 0, st>>>(F, ldf, inv, T, Tb, n, (int)nrhs, (int)k, b, (int)(k + b),
+                                                           (int)n);
+    }
+    for (long kb = nblk - 1; kb >= 0; --kb) {
+      const long k = kb * MB;
+      const int b = (int)std::min<long>(MB, n - k);
+      const unsigned g = (unsigned)std::max<long>(1, (k + 63) / 64);
+      const float* inv = f.chol ? f.inv1 + kb * MB * MB : f.inv2 + kb * MB * MB;
+      // LU: inv(U11) = inv(U11^T)^T, U(r, c) = F[c + r * ldf]; Cholesky: inv(L11)^T, L^T(r, c) = F[c + r * ldf]
+      solve_step_kernel<true, true><<<g, 256, 0, st>>>(F, ldf, inv, Tb, T, n, (int)nrhs, (int)k, b, 0, (int)k);
+    }
+    count_launch((unsigned)(2 * nblk));
+    FB_CK(cudaGetLastError());
+  } else {
+    // wide right-hand sides: sgemm per block
+    for (long kb = 0; kb < nblk; ++kb) {
+      const long k = kb * MB;
+      const int b = (int)std::min<long>(MB, n - k);
+      const long rest = n - k - b;
+      const float* inv = f.inv1 + kb * MB * MB;
+      if (sgemm(st, !f.chol, false, b, nrhs, b, 1.f, inv, MB, T + k, n, 0.f, Tb, MB) != FLA_SUCCESS) return FLA_FAILURE;
+      FB_CK(cudaMemcpy2DAsync(T + k, sizeof(float) * n, Tb, sizeof(float) * MB, sizeof(float) * b, nrhs,
+                              cudaMemcpyDeviceToDevice, st));
+      if (rest > 0) {
+        if (!f.chol) {
+          if (sgemm(st, true, false, rest, nrhs, b, -1.f, F + k + (k + b) * ldf, ldf, Tb, MB, 1.f, T + k + b, n) !=
+              FLA_SUCCESS)
+            return FLA_FAILURE;
+        } else {
+          if (sgemm(st, false, false, rest, nrhs, b, -1.f, F + (k + b) + k * ldf, ldf, Tb, MB, 1.f, T + k + b, n) !=
+              FLA_SUCCESS)
+            return FLA_FAILURE;
+        }
       }
     }
-  }
-  // backward: U x = y (LU) or L^T x = y (Cholesky)
-  for (long kb = nblk - 1; kb >= 0; --kb) {
-    const long k = kb * MB;
-    const int b = (int)std::min<long>(MB, n - k);
-    const float* inv = f.chol ? f.inv1 + kb * MB * MB : f.inv2 + kb * MB * MB;
-    // LU: inv(U11) = inv(U11^T)^T; Cholesky: inv(L11^T) = inv(L11)^T
-    if (sgemm(st, true, false, b, nrhs, b, 1.f, inv, MB, T + k, n, 0.f, Tb, MB) != FLA_SUCCESS) return FLA_FAILURE;
-    FB_CK(cudaMemcpy2DAsync(T + k, sizeof(float) * n, Tb, sizeof(float) * MB, sizeof(float) * b, nrhs,
-                            cudaMemcpyDeviceToDevice, st));
-    if (k > 0) {
-      // LU: U(i, k + j) = F[(k + j) + i * ldf];  Cholesky: L^T(i, k + j) = F[(k + j) + i * ldf]
-      if (sgemm(st, true, false, k, nrhs, b, -1.f, F + k, ldf, Tb, MB, 1.f, T, n) != FLA_SUCCESS) return FLA_FAILURE;
+    for (long kb = nblk - 1; kb >= 0; --kb) {
+      const long k = kb * MB;
+      const int b = (int)std::min<long>(MB, n - k);
+      const float* inv = f.chol ? f.inv1 + kb * MB * MB : f.inv2 + kb * MB * MB;
+      if (sgemm(st, true, false, b, nrhs, b, 1.f, inv, MB, T + k, n, 0.f, Tb, MB) != FLA_SUCCESS) return FLA_FAILURE;
+      FB_CK(cudaMemcpy2DAsync(T + k, sizeof(float) * n, Tb, sizeof(float) * MB, sizeof(float) * b, nrhs,
+                              cudaMemcpyDeviceToDevice, st));
+      if (k > 0) {
+        if (sgemm(st, true, false, k, nrhs, b, -1.f, F + k, ldf, Tb, MB, 1.f, T, n) != FLA_SUCCESS) return FLA_FAILURE;
+      }
     }
   }
   scale_copy_kernel<double, float><<<grid_for(n * nrhs), 256, 0, st>>>(T, n, D, ldd, (int)n, (int)nrhs,
@@ -709,7 +783,7 @@ int ir_refine(const DMat& A, const DMat& B, double* X, long ldx, const LpFactor&
   const int m = std::max(1, cfg.gmres_m);
   const long ldn = (n + 1) & ~1L;  // 16-byte leading dimensions for the GEMM engine
   const size_t nb = (size_t)ldn * nrhs;
-  char* w0 = (char*)ws_get(WS_IR0, sizeof(double) * 3 * nb + sizeof(float) * (nb + (size_t)MB * nrhs) + 4096);
+  char* w0 = (char*)ws_get(WS_IR0, sizeof(double) * 3 * nb + sizeof(float) * (2 * nb + (size_t)MB * nrhs) + 4096);
   double* v = cfg.solver == IR_GMRES ? (double*)ws_get(WS_IR1, sizeof(double) * (size_t)(m + 2) * nb) : nullptr;
   char* w2 = (char*)ws_get(WS_IR2, sizeof(double) * (size_t)(m + 2) * (nrhs + 2) + 4096);
   if (!w0 || !w2 || (cfg.solver == IR_GMRES && !v)) return FLA_FAILURE;
