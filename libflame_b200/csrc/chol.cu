@@ -16,6 +16,7 @@
 // zero-based global column in the status block; every later kernel of the
 // factorization sees it and returns without touching memory.
 #include <climits>
+#include <cstdlib>
 
 #include "common.h"
 #include "dev_util.cuh"
@@ -36,74 +37,114 @@ __device__ __forceinline__ bool guard_failed(const int* info) {
 
 // Factor the b x b (b <= 128) lower-triangular diagonal block at A (ld) in
 // place.  gcol = global index of its first column (for the info word).
-__global__ void __launch_bounds__(POTRF_THREADS) potrf_diag_kernel(double* A, long ld, int b, int gcol,
+// Per 32-column step: (a) warp 0 factors the 32 x 32 diagonal block with one
+// row per lane in registers (the columns are broadcast by shuffles), (b) one
+// thread per row below solves X := X inv(L11)^T with its row in registers,
+// (c) the trailing lower triangle is updated by a 16 x 16 thread grid, each
+// thread a 6 x 6 interleaved tile (rows ty + 16a, columns tx + 16b), so the
+// shared-memory loads of one warp are broadcasts or consecutive words.
+__global__ void __launch_bounds__(POTRF_THREADS, 1) potrf_diag_kernel(double* A, long ld, int b, int gcol,
                                                                    int* info) {
   extern __shared__ double S[];  // S[r + c*LDS]
   __shared__ int s_fail;
+  __shared__ double s_rinv[IB];
+  __shared__ double s_col[IB];
   if (guard_failed(info)) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   // load lower triangle (and diagonal); upper part of S is never read
-  for (int c = warp; c < b; c += POTRF_THREADS / 32)
-    for (int r = c + lane; r < b; r += 32) S[r + c * LDS] = A[r + (long)c * ld];
+  load_block_f64<POTRF_THREADS, false>(A, ld, b, S, LDS, [](int r, int c) { return r >= c; });
   if (tid == 0) s_fail = -1;
   __syncthreads();
 
   for (int jb = 0; jb < b; jb += IB) {
     const int w = min(IB, b - jb);
-    // (a) warp 0: unblocked Cholesky of the w x w diagonal block
+    // (a) unblocked Cholesky of the w x w diagonal block, row `lane` in a[].
+    //     Every update is unconditional (no divergent branches in the
+    //     chain): a lane only ever reads a[c] of its own row for c <= lane,
+    //     and entries above the diagonal or past w never reach those.
+    //     After a failing pivot the rest of the block is not meaningful;
+    //     the failing column is what is reported.
     if (warp == 0) {
-      for (int j = 0; j < w; ++j) {
-        double d = 0.0;
-        int bad = 0;
-        if (lane == j) {
-          d = S[(jb + j) + (jb + j) * LDS];
-          if (!(d > 0.0)) bad = 1;  // <= 0 or NaN
-          else d = sqrt(d);
-        }
-        d = __shfl_sync(0xffffffffu, d, j);
-        bad = __shfl_sync(0xffffffffu, bad, j);
-        if (bad) {
-          if (lane == 0) s_fail = jb + j;
-          break;
-        }
-        if (lane == j) S[(jb + j) + (jb + j) * LDS] = d;
-        const double rinv = 1.0 / d;
-        if (lane > j && lane < w) S[(jb + lane) + (jb + j) * LDS] *= rinv;
+      double a[IB];
+#pragma unroll
+      for (int c = 0; c < IB; ++c)  // rows past w: unit pivots
+        a[c] = (c <= lane && lane < w) ? S[(jb + lane) + (jb + c) * LDS] : (c == lane ? 1.0 : 0.0);
+      int fail = -1;
+#pragma unroll
+      for (int j = 0; j < IB; ++j) {
+        const double d = __shfl_sync(0xffffffffu, a[j], j);
+        if (!(d > 0.0) && fail < 0 && j < w) fail = j;  // <= 0 or NaN
+        const double sd = sqrt(d), rinv = 1.0 / sd;
+        a[j] = lane == j ? sd : (lane > j ? a[j] * rinv : a[j]);
+        if (lane == 0) s_rinv[j] = rinv;
+        const double lj = a[j];
+        s_col[lane] = lj;
         __syncwarp();
-        if (lane > j && lane < w) {
-          const double lij = S[(jb + lane) + (jb + j) * LDS];
-          for (int c = j + 1; c <= lane; ++c)
-            S[(jb + lane) + (jb + c) * LDS] -= lij * S[(jb + c) + (jb + j) * LDS];
-        }
+#pragma unroll
+        for (int c = j + 1; c < IB; ++c) a[c] -= lj * s_col[c];
         __syncwarp();
       }
+#pragma unroll
+      for (int c = 0; c < IB; ++c)
+        if (c <= lane && lane < w) S[(jb + lane) + (jb + c) * LDS] = a[c];
+      if (lane == 0 && fail >= 0) s_fail = jb + fail;
     }
     __syncthreads();
     if (s_fail >= 0) break;
     const int r0 = jb + w;  // first row below the diagonal block
-    // (b) rows below: X := X inv(D)^T, one thread per row (right-looking,
-    //     multiply by the reciprocal of the pivot like dtrsm R,L,T,N)
+    // (b) rows below: X := X inv(L11)^T, one thread per row (right-looking,
+    //     multiply by the reciprocal of the pivot like dtrsm R,L,T,N).
+    //     Columns past w only collect values that are never stored.
     for (int r = r0 + tid; r < b; r += POTRF_THREADS) {
-      for (int j = 0; j < w; ++j) {
-        const double x = S[r + (jb + j) * LDS] * (1.0 / S[(jb + j) + (jb + j) * LDS]);
-        S[r + (jb + j) * LDS] = x;
-        for (int c = j + 1; c < w; ++c) S[r + (jb + c) * LDS] -= x * S[(jb + c) + (jb + j) * LDS];
+      double x[IB];
+#pragma unroll
+      for (int c = 0; c < IB; ++c) x[c] = c < w ? S[r + (jb + c) * LDS] : 0.0;
+#pragma unroll
+      for (int j = 0; j < IB; ++j) {
+        x[j] *= s_rinv[j];
+#pragma unroll
+        for (int c = j + 1; c < IB; ++c) x[c] -= x[j] * S[(jb + c) + (jb + j) * LDS];
       }
+#pragma unroll
+      for (int c = 0; c < IB; ++c)
+        if (c < w) S[r + (jb + c) * LDS] = x[c];
     }
     __syncthreads();
     // (c) trailing lower triangle of the block: S22 -= X X^T
     const int m2 = b - r0;
-    const int nel = m2 * (m2 + 1) / 2;
-    for (int e = tid; e < nel; e += POTRF_THREADS) {
-      // map e -> (i, c) with c <= i, column-major over the lower triangle
-      int c = (int)((2.0 * m2 + 1.0 - sqrt((2.0 * m2 + 1.0) * (2.0 * m2 + 1.0) - 8.0 * e)) * 0.5);
-      int start = c * m2 - c * (c - 1) / 2;
-      while (start > e) { --c; start = c * m2 - c * (c - 1) / 2; }
-      while (start + (m2 - c) <= e) { start += m2 - c; ++c; }
-      const int i = c + (e - start);
-      double s = 0.0;
-      for (int j = 0; j < w; ++j) s += S[(r0 + i) + (jb + j) * LDS] * S[(r0 + c) + (jb + j) * LDS];
-      S[(r0 + i) + (r0 + c) * LDS] -= s;
+    if (m2 > 0) {
+      const int tx = tid & 15, ty = tid >> 4;
+      double acc[6][6];
+#pragma unroll
+      for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int j = 0; j < 6; ++j) acc[i][j] = 0.0;
+      int ri[6], ci[6];
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        ri[i] = min(r0 + ty + 16 * i, b - 1);
+        ci[i] = min(r0 + tx + 16 * i, b - 1);
+      }
+      for (int k = 0; k < w; ++k) {
+        const double* col = S + (jb + k) * LDS;
+        double xr[6], xc[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+          xr[i] = col[ri[i]];
+          xc[i] = col[ci[i]];
+        }
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+#pragma unroll
+          for (int j = 0; j < 6; ++j) acc[i][j] += xr[i] * xc[j];
+      }
+#pragma unroll
+      for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+          const int r = r0 + ty + 16 * i, c = r0 + tx + 16 * j;
+          if (r < b && c <= r) S[r + c * LDS] -= acc[i][j];
+        }
     }
     __syncthreads();
   }
@@ -122,13 +163,31 @@ void set_attrs() {
 
 }  // namespace
 
+// Outer blocksize of FLA_Chol: the depth of the trailing updates.  256 by
+// default (the DMMA GEMM runs its K=256 updates about a fifth faster than
+// K=128 ones); FLA_B200_CHOL_BLOCKSIZE = 128 or 256 overrides it.
+int chol_blocksize() {
+  static int nb = 0;
+  if (nb == 0) {
+    nb = 256;
+    if (const char* e = std::getenv("FLA_B200_CHOL_BLOCKSIZE")) {
+      const int v = std::atoi(e);
+      if (v == 128 || v == 256) nb = v;
+    }
+  }
+  return nb;
+}
+
 // Enqueue the blocked factorization of the lower triangle of A on `st`, with
-// a lookahead of one panel when `st` is the library's main stream:
-//   panel k (side stream):  A11 := chol(A11); inv(L11) formed next to it;
-//                           A21 := A21 inv(L11)^T as a DMMA GEMM
-//   main stream, step k:    A22(:, next panel) -= A21 A21(next rows)^T,
-//                           then the next panel goes to the side stream,
-//                           A22(rest) -= A21 A21^T (lower) concurrently.
+// a lookahead of one panel when `st` is the library's main stream.  Outer
+// blocks of NBO = 128 or 256 columns; each outer panel is factored as
+// 128-column sub-panels:
+//   sub-panel j (side stream): A11 := chol(A11); inv(L11) formed next to it;
+//                              A21 := A21 inv(L11)^T as a DMMA GEMM;
+//                              the panel's later columns -= A21 A21^T
+//   main stream, step k:       A22(:, next panel) -= A21 A21(next rows)^T,
+//                              then the next panel goes to the side stream,
+//                              A22(rest) -= A21 A21^T (lower) concurrently.
 // Failure semantics follow FLA_Chol_l_blk_var3: the updates of step k run
 // unless a column before k + b has failed (the guard limit of each launch),
 // so a failure in the next panel does not cut short step k's update.
@@ -140,14 +199,16 @@ int chol_lower_enqueue(DMat A, cudaStream_t st) {
   int* info = cx.d_status + ST_INFO;
   const bool lookahead = (st == cx.stream);
   cudaStream_t sd = lookahead ? cx.side : st;
+  const long NBO = chol_blocksize();
   double* Linv = (double*)ws_get(WS_MISC, sizeof(double) * NB * NB);
   double* W = (double*)ws_get(WS_MISC2, sizeof(double) * NB * (size_t)(std::max<long>(0, n - NB) + 2));
   if (!Linv || !W) return FLA_FAILURE;
   cudaEvent_t ev_look = cx.ev[2], ev_panel = cx.ev[3];
   auto at = [&](long i, long j) { return A.p + i + j * ld; };
 
-  // Panel k: diagonal block, its inverse, and the block column below it.
-  auto panel = [&](long k, cudaStream_t s) -> int {
+  // 128-column sub-panel at column k: diagonal block, its inverse, and the
+  // block column below it.
+  auto sub = [&](long k, cudaStream_t s) -> int {
     const int b = (int)std::min<long>(NB, n - k);
     int ps = prof_begin(s);
     potrf_diag_kernel<<<1, POTRF_THREADS, POTRF_SMEM, s>>>(at(k, k), ld, b, (int)k, info);
@@ -164,14 +225,28 @@ int chol_lower_enqueue(DMat A, cudaStream_t st) {
     return gemm_f64(s, false, true, m2, b, b, 1.0, W, ldw, Linv, ldl, 0.0, at(k + b, k), ld, GEMM_FULL, 0, info,
                     (int)(k + b));
   };
+  // Outer panel at column k: its sub-panels left to right, each followed by
+  // the update of the panel's remaining columns.
+  auto panel = [&](long k, cudaStream_t s) -> int {
+    const long kend = std::min<long>(n, k + NBO);
+    for (long j = k; j < kend; j += NB) {
+      if (sub(j, s) != FLA_SUCCESS) return FLA_FAILURE;
+      const long bj = std::min<long>(NB, n - j), j2 = j + bj;
+      if (j2 >= kend) break;
+      if (gemm_f64(s, false, true, n - j2, kend - j2, bj, -1.0, at(j2, j), ld, at(j2, j), ld, 1.0, at(j2, j2), ld,
+                   GEMM_LOWER, 0, info, (int)j2) != FLA_SUCCESS)
+        return FLA_FAILURE;
+    }
+    return FLA_SUCCESS;
+  };
 
   if (panel(0, st) != FLA_SUCCESS) return FLA_FAILURE;
-  for (long k = 0; k < n; k += NB) {
-    const int b = (int)std::min<long>(NB, n - k);
+  for (long k = 0; k < n; k += NBO) {
+    const long b = std::min<long>(NBO, n - k);
     const long m2 = n - k - b;
     if (m2 <= 0) break;
     const int lim = (int)(k + b);
-    const int nb2 = (int)std::min<long>(NB, m2);
+    const long nb2 = std::min<long>(NBO, m2);
     // the next panel's columns first
     if (gemm_f64(st, false, true, m2, nb2, b, -1.0, at(k + b, k), ld, at(k + b, k), ld, 1.0, at(k + b, k + b), ld,
                  GEMM_LOWER, 0, info, lim) != FLA_SUCCESS)

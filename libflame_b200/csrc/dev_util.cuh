@@ -123,3 +123,35 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* counter, unsigned int
 }
 
 }  // namespace fb
+
+namespace fb {
+
+// Copy the b x b (b <= 128) block at A (ld) into S (stride lds) with
+// NT threads: each thread issues 16 independent loads before it stores any,
+// so the copy costs a few memory latencies instead of one per element.
+// keep(r, c) selects the elements copied; the others are written as zero
+// when zero_rest, else left alone.
+template <int NT, bool ZERO_REST, class Keep>
+__device__ __forceinline__ void load_block_f64(const double* __restrict__ A, long ld, int b, double* S, int lds,
+                                               Keep keep) {
+  constexpr int PER = 128 * 128 / NT;
+  constexpr int BATCH = PER < 16 ? PER : 16;
+#pragma unroll 1
+  for (int j0 = 0; j0 < PER; j0 += BATCH) {
+    double v[BATCH];
+#pragma unroll
+    for (int j = 0; j < BATCH; ++j) {
+      const int e = threadIdx.x + (j0 + j) * NT;
+      const int r = e & 127, c = e >> 7;
+      v[j] = (r < b && c < b && keep(r, c)) ? A[r + (long)c * ld] : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < BATCH; ++j) {
+      const int e = threadIdx.x + (j0 + j) * NT;
+      const int r = e & 127, c = e >> 7;
+      if (r < b && c < b && (ZERO_REST || keep(r, c))) S[r + c * lds] = v[j];
+    }
+  }
+}
+
+}  // namespace fb

@@ -253,54 +253,116 @@ __global__ void gather_rows_kernel(const double* __restrict__ R, long ldr, const
   }
 }
 
-// One block step of a blocked triangular sweep with the inverted diagonal
-// block (FP32, nr <= 32 right-hand sides):
-//   Xb := op(Inv) Yin(b0 : b0+w, :)         (every CTA forms it; CTA 0 stores it
-//                                            into Xout(b0 : b0+w, :))
-//   Yin(r, :) -= op(F)(r, b0 : b0+w) Xb      for r in [r_lo, r_hi), 64 rows per CTA
+// One block step of a blocked triangular sweep with inverted diagonal blocks
+// (FP32, nr <= 32 right-hand sides), 128 rows per CTA:
+//   Y(r, :) -= op(F)(r, b0 : b0+w) X(b0 : b0+w, :)     r in [r_lo, r_hi)
+// and the CTA whose rows are the next diagonal block [own_lo, own_lo+wn)
+// finishes that block in place: X(own_lo + i, :) = sum_k op(Inv)(i, k) Y(own_lo + k, :).
+// The solved block of this step was written by the previous launch (or by
+// the prologue launch, w = 0), so the inverse multiply is done once per
+// block rather than by every CTA, and X and Y are separate buffers: no CTA
+// reads rows another CTA of the same launch writes.
 // op(Inv)(i, k) = Inv[k + i * 128] when TI (else Inv[i + k * 128]);
 // op(F)(r, b0 + k) = F[(b0 + k) + r * ldf] when TF (else F[r + (b0 + k) * ldf]).
-// The solved block goes to a second buffer, so no CTA reads rows another
-// CTA of the same launch writes.
+// 32-column slab of a 128-row operand, 16 values per thread: all loads are
+// issued before any is used, so one slab costs one memory latency.
+// ROWMAJ: element (i, k) at P[k + i * ld] (else P[i + k * ld]); rows i < mi,
+// columns k < mk are read, the rest are zero.
+template <bool ROWMAJ>
+__device__ __forceinline__ void slab_load(const float* __restrict__ P, long ld, int mi, int mk, float (&v)[16]) {
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const int e = threadIdx.x + j * 256;
+    const int i = ROWMAJ ? (e >> 5) : (e & 127), k = ROWMAJ ? (e & 31) : (e >> 7);
+    v[j] = (i < mi && k < mk) ? (ROWMAJ ? P[(long)k + (long)i * ld] : P[(long)i + (long)k * ld]) : 0.f;
+  }
+}
+template <bool ROWMAJ>
+__device__ __forceinline__ void slab_store(float (*sF)[33], const float (&v)[16]) {
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const int e = threadIdx.x + j * 256;
+    const int i = ROWMAJ ? (e >> 5) : (e & 127), k = ROWMAJ ? (e & 31) : (e >> 7);
+    sF[i][k] = v[j];
+  }
+}
+
+// acc(q) += sum_k sF(rr, k) sX(k0 + k, half * 16 + q), k < 32
+__device__ __forceinline__ void slab_fma(const float (*sF)[33], const float (*sX)[36], int k0, int rr, int half,
+                                         float (&acc)[16]) {
+#pragma unroll 8
+  for (int k = 0; k < 32; ++k) {
+    const float f = sF[rr][k];
+    const float4* xk = reinterpret_cast<const float4*>(&sX[k0 + k][half * 16]);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float4 x = xk[j];
+      acc[4 * j] = fmaf(f, x.x, acc[4 * j]);
+      acc[4 * j + 1] = fmaf(f, x.y, acc[4 * j + 1]);
+      acc[4 * j + 2] = fmaf(f, x.z, acc[4 * j + 2]);
+      acc[4 * j + 3] = fmaf(f, x.w, acc[4 * j + 3]);
+    }
+  }
+}
+
 template <bool TI, bool TF>
 __global__ void __launch_bounds__(256) solve_step_kernel(const float* __restrict__ F, long ldf,
-                                                         const float* __restrict__ Inv, float* __restrict__ Yin,
-                                                         float* __restrict__ Xout, long ldy, int nr, int b0, int w,
-                                                         int r_lo, int r_hi) {
-  __shared__ float sY[128][33];
-  __shared__ float sX[128][33];
+                                                         const float* __restrict__ Inv, float* __restrict__ X,
+                                                         float* __restrict__ Y, long ldy, int nr, int b0, int w,
+                                                         int r_lo, int r_hi, int own_lo, int wn) {
+  __shared__ __align__(16) float sX[128][36];  // X(b0 : b0+w, :), then the owner's updated rows
+  __shared__ float sF[128][33];                // 32-column slab of op(F) or op(Inv)
   const int tid = threadIdx.x;
-  for (int e = tid; e < w * nr; e += 256) {
-    const int i = e % w, c = e / w;
-    sY[i][c] = Yin[(long)(b0 + i) + (long)c * ldy];
+  const int rr = tid & 127, half = tid >> 7;
+  const int r0 = r_lo + blockIdx.x * 128;
+  const int r = r0 + rr;
+  float v[16];
+  // X block: element (k, c) at X[b0 + k + c * ldy]
+  slab_load<false>(X + b0, ldy, w, nr, v);
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const int e = tid + j * 256;
+    sX[e & 127][e >> 7] = v[j];
   }
+  float acc[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) acc[q] = 0.f;
+  const float* Fb = TF ? F + b0 + (long)r0 * ldf : F + r0 + (long)b0 * ldf;
+  if (w > 0) slab_load<TF>(Fb, ldf, r_hi - r0, w, v);
+  for (int k0 = 0; k0 < w; k0 += 32) {
+    __syncthreads();
+    slab_store<TF>(sF, v);
+    __syncthreads();
+    if (k0 + 32 < w) slab_load<TF>(TF ? Fb + k0 + 32 : Fb + (long)(k0 + 32) * ldf, ldf, r_hi - r0, w - k0 - 32, v);
+    slab_fma(sF, sX, k0, rr, half, acc);
+  }
+  if (r0 != own_lo) {
+    if (r < r_hi)
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+        if (half * 16 + q < nr) Y[(long)r + (long)(half * 16 + q) * ldy] -= acc[q];
+    return;
+  }
+  // owner: the next diagonal block, updated, into sX; then X := op(Inv) sX
+  slab_load<TI>(Inv, 128, wn, wn, v);
   __syncthreads();
-  for (int e = tid; e < w * nr; e += 256) {
-    const int i = e % w, c = e / w;
-    float s = 0.f;
-    for (int k = 0; k < w; ++k) s = fmaf(TI ? Inv[k + i * 128] : Inv[i + k * 128], sY[k][c], s);
-    sX[i][c] = s;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int c = half * 16 + q;
+    sX[rr][c] = (rr < wn && c < nr) ? Y[(long)r + (long)c * ldy] - acc[q] : 0.f;
+    acc[q] = 0.f;
   }
-  __syncthreads();
-  if (blockIdx.x == 0)
-    for (int e = tid; e < w * nr; e += 256) {
-      const int i = e % w, c = e / w;
-      Xout[(long)(b0 + i) + (long)c * ldy] = sX[i][c];
-    }
-  const int r = r_lo + blockIdx.x * 64 + (tid & 63);
-  const int cg = tid >> 6;  // 4 groups of 8 right-hand sides
-  if (r >= r_hi || cg * 8 >= nr) return;
-  float acc[8];
-#pragma unroll
-  for (int q = 0; q < 8; ++q) acc[q] = 0.f;
-  for (int k = 0; k < w; ++k) {
-    const float f = TF ? F[(long)(b0 + k) + (long)r * ldf] : F[(long)r + (long)(b0 + k) * ldf];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) acc[q] = fmaf(f, sX[k][cg * 8 + q], acc[q]);
+  for (int k0 = 0; k0 < wn; k0 += 32) {
+    __syncthreads();
+    slab_store<TI>(sF, v);
+    __syncthreads();
+    if (k0 + 32 < wn) slab_load<TI>(TI ? Inv + k0 + 32 : Inv + (long)(k0 + 32) * 128, 128, wn, wn - k0 - 32, v);
+    slab_fma(sF, sX, k0, rr, half, acc);
   }
+  if (rr < wn)
 #pragma unroll
-  for (int q = 0; q < 8; ++q)
-    if (cg * 8 + q < nr) Yin[(long)r + (long)(cg * 8 + q) * ldy] -= acc[q];
+    for (int q = 0; q < 16; ++q)
+      if (half * 16 + q < nr) X[(long)r + (long)(half * 16 + q) * ldy] = acc[q];
 }
 
 inline int grid_for(long total) { return (int)std::min<long>(8192, (total + 255) / 256); }
@@ -562,27 +624,39 @@ int lp_solve(const LpFactor& f, const double* R, long ldr, double* D, long ldd, 
   // Forward sweep L y = T (T -> Tb), backward sweep U x = y or L^T x = y
   // (Tb -> T), one fused launch per 128-row block while nrhs <= 32.
   if (nrhs <= 32) {
-    for (long kb = 0; kb < nblk; ++kb) {
-      const long k = kb * MB;
-      const int b = (int)std::min<long>(MB, n - k);
-      const long rest = n - k - b;
-      const unsigned g = (unsigned)std::max<long>(1, (rest + 63) / 64);
-      const float* inv = f.inv1 + kb * MB * MB;
-      // LU: inv(L11) = inv(L11^T)^T, L(r, c) = F[c + r * ldf]; Cholesky: inv(L11), L(r, c) = F[r + c * ldf]
+    auto blk = [&](long kb) { return std::make_pair(kb * MB, (int)std::min<long>(MB, n - kb * MB)); };
+    // LU: inv(L11) = inv(L11^T)^T, L(r, c) = F[c + r * ldf]; Cholesky: inv(L11), L(r, c) = F[r + c * ldf]
+    auto fwd = [&](long kb, int w, long r_lo, long r_hi, long own) {
+      const unsigned g = (unsigned)std::max<long>(1, (r_hi - r_lo + 127) / 128);
+      const auto nx = blk(own / MB);
+      const float* inv = f.inv1 + (own / MB) * MB * MB;
       if (!f.chol)
-        solve_step_kernel<true, true><<<g, 256, 0, st>>>(F, ldf, inv, T, Tb, n, (int)nrhs, (int)k, b, (int)(k + b),
-                                                         (int)n);
+        solve_step_kernel<true, true><<<g, 256, 0, st>>>(F, ldf, inv, Tb, T, n, (int)nrhs, (int)(kb * MB), w,
+                                                         (int)r_lo, (int)r_hi, (int)own, nx.second);
       else
-        solve_step_kernel<false, false><<<g, 256, 0, st>>>(F, ldf, inv, T, Tb, n, (int)nrhs, (int)k, b, (int)(k + b),
-                                                           (int)n);
+        solve_step_kernel<false, false><<<g, 256, 0, st>>>(F, ldf, inv, Tb, T, n, (int)nrhs, (int)(kb * MB), w,
+                                                           (int)r_lo, (int)r_hi, (int)own, nx.second);
+    };
+    // Forward sweep L y = T: y into Tb block by block
+    fwd(0, 0, 0, blk(0).second, 0);
+    for (long kb = 0; kb + 1 < nblk; ++kb) {
+      const auto c = blk(kb);
+      fwd(kb, c.second, c.first + c.second, n, c.first + c.second);
     }
-    for (long kb = nblk - 1; kb >= 0; --kb) {
-      const long k = kb * MB;
-      const int b = (int)std::min<long>(MB, n - k);
-      const unsigned g = (unsigned)std::max<long>(1, (k + 63) / 64);
-      const float* inv = f.chol ? f.inv1 + kb * MB * MB : f.inv2 + kb * MB * MB;
-      // LU: inv(U11) = inv(U11^T)^T, U(r, c) = F[c + r * ldf]; Cholesky: inv(L11)^T, L^T(r, c) = F[c + r * ldf]
-      solve_step_kernel<true, true><<<g, 256, 0, st>>>(F, ldf, inv, Tb, T, n, (int)nrhs, (int)k, b, 0, (int)k);
+    // Backward sweep U x = y or L^T x = y: Tb is updated, x into T.
+    // LU: inv(U11) = inv(U11^T)^T, U(r, c) = F[c + r * ldf]; Cholesky: inv(L11)^T, L^T(r, c) = F[c + r * ldf]
+    auto bwd = [&](long kb, int w, long r_lo, long r_hi, long own) {
+      const unsigned g = (unsigned)std::max<long>(1, (r_hi - r_lo + 127) / 128);
+      const auto nx = blk(own / MB);
+      const float* inv = (f.chol ? f.inv1 : f.inv2) + (own / MB) * MB * MB;
+      solve_step_kernel<true, true><<<g, 256, 0, st>>>(F, ldf, inv, T, Tb, n, (int)nrhs, (int)(kb * MB), w,
+                                                       (int)r_lo, (int)r_hi, (int)own, nx.second);
+    };
+    const auto last = blk(nblk - 1);
+    bwd(nblk - 1, 0, last.first, n, last.first);
+    for (long kb = nblk - 1; kb >= 1; --kb) {
+      const auto c = blk(kb);
+      bwd(kb, c.second, 0, c.first, c.first - MB);
     }
     count_launch((unsigned)(2 * nblk));
     FB_CK(cudaGetLastError());

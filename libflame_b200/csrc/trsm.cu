@@ -19,6 +19,7 @@
 #include <algorithm>
 
 #include "common.h"
+#include "dev_util.cuh"
 
 namespace fb {
 
@@ -51,9 +52,7 @@ __global__ void __launch_bounds__(THREADS) trsm_tile_kernel(const double* __rest
   const int tid = threadIdx.x;
   const int v0 = blockIdx.x * NV;
   const int nv = min(NV, nvec - v0);
-  for (int c = tid >> 5; c < b; c += THREADS / 32)
-    for (int r = tid & 31; r < b; r += 32)
-      ST[r + c * LDT] = (LOWER ? (r >= c) : (r <= c)) ? T[r + (long)c * ldt] : 0.0;
+  load_block_f64<THREADS, true>(T, ldt, b, ST, LDT, [](int r, int c) { return LOWER ? (r >= c) : (r <= c); });
   // right-hand side v, unknown r: left -> X(r, v0+v); right -> X(v0+v, r)
   if (!RIGHT) {
     for (int v = tid >> 5; v < nv; v += THREADS / 32)
@@ -126,9 +125,7 @@ __global__ void __launch_bounds__(INV_WARPS * 32) tri_inv_kernel(const double* _
   const int b = min(TB, n - q * TB);
   T += (long)q * TB * (1 + ldt);
   X += (long)q * xstride;
-  for (int c = warp; c < b; c += INV_WARPS)
-    for (int r = lane; r < b; r += 32)
-      ST[r + c * LDT] = (LOWER ? (r >= c) : (r <= c)) ? T[r + (long)c * ldt] : 0.0;
+  load_block_f64<INV_WARPS * 32, true>(T, ldt, b, ST, LDT, [](int r, int c) { return LOWER ? (r >= c) : (r <= c); });
   __syncthreads();
   if (!UNIT)
     for (int j = tid; j < b; j += INV_WARPS * 32) sd[j] = 1.0 / ST[j + j * LDT];
@@ -149,11 +146,12 @@ __global__ void __launch_bounds__(INV_WARPS * 32) tri_inv_kernel(const double* _
       if (slot == m) v = r[m];
     double xj = __shfl_sync(0xffffffffu, v, j & 31);
     if (!UNIT) xj *= sd[j];
+    // branch-free: rows outside the triangle multiply a zero of ST
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       const int i = lane + 32 * m;
-      if (i == j) r[m] = xj;
-      else if (LOWER ? (i > j && i < b) : (i < j)) r[m] -= ST[i + j * LDT] * xj;
+      const double t = r[m] - ST[i + j * LDT] * xj;
+      r[m] = (i == j) ? xj : ((LOWER ? (i > j) : (i < j)) ? t : r[m]);
     }
   }
   (void)j_last;
