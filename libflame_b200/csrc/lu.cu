@@ -25,7 +25,10 @@
 // scales its part of column j and applies the rank-1 update to its slab.
 // It serves the allocation-free single-panel entry point.
 #include <climits>
+#include <cstdio>
+#include <cstdlib>
 #include <mutex>
+#include <vector>
 
 #include "common.h"
 #include "dev_util.cuh"
@@ -606,6 +609,18 @@ int lu_piv_dev(DMat A, int* d_piv, int* info) {
   auto t_at = [&](long i, long j) { return AT + j + i * ldT; };
   if (transpose_dev(A.p, A.ld, AT, ldT, m, n, false, st) != FLA_SUCCESS) return FLA_FAILURE;
 
+  // FLA_B200_LU_TRACE: per-step event timeline (main stream: step start,
+  // lookahead done, trailing update done; side stream: panel done), summed
+  // and printed to stderr after the factorization
+  static const bool trace = std::getenv("FLA_B200_LU_TRACE") != nullptr;
+  std::vector<cudaEvent_t> tev;
+  auto tmark = [&](cudaStream_t s) {
+    if (!trace) return;
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, s);
+    tev.push_back(e);
+  };
   // first panel and its inverse triangle, on the main stream
   {
     const int b = (int)std::min<long>(NBL, mn);
@@ -615,6 +630,8 @@ int lu_piv_dev(DMat A, int* d_piv, int* info) {
   for (long k = 0; k < mn; k += NBL) {
     const int b = (int)std::min<long>(NBL, mn - k);
     const long nr = n - k - b, m2 = m - k - b;
+    const size_t tbase = tev.size();
+    tmark(st);
     if (laswp_t_dev(AT, ldT, (int)k, d_piv + k, b, 0, (int)k, (int)(k + b), (int)nr, st) != FLA_SUCCESS)
       return FLA_FAILURE;
     if (nr <= 0) continue;
@@ -631,21 +648,53 @@ int lu_piv_dev(DMat A, int* d_piv, int* info) {
                    t_at(k + b, k + b), ldT) != FLA_SUCCESS)
         return FLA_FAILURE;
       FB_CK(cudaEventRecord(ev_look, st));
+      tmark(st);
       FB_CK(cudaStreamWaitEvent(sd, ev_look, 0));
       if (lu_panel_factor_t(t_at(k + b, k + b), ldT, m2, nb2, d_piv + k + b, (int)(k + b), sd) != FLA_SUCCESS)
         return FLA_FAILURE;
       if (nr > nb2 && tri_inverse(t_at(k + b, k + b), ldT, nb2, false, true, X, even(nb2), sd) != FLA_SUCCESS)
         return FLA_FAILURE;
       FB_CK(cudaEventRecord(ev_panel, sd));
+      tmark(sd);
     }
     if (nr > nb2 &&
         gemm_f64(st, false, false, nr - nb2, m2, b, -1.0, t_at(k, k + b + nb2), ldT, t_at(k + b, k), ldT, 1.0,
                  t_at(k + b, k + b + nb2), ldT) != FLA_SUCCESS)
       return FLA_FAILURE;
+    if (nb2 > 0) {
+      tmark(st);
+      if (tev.size() != tbase + 4) tev.resize(tbase);  // incomplete step: not traced
+    }
     if (nb2 > 0) FB_CK(cudaStreamWaitEvent(st, ev_panel, 0));
   }
   if (transpose_dev(AT, ldT, A.p, A.ld, n, m, false, st) != FLA_SUCCESS) return FLA_FAILURE;
-  return status_read(info);
+  const int rs = status_read(info);
+  if (trace && !tev.empty()) {
+    // per step: [0] start, [1] lookahead done, [2] panel done, [3] trailing done
+    double serial = 0, panel = 0, trail = 0, crit = 0;
+    int panel_bound = 0;
+    const size_t steps = tev.size() / 4;
+    for (size_t q = 0; q < steps; ++q) {
+      float a = 0, p = 0, t = 0;
+      cudaEventElapsedTime(&a, tev[4 * q], tev[4 * q + 1]);
+      cudaEventElapsedTime(&p, tev[4 * q + 1], tev[4 * q + 2]);
+      cudaEventElapsedTime(&t, tev[4 * q + 1], tev[4 * q + 3]);
+      serial += a;
+      panel += p;
+      trail += t;
+      crit += a + std::max(p, t);
+      if (p > t) ++panel_bound;
+      if (q % 16 == 0 || q + 1 == steps)
+        std::fprintf(stderr, "libflame_b200 lu: step %4zu  lookahead %.3f ms  panel %.3f ms  trailing %.3f ms\n", q, a, p,
+                     t);
+    }
+    std::fprintf(stderr,
+                 "libflame_b200 lu: %zu steps: lookahead part %.2f ms, panels %.2f ms, trailing %.2f ms, "
+                 "critical %.2f ms, %d steps panel-bound\n",
+                 steps, serial, panel, trail, crit, panel_bound);
+    for (cudaEvent_t e : tev) cudaEventDestroy(e);
+  }
+  return rs;
 }
 
 }  // namespace fb

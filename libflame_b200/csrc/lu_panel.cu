@@ -92,10 +92,6 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
 
   const int r0 = c * a.R;
   const int rows = max(0, min(a.R, a.M - r0));
-  int rt_log = 5;  // log2 of the slab height rounded up to a power of two (>= 32)
-  while ((1 << rt_log) < rows && rt_log < 10) ++rt_log;
-  const int rt_mask = (1 << rt_log) - 1;
-  const int i_row0 = tid & rt_mask, cg = tid >> rt_log, cgs = LEAF_THREADS >> rt_log;
   if (RM) {
     // eight independent loads in flight per thread
     const int tot = rows * w;
@@ -124,19 +120,30 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
   }
   __syncthreads();
 
+  // Thread -> (row i = tid mod RT, column group g = tid / RT), RT the slab
+  // height rounded up to a power of two (32 .. 1024); with G = 1024 / RT
+  // groups, group g updates columns j+1+g, j+1+g+G, ... of its rows, so
+  // within a column only the candidate reduction needs a CTA barrier and
+  // the exchange one cluster barrier.  Slabs taller than 1024 rows give each
+  // thread rows i, i + 1024, ... (G = 1).  Group 0 owns column j + 1 and
+  // tracks the next candidate.
+  int rt_log = 5;
+  while ((1 << rt_log) < rows && rt_log < 10) ++rt_log;
+  const int RT = 1 << rt_log, G = LEAF_THREADS >> rt_log;
+  const int my_i = tid & (RT - 1), my_g = tid >> rt_log;
   int first_null = -1;
+  double bv = -1.0;  // this thread's candidate for the current column
+  int bi = INT_MAX;
+  if (my_g == 0)
+    for (int i = my_i; i < rows; i += RT) {
+      const double v = fabs(slab[i]);
+      const int gi = r0 + i;
+      if (v > bv || (v == bv && gi < bi)) { bv = v; bi = gi; }
+    }
   for (int j = 0; j < w; ++j) {
     const int par = j & 1;
-    // ---- 1. local candidate: max |a(i,j)| over rows i >= j, smallest row on ties
-    double bv = -1.0;
-    int bi = INT_MAX;
-    for (int i = tid; i < rows; i += LEAF_THREADS) {
-      const int gi = r0 + i;
-      if (gi >= j) {
-        const double v = fabs(slab[i + j * lds]);
-        if (v > bv || (v == bv && gi < bi)) { bv = v; bi = gi; }
-      }
-    }
+    // ---- 1. CTA candidate: max |a(i,j)| over rows i >= j, smallest row on
+    // ties (warp shuffles, then warp 0 over the warps' results)
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
       const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
@@ -154,16 +161,18 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
         const int oi = __shfl_xor_sync(0xffffffffu, i0, off);
         if (ov > v || (ov == v && oi < i0)) { v = ov; i0 = oi; }
       }
-      if (lane == 0) {
-        s_bv = v;
-        s_bi = i0;
-      }
+      if (lane == 0) { s_bv = v; s_bi = i0; }
     }
     __syncthreads();
+    bv = s_bv;
+    bi = s_bi;
+    // a thread's own a(i, j), read before group 0 overwrites it with l(i, j)
+    // (one row per thread whenever G > 1)
+    const double vj = (G > 1 && my_i < rows) ? slab[my_i + j * lds] : 0.0;
     // ---- 2. push the candidate (and row j, by its owner) to every CTA
     {
-      const int li = s_bi - r0;  // local row of the candidate (if any)
-      const bool have = s_bi != INT_MAX;
+      const int li = bi - r0;  // local row of the candidate (if any)
+      const bool have = bi != INT_MAX;
       const bool own_j = (j >= r0) && (j < r0 + rows);
       const int per = w + 1;
       for (int e = tid; e < C * per; e += LEAF_THREADS) {
@@ -172,8 +181,8 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
           double* dst = cluster.map_shared_rank(xrow + ((size_t)par * C + c) * w + q, d);
           *dst = have ? slab[li + q * lds] : 0.0;
         } else {
-          *cluster.map_shared_rank(xval + par * C + c, d) = s_bv;
-          *cluster.map_shared_rank(xidx + par * C + c, d) = s_bi;
+          *cluster.map_shared_rank(xval + par * C + c, d) = bv;
+          *cluster.map_shared_rank(xidx + par * C + c, d) = bi;
         }
       }
       if (own_j)
@@ -186,71 +195,90 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
     // ---- 3. winner (identical on every CTA: same data, same order)
     if (warp == 0) {
       double v = -2.0;
-      int i0 = INT_MAX, w0 = 0;
+      int i0 = INT_MAX, q0 = 0;
       for (int q = lane; q < C; q += 32) {
         const double cv = xval[par * C + q];
         const int ci = xidx[par * C + q];
-        if (ci != INT_MAX && (cv > v || (cv == v && ci < i0))) { v = cv; i0 = ci; w0 = q; }
+        if (ci != INT_MAX && (cv > v || (cv == v && ci < i0))) { v = cv; i0 = ci; q0 = q; }
       }
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
         const double ov = __shfl_xor_sync(0xffffffffu, v, off);
         const int oi = __shfl_xor_sync(0xffffffffu, i0, off);
-        const int ow = __shfl_xor_sync(0xffffffffu, w0, off);
-        if (ov > v || (ov == v && oi < i0)) { v = ov; i0 = oi; w0 = ow; }
+        const int oq = __shfl_xor_sync(0xffffffffu, q0, off);
+        if (ov > v || (ov == v && oi < i0)) { v = ov; i0 = oi; q0 = oq; }
       }
-      if (lane == 0) { s_wc = w0; s_r = i0; }
+      if (lane == 0) { s_wc = q0; s_r = i0; }
     }
     __syncthreads();
     int r = s_r;
-    const double* u = xrow + ((size_t)par * C + s_wc) * w;  // the pivot row
+    const int w0 = s_wc;
+    const double* u = xrow + ((size_t)par * C + w0) * w;  // the pivot row
     if (r == INT_MAX) {
       // no orderable candidate (every magnitude NaN): keep row j, as idamax
       // does when no later entry compares greater than the first
       r = j;
       u = rowj + par * w;
     }
+    const double* oldj = rowj + par * w;
     const double piv = u[j];
     if (c == 0 && tid == 0) a.piv[j] = r - j;
+    bv = -1.0;
+    bi = INT_MAX;
     if (piv == 0.0) {
+      // null column: no exchange, no scaling, no update
       if (first_null < 0) first_null = j;
-    } else {
-      if (r != j) {
-        // ---- 4. exchange rows j and r (whole leaf row)
-        if (j >= r0 && j < r0 + rows)
-          for (int q = tid; q < w; q += LEAF_THREADS) slab[(j - r0) + q * lds] = u[q];
-        if (r >= r0 && r < r0 + rows)
-          for (int q = tid; q < w; q += LEAF_THREADS) slab[(r - r0) + q * lds] = rowj[par * w + q];
-      }
-      __syncthreads();
-      // ---- 5. scale column j below the pivot (reciprocal multiply, as
-      // bl1_dinvscalv), then the rank-1 update of the slab, one element per
-      // thread and pass (rows fastest), four independent elements in flight
-      const double rinv = 1.0 / piv;
-      const int i_lo = max(0, j + 1 - r0);  // first local row below the pivot
-      for (int i = i_lo + tid; i < rows; i += LEAF_THREADS) slab[i + j * lds] *= rinv;
-      __syncthreads();
-      // thread -> (row i = tid mod RT, column group cg = tid / RT); RT is the
-      // slab height rounded up to a power of two, so no divisions
-      for (int i_row = i_row0 + max(0, ((i_lo - i_row0) + rt_mask) >> rt_log << rt_log); i_row < rows;
-           i_row += rt_mask + 1) {
-        const double l = slab[i_row + j * lds];
-        int q = j + 1 + cg;
-        for (; q + 3 * cgs < w; q += 4 * cgs) {
-          double v[4], uq[4];
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            v[k] = slab[i_row + (q + k * cgs) * lds];
-            uq[k] = u[q + k * cgs];
+      if (j + 1 < w && my_g == 0)
+        for (int i = my_i; i < rows; i += RT) {
+          const int gi = r0 + i;
+          if (gi > j) {
+            const double t = fabs(slab[i + (j + 1) * lds]);
+            if (t > bv || (t == bv && gi < bi)) { bv = t; bi = gi; }
           }
-#pragma unroll
-          for (int k = 0; k < 4; ++k) slab[i_row + (q + k * cgs) * lds] = fma(-l, uq[k], v[k]);
         }
-        for (; q < w; q += cgs) slab[i_row + q * lds] = fma(-l, u[q], slab[i_row + q * lds]);
+      continue;
+    }
+    // ---- 4. exchange rows j and r: warp 0 writes the pivot row into row j,
+    // warp 1 the old row j's first j entries into row r; row r's update
+    // reads the old row j directly.  Then per row: scale column j below the
+    // pivot (reciprocal multiply, as bl1_dinvscalv), rank-1 update of the
+    // rest of the row, and (group 0) the row's candidate for column j + 1.
+    const double rinv = 1.0 / piv;
+    if (r != j) {
+      if (warp == 0 && j >= r0 && j < r0 + rows)
+        for (int q = lane; q < w; q += 32) slab[(j - r0) + q * lds] = u[q];
+      if (warp == 1 && r >= r0 && r < r0 + rows)
+        for (int q = lane; q < j; q += 32) slab[(r - r0) + q * lds] = oldj[q];
+    }
+    for (int i = my_i; i < rows; i += RT) {
+      const int gi = r0 + i;
+      if (gi <= j) continue;
+      const double* src = (gi == r) ? oldj : nullptr;
+      const double l = (src ? src[j] : (G > 1 ? vj : slab[i + j * lds])) * rinv;
+      int q = j + 1 + my_g;
+      if (my_g == 0) {
+        slab[i + j * lds] = l;
+        if (q < w) {
+          const double t = fma(-l, u[q], src ? src[q] : slab[i + q * lds]);
+          slab[i + q * lds] = t;
+          const double at = fabs(t);
+          if (at > bv || (at == bv && gi < bi)) { bv = at; bi = gi; }
+          q += G;
+        }
+      }
+      if (src) {
+        for (; q < w; q += G) slab[i + q * lds] = fma(-l, u[q], src[q]);
+      } else {
+        for (; q + G < w; q += 2 * G) {
+          const double x0 = slab[i + q * lds], x1 = slab[i + (q + G) * lds];
+          slab[i + q * lds] = fma(-l, u[q], x0);
+          slab[i + (q + G) * lds] = fma(-l, u[q + G], x1);
+        }
+        if (q < w) slab[i + q * lds] = fma(-l, u[q], slab[i + q * lds]);
       }
     }
-    __syncthreads();
   }
+  __syncthreads();
   if (RM) {
     for (int e = tid; e < rows * w; e += LEAF_THREADS) {
       const int i = e / w, col = e - i * w;
@@ -263,9 +291,251 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
   if (c == 0 && tid == 0 && first_null >= 0) atomicMin(a.info, a.gcol + first_null);
 }
 
+// Register-resident leaf for a panel stored transposed (element (i, col) at
+// P[i * ld + col]), w == W columns: thread t of each CTA owns the slab rows
+// i = t + k * 512 (k < RPT) and keeps their W entries in registers, so the
+// rank-1 updates never touch memory.  Per column: warp shuffles and warp 0
+// find the CTA's candidate (two CTA barriers); the warp holding the
+// candidate row gathers it by shuffles and pushes it, with the magnitude
+// and row index, into every CTA's shared memory, and the warp holding row j
+// does the same with row j; one cluster barrier; warp 0 picks the winner
+// (one CTA barrier); then each thread exchanges, scales and updates its own
+// rows and forms its candidate for the next column.  Same pivot order, tie
+// rule, null-column and NaN handling as lu_leaf_cluster_kernel.
+constexpr int RLEAF_THREADS = 512;
+
+__host__ __device__ inline size_t rleaf_smem_bytes(int w, int C) {
+  return sizeof(double) * (2 * (size_t)C * w + 2 * C + 2 * w) + sizeof(int) * 2 * C + 64;
+}
+
+template <int W, int RPT>
+__device__ __forceinline__ double rleaf_pick(const double (&rv)[RPT][W], int k, int q) {
+  double v = rv[0][q];
+#pragma unroll
+  for (int kk = 1; kk < RPT; ++kk)
+    if (kk == k) v = rv[kk][q];
+  return v;
+}
+
+// Lane `src` of the calling warp holds the row (slot k); every lane gets it
+// by shuffles and lanes d < C store it into CTA d's buffer at dst.
+template <int W, int RPT>
+__device__ __forceinline__ void rleaf_push_row(const double (&rv)[RPT][W], int k, int src, double* dst, int C,
+                                               cg::cluster_group& cluster) {
+  const int lane = threadIdx.x & 31;
+  double* d = cluster.map_shared_rank(dst, lane < C ? lane : 0);
+#pragma unroll
+  for (int q0 = 0; q0 < W; q0 += 4) {
+    double row[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) row[q] = __shfl_sync(0xffffffffu, rleaf_pick<W, RPT>(rv, k, q0 + q), src);
+    if (lane < C)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) d[q0 + q] = row[q];
+  }
+}
+
+// Entry j (run-time) of a register row: a select chain over compile-time
+// indices, so the row stays in registers.
+template <int W>
+__device__ __forceinline__ double rleaf_pick_col(const double (&row)[W], int j) {
+  double v = row[0];
+#pragma unroll
+  for (int q = 1; q < W; ++q)
+    if (q == j) v = row[q];
+  return v;
+}
+
+// Column J of the leaf for the calling thread's rows, J a compile-time
+// constant so every register of a row is addressed directly: exchange
+// rows j and r, scale column J below the pivot (reciprocal multiply, as
+// bl1_dinvscalv), rank-1 update, and the candidate for column J + 1.
+template <int W, int RPT, int J>
+__device__ __forceinline__ void rleaf_column(double (&rv)[RPT][W], int tid, int r0, int rows, int r,
+                                             const double* u, const double* oldj, double rinv, double& bv,
+                                             int& bi) {
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) {
+    const int i = tid + k * RLEAF_THREADS, gi = r0 + i;
+    if (i >= rows || gi < J) continue;
+    if (gi == J) {
+      if (r != J)
+#pragma unroll
+        for (int q = 0; q < W; ++q) rv[k][q] = u[q];
+      continue;
+    }
+    if (gi == r)
+#pragma unroll
+      for (int q = 0; q < W; ++q) rv[k][q] = oldj[q];
+    const double l = rv[k][J] * rinv;
+    rv[k][J] = l;
+#pragma unroll
+    for (int q = J + 1; q < W; ++q) rv[k][q] = fma(-l, u[q], rv[k][q]);
+    if constexpr (J + 1 < W) {
+      const double t = fabs(rv[k][J + 1]);
+      if (t > bv) { bv = t; bi = gi; }
+    }
+  }
+}
+
+template <int W, int RPT, int J = 0>
+__device__ __forceinline__ void rleaf_column_at(int j, double (&rv)[RPT][W], int tid, int r0, int rows, int r,
+                                                const double* u, const double* oldj, double rinv, double& bv,
+                                                int& bi) {
+  if constexpr (J < W) {
+    if (j == J) {
+      rleaf_column<W, RPT, J>(rv, tid, r0, rows, r, u, oldj, rinv, bv, bi);
+      return;
+    }
+    rleaf_column_at<W, RPT, J + 1>(j, rv, tid, r0, rows, r, u, oldj, rinv, bv, bi);
+  }
+}
+
+template <int W, int RPT>
+__global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs a) {
+  extern __shared__ double S[];
+  constexpr int NW = RLEAF_THREADS / 32;
+  __shared__ double s_rv[2][NW];
+  __shared__ int s_ri[2][NW];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int C = (int)cluster.num_blocks();
+  const int c = (int)cluster.block_rank();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double* xrow = S;                                  // [2][C][W] candidate rows
+  double* xval = xrow + 2 * (size_t)C * W;           // [2][C] candidate magnitudes
+  double* rowj = xval + 2 * C;                       // [2][W] row j
+  int* xidx = reinterpret_cast<int*>(rowj + 2 * W);  // [2][C] candidate rows (INT_MAX: none)
+  const int r0 = c * a.R;
+  const int rows = max(0, min(a.R, a.M - r0));
+
+  double rv[RPT][W];
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) {
+    const int i = tid + k * RLEAF_THREADS;
+#pragma unroll
+    for (int q = 0; q < W; ++q) rv[k][q] = (i < rows) ? a.P[(long)(r0 + i) * a.ld + q] : 0.0;
+  }
+  int first_null = -1;
+  double bv = -1.0;
+  int bi = INT_MAX;
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) {
+    const int i = tid + k * RLEAF_THREADS;
+    if (i < rows) {
+      const double v = fabs(rv[k][0]);
+      if (v > bv) { bv = v; bi = r0 + i; }  // rows ascend with k
+    }
+  }
+  // The column loop is not unrolled (the unrolled body would overflow the
+  // instruction cache); the per-column update is dispatched to a
+  // compile-time column.  Per column one CTA barrier (the warps' candidates)
+  // and one cluster barrier (the pushed rows); every warp reduces the
+  // warps' candidates and the CTAs' candidates itself.
+#pragma unroll 1
+  for (int j = 0; j < W; ++j) {
+    const int par = j & 1;
+    // ---- 1. CTA candidate
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    }
+    if (lane == 0) { s_rv[par][warp] = bv; s_ri[par][warp] = bi; }
+    __syncthreads();
+    {
+      double v = lane < NW ? s_rv[par][lane] : -1.0;
+      int i0 = lane < NW ? s_ri[par][lane] : INT_MAX;
+      // all 32 lanes take part (lanes >= NW hold the neutral element), so
+      // every lane of every warp ends with the same candidate
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, i0, off);
+        if (ov > v || (ov == v && oi < i0)) { v = ov; i0 = oi; }
+      }
+      bv = v;
+      bi = i0;
+    }
+    // ---- 2. push the candidate row and row j to every CTA
+    if (bi != INT_MAX) {
+      const int li = bi - r0, ot = li & (RLEAF_THREADS - 1);
+      if (li >= 0 && li < rows && warp == (ot >> 5))
+        rleaf_push_row<W, RPT>(rv, li / RLEAF_THREADS, ot & 31, xrow + ((size_t)par * C + c) * W, C, cluster);
+    }
+    if (warp == 0 && lane < C) {
+      *cluster.map_shared_rank(xval + par * C + c, lane) = bv;
+      *cluster.map_shared_rank(xidx + par * C + c, lane) = bi;
+    }
+    if (j >= r0 && j < r0 + rows) {
+      const int lj = j - r0, jt = lj & (RLEAF_THREADS - 1);
+      if (warp == (jt >> 5)) rleaf_push_row<W, RPT>(rv, lj / RLEAF_THREADS, jt & 31, rowj + par * W, C, cluster);
+    }
+    cluster.sync();
+    // ---- 3. winner (identical in every warp of every CTA: same data, same
+    // order)
+    int r, w0;
+    {
+      double v = -2.0;
+      int i0 = INT_MAX, q0 = 0;
+      for (int q = lane; q < C; q += 32) {
+        const double cv = xval[par * C + q];
+        const int ci = xidx[par * C + q];
+        if (ci != INT_MAX && (cv > v || (cv == v && ci < i0))) { v = cv; i0 = ci; q0 = q; }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, i0, off);
+        const int oq = __shfl_xor_sync(0xffffffffu, q0, off);
+        if (ov > v || (ov == v && oi < i0)) { v = ov; i0 = oi; q0 = oq; }
+      }
+      r = i0;
+      w0 = q0;
+    }
+    const double* u = xrow + ((size_t)par * C + w0) * W;  // the pivot row
+    if (r == INT_MAX) {
+      // no orderable candidate (every magnitude NaN): keep row j, as idamax
+      // does when no later entry compares greater than the first
+      r = j;
+      u = rowj + par * W;
+    }
+    const double* oldj = rowj + par * W;
+    const double piv = u[j];
+    if (c == 0 && tid == 0) a.piv[j] = r - j;
+    bv = -1.0;
+    bi = INT_MAX;
+    if (piv == 0.0) {
+      // null column: no exchange, no scaling, no update
+      if (first_null < 0) first_null = j;
+      if (j + 1 < W)
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+          const int i = tid + k * RLEAF_THREADS, gi = r0 + i;
+          if (i < rows && gi > j) {
+            const double t = fabs(rleaf_pick_col<W>(rv[k], j + 1));
+            if (t > bv) { bv = t; bi = gi; }
+          }
+        }
+      continue;
+    }
+    // ---- 4. exchange, scale, update, next candidate
+    rleaf_column_at<W, RPT>(j, rv, tid, r0, rows, r, u, oldj, 1.0 / piv, bv, bi);
+  }
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) {
+    const int i = tid + k * RLEAF_THREADS;
+    if (i < rows)
+#pragma unroll
+      for (int q = 0; q < W; ++q) a.P[(long)(r0 + i) * a.ld + q] = rv[k][q];
+  }
+  if (c == 0 && tid == 0 && first_null >= 0) atomicMin(a.info, a.gcol + first_null);
+}
+
 struct LeafConfig {
   bool ready = false;
   int max_cluster = 8;
+  int max_cluster_reg = 8;  // register-resident leaf
   size_t smem_cap = 0;  // usable dynamic SMEM per CTA
 };
 LeafConfig g_leaf;
@@ -301,7 +571,85 @@ int leaf_setup() {
     }
     cudaGetLastError();
   }
+  // the register-resident leaf: 512 threads, a few KB of SMEM
+  for (auto kern : {lu_leaf_reg_kernel<8, 4>, lu_leaf_reg_kernel<16, 2>, lu_leaf_reg_kernel<32, 1>})
+    FB_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  g_leaf.max_cluster_reg = 1;
+  for (int cs = LEAF_MAXC; cs >= 2; cs >>= 1) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(RLEAF_THREADS);
+    cfg.dynamicSmemBytes = rleaf_smem_bytes(32, cs);
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    bool ok = true;
+    for (auto kern : {lu_leaf_reg_kernel<8, 4>, lu_leaf_reg_kernel<16, 2>, lu_leaf_reg_kernel<32, 1>}) {
+      nclusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg) != cudaSuccess || nclusters <= 0) ok = false;
+      cudaGetLastError();
+    }
+    if (ok) {
+      g_leaf.max_cluster_reg = cs;
+      break;
+    }
+  }
   g_leaf.ready = true;
+  return FLA_SUCCESS;
+}
+
+// Cluster geometry of the register-resident leaf for an M x w panel:
+// w must be 8, 16 or 32 and the rows must fit 512 x RPT per CTA.
+bool rleaf_geometry(long M, int w, int* C, int* R) {
+  if (w != 8 && w != 16 && w != 32) return false;
+  const long cap = (long)RLEAF_THREADS * (w == 8 ? 4 : w == 16 ? 2 : 1);
+  int cs = 1;
+  while (cs < g_leaf.max_cluster_reg && (M + cs - 1) / cs > cap) cs <<= 1;
+  if ((M + cs - 1) / cs > cap) return false;
+  *C = cs;
+  *R = (int)((M + cs - 1) / cs);
+  return true;
+}
+
+int rleaf_launch(double* P, long ld, long M, int w, int* d_piv, int gcol, cudaStream_t st) {
+  int C = 0, R = 0;
+  if (!rleaf_geometry(M, w, &C, &R)) {
+    set_last_error("LU panel leaf does not fit in a cluster");
+    return FLA_FAILURE;
+  }
+  LeafArgs la;
+  la.P = P;
+  la.ld = ld;
+  la.M = (int)M;
+  la.w = w;
+  la.R = R;
+  la.lds = 0;
+  la.gcol = gcol;
+  la.piv = d_piv;
+  la.info = ctx().d_status + ST_INFO;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(C);
+  cfg.blockDim = dim3(RLEAF_THREADS);
+  cfg.dynamicSmemBytes = rleaf_smem_bytes(w, C);
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const int ps = prof_begin(st);
+  if (w == 8) FB_CK(cudaLaunchKernelEx(&cfg, lu_leaf_reg_kernel<8, 4>, la));
+  else if (w == 16) FB_CK(cudaLaunchKernelEx(&cfg, lu_leaf_reg_kernel<16, 2>, la));
+  else FB_CK(cudaLaunchKernelEx(&cfg, lu_leaf_reg_kernel<32, 1>, la));
+  prof_end(ps, st, PROF_PANEL, 0.0);
+  count_launch();
   return FLA_SUCCESS;
 }
 
@@ -312,7 +660,7 @@ int leaf_setup() {
 int leaf_maxw() {
   static int mw = 0;
   if (mw == 0) {
-    mw = 64;
+    mw = 32;
     if (const char* e = std::getenv("FLA_B200_LU_LEAF_MAXW")) {
       const int v = std::atoi(e);
       if (v >= 8 && v <= LEAF_MAXW) mw = v;
@@ -418,6 +766,7 @@ int lu_panel_factor_t(double* P, long ld, long M, int w, int* d_piv, int gcol, c
   if (w <= 0 || M <= 0) return FLA_SUCCESS;
   int C, R, lds;
   size_t smem;
+  if (rleaf_geometry(M, w, &C, &R)) return rleaf_launch(P, ld, M, w, d_piv, gcol, st);
   if (leaf_geometry(M, w, &C, &R, &lds, &smem) || w <= 2) return leaf_launch(P, ld, M, w, d_piv, gcol, true, st);
   const int w1 = std::max(2, (w / 2) & ~1);
   const int w2 = w - w1;

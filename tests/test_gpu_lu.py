@@ -25,7 +25,9 @@ def run_lu(cuda, flame, A):
 
 
 @pytest.mark.parametrize("m,n", [(1, 1), (2, 2), (7, 5), (5, 7), (64, 64), (129, 129), (200, 150),
-                                 (150, 200), (300, 300), (513, 257), (1024, 1024)])
+                                 (150, 200), (300, 300), (513, 257), (1024, 1024),
+                                 # tall panels: 16-CTA clusters with 1024 and more rows per CTA
+                                 (16384, 48), (20000, 64), (40000, 24)])
 def test_lu_matches_oracle(cuda, flame, oracle, m, n):
     rng = seeded(m * 7 + n)
     A = rng.uniform(-1, 1, (m, n))
