@@ -277,92 +277,143 @@ __device__ __forceinline__ void slab_load(const float* __restrict__ P, long ld, 
     v[j] = (i < mi && k < mk) ? (ROWMAJ ? P[(long)k + (long)i * ld] : P[(long)i + (long)k * ld]) : 0.f;
   }
 }
+// 128 x 128 block of op(P) into registers, 16 float4 per thread, every load
+// in flight at once.  ROWMAJ: element (i, k) at P[k + i * ld], else
+// P[i + k * ld]; the contiguous index runs in float4 steps (the caller
+// guarantees 16-byte alignment and that the float4 holding the last valid
+// element lies inside the allocation).  Columns k >= mk are zero (padding
+// columns would otherwise multiply zeros of the right-hand block by
+// whatever the workspace holds); rows i >= mi are zero too.
 template <bool ROWMAJ>
-__device__ __forceinline__ void slab_store(float (*sF)[33], const float (&v)[16]) {
+__device__ __forceinline__ void block_load(const float* __restrict__ P, long ld, int mi, int mk, float4 (&v)[16]) {
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
-    const int e = threadIdx.x + j * 256;
-    const int i = ROWMAJ ? (e >> 5) : (e & 127), k = ROWMAJ ? (e & 31) : (e >> 7);
-    sF[i][k] = v[j];
+    const int e4 = threadIdx.x + j * 256;
+    const int a = e4 >> 5, b4 = (e4 & 31) * 4;  // ROWMAJ: (row a, columns b4..); else (column a, rows b4..)
+    const int i = ROWMAJ ? a : b4, k = ROWMAJ ? b4 : a;
+    float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (ROWMAJ ? (i < mi && k < mk) : (k < mk && i < mi))
+      x = *reinterpret_cast<const float4*>(ROWMAJ ? P + k + (long)i * ld : P + i + (long)k * ld);
+    if (ROWMAJ) {
+      if (k + 1 >= mk) x.y = 0.f;
+      if (k + 2 >= mk) x.z = 0.f;
+      if (k + 3 >= mk) x.w = 0.f;
+    } else {
+      if (i + 1 >= mi) x.y = 0.f;
+      if (i + 2 >= mi) x.z = 0.f;
+      if (i + 3 >= mi) x.w = 0.f;
+    }
+    v[j] = x;
   }
 }
-
-// acc(q) += sum_k sF(rr, k) sX(k0 + k, half * 16 + q), k < 32
-__device__ __forceinline__ void slab_fma(const float (*sF)[33], const float (*sX)[36], int k0, int rr, int half,
-                                         float (&acc)[16]) {
-#pragma unroll 8
-  for (int k = 0; k < 32; ++k) {
-    const float f = sF[rr][k];
-    const float4* xk = reinterpret_cast<const float4*>(&sX[k0 + k][half * 16]);
+// ... and into shared memory as sF[i * 129 + k]
+template <bool ROWMAJ>
+__device__ __forceinline__ void block_store(float* sF, const float4 (&v)[16]) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const float4 x = xk[j];
-      acc[4 * j] = fmaf(f, x.x, acc[4 * j]);
-      acc[4 * j + 1] = fmaf(f, x.y, acc[4 * j + 1]);
-      acc[4 * j + 2] = fmaf(f, x.z, acc[4 * j + 2]);
-      acc[4 * j + 3] = fmaf(f, x.w, acc[4 * j + 3]);
+  for (int j = 0; j < 16; ++j) {
+    const int e4 = threadIdx.x + j * 256;
+    const int a = e4 >> 5, b4 = (e4 & 31) * 4;
+    if (ROWMAJ) {
+      float* d = sF + a * 129 + b4;
+      d[0] = v[j].x; d[1] = v[j].y; d[2] = v[j].z; d[3] = v[j].w;
+    } else {
+      float* d = sF + b4 * 129 + a;
+      d[0] = v[j].x; d[129] = v[j].y; d[258] = v[j].z; d[387] = v[j].w;
     }
   }
 }
+// acc(a, b) += sum_{k < kn} sF(rg + 32 a, k) sX(k, 4 cg + b): lane rg takes
+// rows rg, rg+32, rg+64, rg+96 (conflict-free scalar reads of sF, stride
+// 129), warp cg takes right-hand sides 4cg..4cg+3 (one broadcast float4 of
+// sX per k): 16 FMAs per 5 shared loads.
+__device__ __forceinline__ void block_fma(const float* sF, const float (*sX)[36], int kn, int rg, int cg,
+                                          float (&acc)[4][4]) {
+#pragma unroll 8
+  for (int k = 0; k < kn; ++k) {
+    const float4 x = *reinterpret_cast<const float4*>(&sX[k][4 * cg]);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const float f = sF[(rg + 32 * a) * 129 + k];
+      acc[a][0] = fmaf(f, x.x, acc[a][0]);
+      acc[a][1] = fmaf(f, x.y, acc[a][1]);
+      acc[a][2] = fmaf(f, x.z, acc[a][2]);
+      acc[a][3] = fmaf(f, x.w, acc[a][3]);
+    }
+  }
+}
+
+constexpr int SOLVE_SMEM = (128 * 36 + 128 * 129) * 4;
 
 template <bool TI, bool TF>
 __global__ void __launch_bounds__(256) solve_step_kernel(const float* __restrict__ F, long ldf,
                                                          const float* __restrict__ Inv, float* __restrict__ X,
                                                          float* __restrict__ Y, long ldy, int nr, int b0, int w,
                                                          int r_lo, int r_hi, int own_lo, int wn) {
-  __shared__ __align__(16) float sX[128][36];  // X(b0 : b0+w, :), then the owner's updated rows
-  __shared__ float sF[128][33];                // 32-column slab of op(F) or op(Inv)
+  extern __shared__ __align__(16) float sm_solve[];
+  float (*sX)[36] = reinterpret_cast<float (*)[36]>(sm_solve);  // X(b0 : b0+w, :), then the owner's rows
+  float* sF = sm_solve + 128 * 36;                              // op(F) block, then op(Inv)
   const int tid = threadIdx.x;
-  const int rr = tid & 127, half = tid >> 7;
+  const int rg = tid & 31, cg = tid >> 5;
   const int r0 = r_lo + blockIdx.x * 128;
-  const int r = r0 + rr;
-  float v[16];
-  // X block: element (k, c) at X[b0 + k + c * ldy]
-  slab_load<false>(X + b0, ldy, w, nr, v);
-#pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    const int e = tid + j * 256;
-    sX[e & 127][e >> 7] = v[j];
-  }
-  float acc[16];
-#pragma unroll
-  for (int q = 0; q < 16; ++q) acc[q] = 0.f;
+  const bool owner = (r0 == own_lo);
+  // the whole op(F) block (rows r0.., columns b0..b0+w) in flight first
+  float4 v[16];
   const float* Fb = TF ? F + b0 + (long)r0 * ldf : F + r0 + (long)b0 * ldf;
-  if (w > 0) slab_load<TF>(Fb, ldf, r_hi - r0, w, v);
-  for (int k0 = 0; k0 < w; k0 += 32) {
-    __syncthreads();
-    slab_store<TF>(sF, v);
-    __syncthreads();
-    if (k0 + 32 < w) slab_load<TF>(TF ? Fb + k0 + 32 : Fb + (long)(k0 + 32) * ldf, ldf, r_hi - r0, w - k0 - 32, v);
-    slab_fma(sF, sX, k0, rr, half, acc);
-  }
-  if (r0 != own_lo) {
-    if (r < r_hi)
+  if (w > 0) block_load<TF>(Fb, ldf, r_hi - r0, w, v);
+  {
+    // X block: element (k, c) at X[b0 + k + c * ldy]
+    float xv[16];
+    slab_load<false>(X + b0, ldy, w, nr, xv);
 #pragma unroll
-      for (int q = 0; q < 16; ++q)
-        if (half * 16 + q < nr) Y[(long)r + (long)(half * 16 + q) * ldy] -= acc[q];
+    for (int j = 0; j < 16; ++j) {
+      const int e = tid + j * 256;
+      sX[e & 127][e >> 7] = xv[j];
+    }
+  }
+  if (w > 0) block_store<TF>(sF, v);
+  // the owner's inverse block loads overlap the update
+  if (owner) block_load<TI>(Inv, 128, wn, wn, v);
+  __syncthreads();
+  float acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
+  block_fma(sF, sX, w, rg, cg, acc);
+  if (!owner) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int r = r0 + rg + 32 * a;
+      if (r < r_hi)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+          if (4 * cg + b < nr) Y[(long)r + (long)(4 * cg + b) * ldy] -= acc[a][b];
+    }
     return;
   }
   // owner: the next diagonal block, updated, into sX; then X := op(Inv) sX
-  slab_load<TI>(Inv, 128, wn, wn, v);
   __syncthreads();
 #pragma unroll
-  for (int q = 0; q < 16; ++q) {
-    const int c = half * 16 + q;
-    sX[rr][c] = (rr < wn && c < nr) ? Y[(long)r + (long)c * ldy] - acc[q] : 0.f;
-    acc[q] = 0.f;
-  }
-  for (int k0 = 0; k0 < wn; k0 += 32) {
-    __syncthreads();
-    slab_store<TI>(sF, v);
-    __syncthreads();
-    if (k0 + 32 < wn) slab_load<TI>(TI ? Inv + k0 + 32 : Inv + (long)(k0 + 32) * 128, 128, wn, wn - k0 - 32, v);
-    slab_fma(sF, sX, k0, rr, half, acc);
-  }
-  if (rr < wn)
+  for (int a = 0; a < 4; ++a) {
+    const int i = rg + 32 * a;
 #pragma unroll
-    for (int q = 0; q < 16; ++q)
-      if (half * 16 + q < nr) X[(long)r + (long)(half * 16 + q) * ldy] = acc[q];
+    for (int b = 0; b < 4; ++b) {
+      const int c = 4 * cg + b;
+      sX[i][c] = (i < wn && c < nr) ? Y[(long)(r0 + i) + (long)c * ldy] - acc[a][b] : 0.f;
+      acc[a][b] = 0.f;
+    }
+  }
+  block_store<TI>(sF, v);
+  __syncthreads();
+  block_fma(sF, sX, wn, rg, cg, acc);
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int i = rg + 32 * a;
+    if (i < wn)
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+        if (4 * cg + b < nr) X[(long)(r0 + i) + (long)(4 * cg + b) * ldy] = acc[a][b];
+  }
 }
 
 inline int grid_for(long total) { return (int)std::min<long>(8192, (total + 255) / 256); }
@@ -624,6 +675,14 @@ int lp_solve(const LpFactor& f, const double* R, long ldr, double* D, long ldd, 
   // Forward sweep L y = T (T -> Tb), backward sweep U x = y or L^T x = y
   // (Tb -> T), one fused launch per 128-row block while nrhs <= 32.
   if (nrhs <= 32) {
+    static bool attr = false;
+    if (!attr) {
+      FB_CK(cudaFuncSetAttribute(solve_step_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 SOLVE_SMEM));
+      FB_CK(cudaFuncSetAttribute(solve_step_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 SOLVE_SMEM));
+      attr = true;
+    }
     auto blk = [&](long kb) { return std::make_pair(kb * MB, (int)std::min<long>(MB, n - kb * MB)); };
     // LU: inv(L11) = inv(L11^T)^T, L(r, c) = F[c + r * ldf]; Cholesky: inv(L11), L(r, c) = F[r + c * ldf]
     auto fwd = [&](long kb, int w, long r_lo, long r_hi, long own) {
@@ -631,10 +690,10 @@ int lp_solve(const LpFactor& f, const double* R, long ldr, double* D, long ldd, 
       const auto nx = blk(own / MB);
       const float* inv = f.inv1 + (own / MB) * MB * MB;
       if (!f.chol)
-        solve_step_kernel<true, true><<<g, 256, 0, st>>>(F, ldf, inv, Tb, T, n, (int)nrhs, (int)(kb * MB), w,
+        solve_step_kernel<true, true><<<g, 256, SOLVE_SMEM, st>>>(F, ldf, inv, Tb, T, n, (int)nrhs, (int)(kb * MB), w,
                                                          (int)r_lo, (int)r_hi, (int)own, nx.second);
       else
-        solve_step_kernel<false, false><<<g, 256, 0, st>>>(F, ldf, inv, Tb, T, n, (int)nrhs, (int)(kb * MB), w,
+        solve_step_kernel<false, false><<<g, 256, SOLVE_SMEM, st>>>(F, ldf, inv, Tb, T, n, (int)nrhs, (int)(kb * MB), w,
                                                            (int)r_lo, (int)r_hi, (int)own, nx.second);
     };
     // Forward sweep L y = T: y into Tb block by block
@@ -649,7 +708,7 @@ int lp_solve(const LpFactor& f, const double* R, long ldr, double* D, long ldd, 
       const unsigned g = (unsigned)std::max<long>(1, (r_hi - r_lo + 127) / 128);
       const auto nx = blk(own / MB);
       const float* inv = (f.chol ? f.inv1 : f.inv2) + (own / MB) * MB * MB;
-      solve_step_kernel<true, true><<<g, 256, 0, st>>>(F, ldf, inv, T, Tb, n, (int)nrhs, (int)(kb * MB), w,
+      solve_step_kernel<true, true><<<g, 256, SOLVE_SMEM, st>>>(F, ldf, inv, T, Tb, n, (int)nrhs, (int)(kb * MB), w,
                                                        (int)r_lo, (int)r_hi, (int)own, nx.second);
     };
     const auto last = blk(nblk - 1);
