@@ -64,11 +64,15 @@ int           FLA_B200_LU_piv_panel_noalloc( int m, int n, double* A, int lda, i
  * factorization runs in low precision (FP32 storage, 16-bit tensor-core
  * trailing updates with FP32 accumulation, panels in FP64) and FP64
  * iterative refinement restores FP64 accuracy; A is left unchanged.
- * prec: 0 BF16, 1 FP16 with power-of-two equilibration, -1 the library
- * default (FLA_B200_IR_PREC, else FP16).  solver: 0 classic refinement
- * (dsgesv_'s), 1 GMRES-IR (GMRES in FP64 preconditioned by the
- * low-precision factors, for ill-conditioned A), -1 the default
- * (FLA_B200_IR_SOLVER, else GMRES-IR).  iter (optional) receives the
+ * prec: 0 BF16, 1 FP16 with power-of-two equilibration, 2 3xTF32
+ * (FP32-accurate), -1 the library default (FLA_B200_IR_PREC, else FP16).
+ * solver: 0 classic refinement (dsgesv_'s), 1 GMRES-IR (GMRES in FP64
+ * preconditioned by the low-precision factors, for ill-conditioned A),
+ * 2 adaptive (classic refinement while each step cuts the backward error
+ * at least fourfold, else straight to the FP64 factorization), -1 the
+ * default (FLA_B200_IR_SOLVER = ir | gmres | auto, else adaptive).
+ * Classic and GMRES-IR escalate to 3xTF32 before the FP64 factorization.
+ * iter (optional) receives the
  * number of refinement steps, or -3 (low-precision factorization failed)
  * / -31 (no convergence in 30 steps) when the FP64 factorization of a copy
  * produced X; inner (optional) the GMRES iterations.  Returns FLA_SUCCESS,

@@ -263,9 +263,11 @@ FLA_Error FLA_B200_Chol_logdet_adjoint(FLA_Obj L, FLA_Obj Lbar, double scale, do
     return FLA_FAILURE;
   }
   cudaStream_t st = ctx().stream;
+  op_begin(st);
   if (logdet && logdet_dev((const double*)sl.dev, sl.ld, (long)L.m, logdet, st) != FLA_SUCCESS) return FLA_FAILURE;
   if (logdet_adjoint_dev((const double*)sl.dev, (double*)sb.dev, sb.ld, (long)L.m, scale, st) != FLA_SUCCESS)
     return FLA_FAILURE;
+  op_end(st);
   if (unstage(sb) != FLA_SUCCESS || sync_all() != FLA_SUCCESS) return FLA_FAILURE;
   return FLA_SUCCESS;
 }

@@ -1003,7 +1003,9 @@ int ir_refine(const DMat& A, const DMat& B, double* X, long ldx, const LpFactor&
     }
     if (ok) met = true;
     // stagnation: three steps in a row without halving the backward error
+    // (adaptive solver: one step without a fourfold reduction)
     stall = (now < 0.5 * last) ? 0 : stall + 1;
+    if (!met && cfg.solver == IR_AUTO && !(now < 0.25 * last)) stall = 3;
     if (!met && stall >= 3) {
       res->iter = -(cfg.itermax + 1);
       res->stalled = true;
@@ -1040,6 +1042,7 @@ IrConfig ir_default_config() {
     const std::string s(e);
     if (s == "ir") c.solver = IR_CLASSIC;
     if (s == "gmres") c.solver = IR_GMRES;
+    if (s == "auto") c.solver = IR_AUTO;
   }
   return c;
 }

@@ -5,12 +5,16 @@
 
 namespace fb {
 
-enum IrSolver : int { IR_CLASSIC = 0, IR_GMRES = 1 };
+// IR_AUTO: classic refinement while every step reduces the backward error at
+// least fourfold; otherwise the caller falls back to the FP64 factorization
+// (on B200 the FP32-accurate tensor-core factorization costs about as much as
+// the FP64 one, so no intermediate format is tried).
+enum IrSolver : int { IR_CLASSIC = 0, IR_GMRES = 1, IR_AUTO = 2 };
 
 struct IrConfig {
   LowPrec prec = LP_FP16;   // format of the tensor-core updates (escalates to LP_TF32X3)
   bool scale = true;        // power-of-two equilibration before rounding
-  IrSolver solver = IR_GMRES;
+  IrSolver solver = IR_AUTO;
   int itermax = 30;         // ITERMAX of dsgesv_/dsposv_
   int gmres_m = 30;         // GMRES restart length (inner iterations per step)
   double gmres_tol = 1e-8;  // inner relative residual target

@@ -571,10 +571,10 @@ int mixed_solve_dev(bool chol, bool upper, DMat A, DMat B, DMat X, int* d_piv, c
   }
   // Escalation: the requested format first; if its factorization breaks
   // down or the refinement stalls, the FP32-accurate tensor-core format
-  // (3xTF32); then the FP64 factorization.
+  // (3xTF32, classic and GMRES-IR only); then the FP64 factorization.
   int steps = 0, code = -31;
   std::vector<LowPrec> ladder{cfg.prec};
-  if (cfg.prec != LP_TF32X3) ladder.push_back(LP_TF32X3);
+  if (cfg.prec != LP_TF32X3 && cfg.solver != IR_AUTO) ladder.push_back(LP_TF32X3);
   static const bool trace = std::getenv("FLA_B200_IR_TRACE") != nullptr;
   for (LowPrec p : ladder) {
     LpFactor f;
@@ -650,6 +650,7 @@ IrConfig config_from(int prec, int solver) {
   if (prec == 2) c.prec = LP_TF32X3;
   if (solver == 0) c.solver = IR_CLASSIC;
   if (solver == 1) c.solver = IR_GMRES;
+  if (solver == 2) c.solver = IR_AUTO;
   return c;
 }
 

@@ -84,6 +84,32 @@ def test_lu_solve_mixed_matches_oracle(cuda, flame, oracle, n, kappa, prec, solv
     assert it >= 0, "refinement should converge here (iter=%d)" % it
 
 
+@pytest.mark.parametrize("n,kappa", [(300, 1e2), (1000, 1e8)])
+@pytest.mark.parametrize("spd", [False, True])
+def test_adaptive_solver(cuda, flame, oracle, n, kappa, spd):
+    """solver 2: classic refinement while it contracts fast, else the FP64
+    factorization (iter < 0); either way the FP64 form's accuracy."""
+    rng = seeded(n + int(np.log10(kappa)) + (5 if spd else 0))
+    A = conditioned(rng, n, kappa, spd=spd)
+    B = rng.standard_normal((n, 4))
+    Ad, Bd = to_dev(cuda, A), to_dev(cuda, B)
+    Xd = to_dev(cuda, np.zeros_like(B))
+    if spd:
+        r, it, inner = flame.chol_solve_mixed(Ad, Bd, Xd, flame.FLA_LOWER_TRIANGULAR, 1, 2)
+        Lo, ro = oracle.chol(A)
+        Xo = oracle.chol_solve(Lo, B)
+    else:
+        r, it, inner = flame.lu_piv_solve_mixed(Ad, Bd, Xd, 1, 2)
+        Xo = _oracle_lu_solution(oracle, A, B)
+    assert r == flame.FLA_SUCCESS, flame.last_error()
+    assert inner == 0
+    X = to_host(Xd)
+    be, be_o = backward_error(A, X, B), backward_error(A, Xo, B)
+    assert be <= max(4 * be_o, 1e-15), (be, be_o, it)
+    if kappa <= 1e2:
+        assert it >= 0, "fast contraction: the 16-bit factors suffice (iter=%d)" % it
+
+
 @pytest.mark.parametrize("n,kappa", [(300, 1e2), (1000, 1e5), (1000, 1e8)])
 @pytest.mark.parametrize("uplo", ["L", "U"])
 def test_chol_solve_mixed_matches_oracle(cuda, flame, oracle, n, kappa, uplo):
