@@ -101,6 +101,7 @@ enum WsSlot : int {
   WS_PERM_T,        // gathered rows
   WS_TRINV,         // inverted diagonal blocks of the solves
   WS_SOLVE_W,       // block of solved unknowns
+  WS_SPLITK,        // partial products of split-K GEMMs
   WS_NSLOTS
 };
 void* ws_get(int slot, size_t bytes);  // nullptr on allocation failure

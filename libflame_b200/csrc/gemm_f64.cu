@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(Tile<BM_>::THREADS, Tile<BM_>::MINB)
     dgemm_tma_kernel(const __grid_constant__ CUtensorMap mapA,
                      const __grid_constant__ CUtensorMap mapB, double* __restrict__ C, long ldc,
                      int M, int N, int K, double alpha, double beta, int mode, long diag_off,
-                     int* err, const int* guard, int guard_limit) {
+                     int* err, const int* guard, int guard_limit, int k_chunk, long c_zstride) {
   using TC = Tile<BM_>;
   constexpr int BM = TC::BM, STAGES = TC::STAGES, THREADS = TC::THREADS, CONSUMER_WARPS = TC::WARPS;
   constexpr int A_STAGE_BYTES = TC::A_STAGE_BYTES, STAGE_BYTES = TC::STAGE_BYTES;
@@ -125,7 +125,12 @@ __global__ void __launch_bounds__(Tile<BM_>::THREADS, Tile<BM_>::MINB)
   const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int KT = (K + BK - 1) / BK;
+  // split K (k_chunk > 0, a multiple of BK): slice blockIdx.z of the k range
+  // into its own partial product at C + blockIdx.z * c_zstride
+  const int ks = blockIdx.z * k_chunk;
+  const int Kz = k_chunk ? min(K - ks, k_chunk) : K;
+  C += (long)blockIdx.z * c_zstride;
+  const int KT = (Kz + BK - 1) / BK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -142,7 +147,7 @@ __global__ void __launch_bounds__(Tile<BM_>::THREADS, Tile<BM_>::MINB)
     uint32_t fb_ = full0 + 8 * st;
     mbar_arrive_expect_tx(fb_, STAGE_BYTES);
     uint32_t dA = sm_base + st * STAGE_BYTES, dB = dA + A_STAGE_BYTES;
-    int k0 = kt * BK;
+    int k0 = ks + kt * BK;
     if (A_K) {
       tma_load_2d(dA, &mapA, k0, tile_m, fb_);  // box {16 k, 128 m}
     } else {
@@ -366,10 +371,26 @@ void set_attrs() {
 template <bool A_K, bool B_K, int BM_>
 void launch(dim3 grid, cudaStream_t st, const CUtensorMap& mA, const CUtensorMap& mB, double* C, long ldc, long m,
             long n, long k, double alpha, double beta, GemmMode mode, long diag_off, int* err, const int* guard,
-            int guard_limit) {
+            int guard_limit, int k_chunk, long c_zstride) {
   set_attrs<A_K, B_K, BM_>();
   dgemm_tma_kernel<A_K, B_K, BM_><<<grid, Tile<BM_>::THREADS, Tile<BM_>::SMEM_BYTES, st>>>(
-      mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard, guard_limit);
+      mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard, guard_limit, k_chunk,
+      c_zstride);
+}
+
+// C := alpha * sum_z P_z + beta * C over the S partial products of a split-K
+// GEMM (P_z at P + z * zs, ld ldp), summed in z order (deterministic).
+__global__ void splitk_reduce_kernel(const double* __restrict__ P, long ldp, long zs, int S, int m, int n,
+                                     double alpha, double beta, double* __restrict__ C, long ldc) {
+  const long total = (long)m * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long i = e % m, j = e / m;
+    const double* p = P + i + j * ldp;
+    double s = 0.0;
+    for (int z = 0; z < S; ++z) s += p[(long)z * zs];
+    double* c = C + i + j * ldc;
+    *c = beta != 0.0 ? fma(beta, *c, alpha * s) : alpha * s;
+  }
 }
 
 // Tile height: 64 (four CTAs per SM hide one another's prologue and
@@ -421,17 +442,46 @@ int gemm_f64(cudaStream_t st, bool ta, bool tb, long m, long n, long k, double a
   }
   dim3 grid((unsigned)((m + BMv - 1) / BMv), (unsigned)((n + BN - 1) / BN));
   int* err = ctx().d_status + ST_ERROR;
+  // Split K when the output has too few tiles to occupy the GPU and K is
+  // long (the W = U^T B products of the QR updates and of FLA_Apply_Q_UT):
+  // slices of K go to blockIdx.z, each into its own partial product, and one
+  // reduction adds them in a fixed order.
+  const long tiles = (long)grid.x * grid.y;
+  const int sms = ctx().num_sms;
+  long S = 1, kc = 0, ldp = 0, zs = 0;
+  double* Pz = nullptr;
+  if (mode == GEMM_FULL && !guard && tiles * 2 <= sms && k >= 2048) {
+    S = std::min<long>(std::min<long>((2L * sms + tiles - 1) / tiles, k / 512), 64);
+    if (S > 1) {
+      kc = ((k + S - 1) / S + BK - 1) / BK * BK;
+      S = (k + kc - 1) / kc;
+      ldp = (m + 1) & ~1L;
+      zs = ldp * n;
+      Pz = (double*)ws_get(WS_SPLITK, sizeof(double) * (size_t)(S * zs));
+      if (!Pz) return FLA_FAILURE;
+      grid.z = (unsigned)S;
+    }
+  }
+  double* Cl = S > 1 ? Pz : C;
+  const long ldcl = S > 1 ? ldp : ldc;
+  const double al = S > 1 ? 1.0 : alpha, be = S > 1 ? 0.0 : beta;
   const int pslot = prof_begin(st);
 #define FB_GEMM_LAUNCH(AK, BK_)                                                                                  \
-  (BMv == 64 ? launch<AK, BK_, 64>(grid, st, mA, mB, C, ldc, m, n, k, alpha, beta, mode, diag_off, err, guard,  \
-                                   guard_limit)                                                                 \
-             : launch<AK, BK_, 128>(grid, st, mA, mB, C, ldc, m, n, k, alpha, beta, mode, diag_off, err, guard, \
-                                    guard_limit))
+  (BMv == 64 ? launch<AK, BK_, 64>(grid, st, mA, mB, Cl, ldcl, m, n, k, al, be, mode, diag_off, err, guard,     \
+                                   guard_limit, (int)kc, zs)                                                    \
+             : launch<AK, BK_, 128>(grid, st, mA, mB, Cl, ldcl, m, n, k, al, be, mode, diag_off, err, guard,    \
+                                    guard_limit, (int)kc, zs))
   if (ta && !tb) FB_GEMM_LAUNCH(true, true);
   else if (ta && tb) FB_GEMM_LAUNCH(true, false);
   else if (!ta && !tb) FB_GEMM_LAUNCH(false, true);
   else FB_GEMM_LAUNCH(false, false);
 #undef FB_GEMM_LAUNCH
+  if (S > 1) {
+    const long total = m * n;
+    splitk_reduce_kernel<<<(unsigned)std::min<long>(4L * sms, (total + 255) / 256), 256, 0, st>>>(
+        Pz, ldp, zs, (int)S, (int)m, (int)n, alpha, beta, C, ldc);
+    count_launch();
+  }
   prof_end(pslot, st, PROF_GEMM,
            mode == GEMM_LOWER && m == n ? (double)m * (double)(m + 1) * (double)k
                                         : 2.0 * (double)m * (double)n * (double)k);
