@@ -121,3 +121,32 @@ def test_batched_tuner(cuda, flame):
     nbs = [flame.lib().FLA_B200_batched_nb(0, 1, n) for n in (16, 48, 100, 200, 400)]
     assert all(v in (8, 16, 24, 32) for v in nbs)
     assert all(t > 0 for t in times)
+
+
+def test_batched_sharded_single_rank(cuda, flame, oracle):
+    """The sharded entry on a one-rank process group: the whole batch is this
+    rank's share, factored in one launch, info gathered back in order."""
+    import socket
+    import torch.distributed as dist
+    from libflame_b200.shard import batched_sharded
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=0, world_size=1)
+    try:
+        rng = seeded(61)
+        sizes = [3, 40, 129, 300]
+        mats = [spd(rng, n) for n in sizes]
+        mats[1] = mats[1].copy()
+        mats[1][5, 5] = -1.0
+        dev = [to_dev(cuda, A) for A in mats]
+        r, info = batched_sharded("chol", dev)
+        assert r == flame.FLA_SUCCESS, flame.last_error()
+        for i, A in enumerate(mats):
+            Lo, ro = oracle.chol(A)
+            assert info[i] == ro
+            if ro == -1:
+                assert rel_fro(np.tril(to_host(dev[i])), np.tril(Lo)) < 1e-12
+    finally:
+        dist.destroy_process_group()
