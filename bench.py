@@ -491,7 +491,11 @@ def run_ours(args, rank, world):
             "frac": achieved / peak if achieved else None,
             "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul fp64) measured in this run; "
                            "MEASURED_PEAKS.json has no FP64 figure",
-            "traffic": None,
+            # DRAM bytes per launch: the ncu capture's bytes per flop (0.0574,
+            # profiles/dgemm_tma_kernel_lu_n6144.md) times this run's average
+            # launch; algorithmic bytes per launch (C read + write) beside it
+            "traffic": 0.0574 * gemm_flops / gemm_n if gemm_n else None,
+            "traffic_unit": "bytes per launch (ncu DRAM read + write, scaled per flop from n=6144)",
             "launches_per_step": gemm_n,
             "share_of_step": gemm_ms / total_ms if total_ms > 0 else None,
             "whole_factorization_frac_of_peak": value / world / peak,
@@ -503,7 +507,7 @@ def run_ours(args, rank, world):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": "FLA_LU_piv n=%d FP64, A iid U(-1,1) seeded, column-major in HBM" % n,
-                       "n": n, "blocksize": 128, "parallelism": "replicas" if world > 1 else "single",
+                       "n": n, "blocksize": 128, "chol_blocksize": 256, "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs (2 GiB) larger than L2; the per-step restore of A also flushes L2"},
             "roofline": roofline, "breakdown_ms": breakdown,
             "gpu_launches": launches, "clocks": clocks,

@@ -177,84 +177,65 @@ __global__ void __launch_bounds__(PANEL_THREADS) lu_panel_kernel(PanelArgs a) {
 //
 // Blocked form (npiv <= LASWP_MAXP): the interchanges touch at most 2*npiv
 // rows ("slots": rows row0..row0+npiv-1, then each distinct target below
-// them).  laswp_compose_kernel (one CTA) composes the whole sequence of
-// interchanges into one permutation of the slots and writes it to a small
-// device table; laswp_apply_kernel then moves every column's slot values
-// with independent, coalesced loads and stores, LASWP_NC columns per CTA.
+// them).  Each CTA of laswp_apply_kernel composes the whole sequence of
+// interchanges into one permutation of the slots (in shared memory) and
+// then moves its columns' slot values with independent, coalesced loads
+// and stores, LASWP_NC columns per CTA.
 // TR: the matrix is stored transposed (element (row, col) of A at
 // A[col + row * ld]); consecutive threads then take consecutive columns of
 // one slot row, which are contiguous.
 constexpr int LASWP_MAXP = 128;
 constexpr int LASWP_NC = 16;  // columns per CTA (static SMEM < 48 KB)
-// table layout (ints): [0] nslot, [1 .. 2*MAXP] slot rows (offset from row0,
-// -1 unused), [1 + 2*MAXP .. 4*MAXP] slot sources
-constexpr int LASWP_TABLE_INTS = 1 + 4 * LASWP_MAXP;
 
-__global__ void __launch_bounds__(256) laswp_compose_kernel(const int* __restrict__ piv, int npiv, int reverse,
-                                                            int* __restrict__ table) {
-  __shared__ int s_piv[LASWP_MAXP];
-  __shared__ int s_tgt[LASWP_MAXP];          // slot of the target of interchange i
-  __shared__ int s_row[2 * LASWP_MAXP];      // row offset (from row0) of each slot, -1 unused
-  __shared__ int s_src[2 * LASWP_MAXP];      // final content of slot s = original slot s_src[s]
+// Composition of the interchange sequence into slot rows and sources, in
+// shared memory (every CTA of the apply kernel forms it itself: the sequence
+// has at most LASWP_MAXP entries, and a separate launch would cost more).
+__device__ void laswp_compose(const int* __restrict__ piv, int npiv, int reverse, int* s_piv, int* s_tgt,
+                              int* s_row, int* s_src) {
   const int tid = threadIdx.x;
   const int nslot = 2 * npiv;
   for (int s = tid; s < nslot; s += blockDim.x) s_row[s] = (s < npiv) ? s : -1;
-  if (tid < npiv) s_piv[tid] = piv[tid];
+  for (int i = tid; i < npiv; i += blockDim.x) s_piv[i] = piv[i];
   __syncthreads();
-  if (tid < npiv) {
-    const int t = tid + s_piv[tid];  // target row offset
+  for (int i = tid; i < npiv; i += blockDim.x) {
+    const int t = i + s_piv[i];  // target row offset
     int slot;
     if (t < npiv) {
       slot = t;
     } else {
-      int first = tid;  // first interchange with the same far target owns the slot
-      for (int i2 = 0; i2 < tid; ++i2)
+      int first = i;  // first interchange with the same far target owns the slot
+      for (int i2 = 0; i2 < i; ++i2)
         if (i2 + s_piv[i2] == t) { first = i2; break; }
       slot = npiv + first;
-      if (first == tid) s_row[slot] = t;
+      if (first == i) s_row[slot] = t;
     }
-    s_tgt[tid] = slot;
+    s_tgt[i] = slot;
   }
   __syncthreads();
   if (tid == 0) {
     for (int s = 0; s < nslot; ++s) s_src[s] = s;
-    if (!reverse) {
-      for (int i = 0; i < npiv; ++i) {
-        const int a = i, b = s_tgt[i];
-        const int x = s_src[a];
-        s_src[a] = s_src[b];
-        s_src[b] = x;
-      }
-    } else {
-      for (int i = npiv - 1; i >= 0; --i) {
-        const int a = i, b = s_tgt[i];
-        const int x = s_src[a];
-        s_src[a] = s_src[b];
-        s_src[b] = x;
-      }
+    for (int q = 0; q < npiv; ++q) {
+      const int i = reverse ? npiv - 1 - q : q;
+      const int a = i, b = s_tgt[i];
+      const int x = s_src[a];
+      s_src[a] = s_src[b];
+      s_src[b] = x;
     }
-    table[0] = nslot;
   }
   __syncthreads();
-  for (int s = tid; s < nslot; s += blockDim.x) {
-    table[1 + s] = s_row[s];
-    table[1 + 2 * LASWP_MAXP + s] = s_src[s];
-  }
 }
 
 template <typename T, bool TR>
-__global__ void __launch_bounds__(256) laswp_apply_kernel(T* A, long ld, int row0, const int* __restrict__ table,
-                                                          int c0, int n0, int c1, int n1) {
+__global__ void __launch_bounds__(256) laswp_apply_kernel(T* A, long ld, int row0, const int* __restrict__ piv,
+                                                          int npiv, int reverse, int c0, int n0, int c1, int n1) {
+  __shared__ int s_piv[LASWP_MAXP];
+  __shared__ int s_tgt[LASWP_MAXP];
   __shared__ int s_row[2 * LASWP_MAXP];
   __shared__ int s_src[2 * LASWP_MAXP];
   __shared__ T s_val[LASWP_NC][2 * LASWP_MAXP + 1];
   const int tid = threadIdx.x;
-  const int nslot = table[0];
-  for (int s = tid; s < nslot; s += blockDim.x) {
-    s_row[s] = table[1 + s];
-    s_src[s] = table[1 + 2 * LASWP_MAXP + s];
-  }
-  __syncthreads();
+  laswp_compose(piv, npiv, reverse, s_piv, s_tgt, s_row, s_src);
+  const int nslot = 2 * npiv;
   const int ncols = n0 + n1;
   const int cbase = blockIdx.x * LASWP_NC;
   // load: consecutive threads take consecutive slots of one column
@@ -317,50 +298,21 @@ void set_attrs() {
   g_attrs = true;
 }
 
-// Panel geometry for an M-row panel: rows per CTA, CTAs, SMEM stride and
-// the widest panel (<= 128, multiple of 16) whose slab fits in SMEM.
-struct PanelGeom {
-  int R, G, lds, nb;
-  size_t smem;
-};
-PanelGeom panel_geom(long M, int nb_max) {
-  Context& cx = ctx();
-  PanelGeom g;
-  int sms = cx.num_sms;
-  g.R = (int)std::max<long>(std::min<long>(M, 32), (M + sms - 1) / sms);
-  g.G = (int)((M + g.R - 1) / g.R);
-  g.lds = g.R | 1;
-  g.nb = nb_max;
-  while (g.nb > 16 && (size_t)g.lds * g.nb * 8 + g.nb * 8 > PANEL_SMEM_CAP) g.nb -= 16;
-  g.smem = (size_t)g.lds * g.nb * 8 + (size_t)g.nb * 8;
-  return g;
-}
 
 }  // namespace
-
-// Slot tables of the blocked row interchanges: one per stream that may run
-// interchanges concurrently (the main and the lookahead stream).
-int* laswp_table(cudaStream_t st) {
-  int* base = (int*)ws_get(WS_PANEL, sizeof(int) * 2 * LASWP_TABLE_INTS + 256);
-  if (!base) return nullptr;
-  return base + (st == ctx().side ? LASWP_TABLE_INTS : 0);
-}
 
 template <typename T>
 int laswp_blocked(T* A, long ld, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
                   bool reverse, bool tr, cudaStream_t st) {
   const int ncols = n0 + n1;
-  int* table = laswp_table(st);
-  if (!table) return FLA_FAILURE;
   const int ps = prof_begin(st);
-  laswp_compose_kernel<<<1, 256, 0, st>>>(d_piv, npiv, reverse ? 1 : 0, table);
   const unsigned grid = (unsigned)((ncols + LASWP_NC - 1) / LASWP_NC);
   if (tr)
-    laswp_apply_kernel<T, true><<<grid, 256, 0, st>>>(A, ld, row0, table, c0, n0, c1, n1);
+    laswp_apply_kernel<T, true><<<grid, 256, 0, st>>>(A, ld, row0, d_piv, npiv, reverse ? 1 : 0, c0, n0, c1, n1);
   else
-    laswp_apply_kernel<T, false><<<grid, 256, 0, st>>>(A, ld, row0, table, c0, n0, c1, n1);
+    laswp_apply_kernel<T, false><<<grid, 256, 0, st>>>(A, ld, row0, d_piv, npiv, reverse ? 1 : 0, c0, n0, c1, n1);
   prof_end(ps, st, PROF_SWAP, 0.0);
-  count_launch(2);
+  count_launch();
   FB_CK(cudaGetLastError());
   return FLA_SUCCESS;
 }
