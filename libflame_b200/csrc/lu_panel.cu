@@ -58,6 +58,7 @@ struct LeafArgs {
   int gcol;    // global column of leaf column 0 (for info)
   int* piv;    // out: w relative pivots
   int* info;   // atomicMin of the first zero-pivot column
+  int* err;    // wait-timeout flag (register-resident leaf)
 };
 
 // Shared-memory layout of one CTA (doubles unless noted):
@@ -317,13 +318,16 @@ __device__ __forceinline__ double rleaf_pick(const double (&rv)[RPT][W], int k, 
   return v;
 }
 
-// Lane `src` of the calling warp holds the row (slot k); every lane gets it
-// by shuffles and lanes d < C store it into CTA d's buffer at dst.
+// Lane `src` of the calling warp holds the row (slot k; have = false pushes
+// zeros); every lane gets it by shuffles and lane d < C stores it into CTA
+// d's buffer at local offset `dst` with st.async, completing bytes on CTA
+// d's mbarrier `bar` (both shared::cta addresses of this CTA, mapped).
 template <int W, int RPT>
-__device__ __forceinline__ void rleaf_push_row(const double (&rv)[RPT][W], int k, int src, double* dst, int C,
-                                               cg::cluster_group& cluster) {
+__device__ __forceinline__ void rleaf_push_row(const double (&rv)[RPT][W], int k, int src, bool have, uint32_t dst,
+                                               uint32_t bar, int C) {
   const int lane = threadIdx.x & 31;
-  double* d = cluster.map_shared_rank(dst, lane < C ? lane : 0);
+  const uint32_t rank = (uint32_t)(lane < C ? lane : 0);
+  const uint32_t rdst = mapa_shared(dst, rank), rbar = mapa_shared(bar, rank);
 #pragma unroll
   for (int q0 = 0; q0 < W; q0 += 4) {
     double row[4];
@@ -331,7 +335,7 @@ __device__ __forceinline__ void rleaf_push_row(const double (&rv)[RPT][W], int k
     for (int q = 0; q < 4; ++q) row[q] = __shfl_sync(0xffffffffu, rleaf_pick<W, RPT>(rv, k, q0 + q), src);
     if (lane < C)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) d[q0 + q] = row[q];
+      for (int q = 0; q < 4; ++q) st_async_f64(rdst + 8 * (q0 + q), have ? row[q] : 0.0, rbar);
   }
 }
 
@@ -407,6 +411,18 @@ __global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs 
   int* xidx = reinterpret_cast<int*>(rowj + 2 * W);  // [2][C] candidate rows (INT_MAX: none)
   const int r0 = c * a.R;
   const int rows = max(0, min(a.R, a.M - r0));
+  // full[p]: the exchange buffers of parity p are complete (armed by thread
+  // 0 with the bytes expected per column, completed by the st.async pushes)
+  __shared__ __align__(8) unsigned long long s_full[2];
+  const uint32_t full0 = smem_u32(&s_full[0]);
+  const uint32_t xrow_s = smem_u32(xrow), xval_s = smem_u32(xval), rowj_s = smem_u32(rowj), xidx_s = smem_u32(xidx);
+  const uint32_t col_bytes = (uint32_t)(C * (8 * W + 8 + 4) + 8 * W);
+  if (tid == 0) {
+    mbar_init(full0, 1);
+    mbar_init(full0 + 8, 1);
+    fence_barrier_init();
+  }
+  cluster.sync();  // every CTA's barriers exist before the first push
 
   double rv[RPT][W];
 #pragma unroll
@@ -457,21 +473,32 @@ __global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs 
       bv = v;
       bi = i0;
     }
-    // ---- 2. push the candidate row and row j to every CTA
-    if (bi != INT_MAX) {
-      const int li = bi - r0, ot = li & (RLEAF_THREADS - 1);
-      if (li >= 0 && li < rows && warp == (ot >> 5))
-        rleaf_push_row<W, RPT>(rv, li / RLEAF_THREADS, ot & 31, xrow + ((size_t)par * C + c) * W, C, cluster);
+    // ---- 2. push the candidate row (zeros when this CTA has none), its
+    // magnitude and row, and row j (by its owner) into every CTA with
+    // st.async; each CTA waits for the column's bytes on its own mbarrier
+    const uint32_t fullp = full0 + 8 * par;
+    {
+      const bool have = bi != INT_MAX && bi - r0 >= 0 && bi - r0 < rows;
+      const int li = have ? bi - r0 : 0, ot = li & (RLEAF_THREADS - 1);
+      if (warp == (ot >> 5))
+        rleaf_push_row<W, RPT>(rv, li / RLEAF_THREADS, ot & 31, have,
+                               xrow_s + 8u * (uint32_t)((par * C + c) * W), fullp, C);
     }
-    if (warp == 0 && lane < C) {
-      *cluster.map_shared_rank(xval + par * C + c, lane) = bv;
-      *cluster.map_shared_rank(xidx + par * C + c, lane) = bi;
+    if (warp == NW - 1 && lane < C) {
+      const uint32_t rbar = mapa_shared(fullp, (uint32_t)lane);
+      st_async_f64(mapa_shared(xval_s + 8u * (uint32_t)(par * C + c), (uint32_t)lane), bv, rbar);
+      st_async_b32(mapa_shared(xidx_s + 4u * (uint32_t)(par * C + c), (uint32_t)lane), (uint32_t)bi, rbar);
     }
     if (j >= r0 && j < r0 + rows) {
       const int lj = j - r0, jt = lj & (RLEAF_THREADS - 1);
-      if (warp == (jt >> 5)) rleaf_push_row<W, RPT>(rv, lj / RLEAF_THREADS, jt & 31, rowj + par * W, C, cluster);
+      if (warp == (jt >> 5))
+        rleaf_push_row<W, RPT>(rv, lj / RLEAF_THREADS, jt & 31, true, rowj_s + 8u * (uint32_t)(par * W), fullp, C);
     }
-    cluster.sync();
+    if (tid == 0) mbar_arrive_expect_tx(fullp, col_bytes);
+    // every thread waits with cluster-scope acquire; the CTA leaves the loop
+    // together if the (bounded) wait ran out
+    const bool got = mbar_wait_cluster(fullp, (uint32_t)((j >> 1) & 1), a.err, 21);
+    if (!__syncthreads_and(got ? 1 : 0)) break;
     // ---- 3. winner (identical in every warp of every CTA: same data, same
     // order)
     int r, w0;
@@ -522,6 +549,8 @@ __global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs 
     // ---- 4. exchange, scale, update, next candidate
     rleaf_column_at<W, RPT>(j, rv, tid, r0, rows, r, u, oldj, 1.0 / piv, bv, bi);
   }
+  // no CTA leaves while another may still push into its shared memory
+  cluster.sync();
 #pragma unroll
   for (int k = 0; k < RPT; ++k) {
     const int i = tid + k * RLEAF_THREADS;
@@ -632,6 +661,7 @@ int rleaf_launch(double* P, long ld, long M, int w, int* d_piv, int gcol, cudaSt
   la.gcol = gcol;
   la.piv = d_piv;
   la.info = ctx().d_status + ST_INFO;
+  la.err = ctx().d_status + ST_ERROR;
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -707,6 +737,7 @@ int leaf_launch(double* P, long ld, long M, int w, int* d_piv, int gcol, bool rm
   la.gcol = gcol;
   la.piv = d_piv;
   la.info = ctx().d_status + ST_INFO;
+  la.err = ctx().d_status + ST_ERROR;
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
