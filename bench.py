@@ -232,14 +232,16 @@ def mixed_ir_section(torch, dev, F, n, nrhs):
                     r2 = L.FLA_LU_piv_solve(vW.obj, vp.obj, vB.obj, v64.obj)
                 m2 = F.last_op_ms()
                 if r1 != F.FLA_SUCCESS or r2 != F.FLA_SUCCESS:
-                    raise RuntimeError("FP64 form failed: %d %d %s" % (r1, r2, F.last_error()))
+                    raise RuntimeError("FP64 form failed (%s, kappa %.0e, rep %d): %d %d %s"
+                                       % (kind, kappa, rep, r1, r2, F.last_error()))
                 t64.append(m1 + m2)
                 if kind == "spd":
                     r, it, inner = F.chol_solve_mixed(A, B, Xmx, F.FLA_LOWER_TRIANGULAR)
                 else:
                     r, it, inner = F.lu_piv_solve_mixed(A, B, Xmx)
                 if r != F.FLA_SUCCESS:
-                    raise RuntimeError("mixed solver failed: %d %s" % (r, F.last_error()))
+                    raise RuntimeError("mixed solver failed (%s, kappa %.0e, rep %d): %d %s"
+                                       % (kind, kappa, rep, r, F.last_error()))
                 tmx.append(F.last_op_ms())
                 rec = {"iter": it, "path": "fp16 factors + refinement" if it >= 0 else "FP64 fallback"}
             f64, fmx = min(t64), min(tmx)
@@ -384,8 +386,9 @@ def gp_section(torch, dev, F, n):
     K = torch.exp(-torch.cdist(x, x) ** 2 / (2 * 0.3 ** 2)) + 1e-2 * torch.eye(n, dtype=torch.float64, device=dev)
     y = torch.randn((n, 1), dtype=torch.float64, device=dev, generator=g)
     Ld = K.clone().t().contiguous().t()
-    if F.chol(Ld) != F.FLA_SUCCESS:
-        raise RuntimeError("FLA_Chol failed: %s" % F.last_error())
+    rc = F.chol(Ld)
+    if rc != F.FLA_SUCCESS:
+        raise RuntimeError("FLA_Chol returned %d: %s" % (rc, F.last_error()))
     t_chol = F.last_op_ms()
     Ld = torch.tril(Ld).t().contiguous().t()
     v = torch.linalg.solve_triangular(Ld, y, upper=False)

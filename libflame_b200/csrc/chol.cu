@@ -178,16 +178,16 @@ int chol_blocksize() {
   return nb;
 }
 
-// Enqueue the blocked factorization of the lower triangle of A on `st`, with
-// a lookahead of one panel when `st` is the library's main stream.  Outer
-// blocks of NBO = 128 or 256 columns; each outer panel is factored as
+// Enqueue the blocked factorization of the lower triangle of A on `st`.
+// Outer blocks of NBO = 128 or 256 columns; each outer panel is factored as
 // 128-column sub-panels:
-//   sub-panel j (side stream): A11 := chol(A11); inv(L11) formed next to it;
-//                              A21 := A21 inv(L11)^T as a DMMA GEMM;
-//                              the panel's later columns -= A21 A21^T
-//   main stream, step k:       A22(:, next panel) -= A21 A21(next rows)^T,
-//                              then the next panel goes to the side stream,
-//                              A22(rest) -= A21 A21^T (lower) concurrently.
+//   sub-panel j:   A11 := chol(A11); inv(L11) formed next to it;
+//                  A21 := A21 inv(L11)^T as a DMMA GEMM;
+//                  the panel's later columns -= A21 A21^T
+//   then the panel's rows below its diagonal block are copied transposed,
+//   and step k updates A22(:, next panel) -= A21 A21(next rows)^T, factors
+//   the next panel, and updates A22(rest) -= A21 A21^T (lower), all in
+//   stream order.
 // Failure semantics follow FLA_Chol_l_blk_var3: the updates of step k run
 // unless a column before k + b has failed (the guard limit of each launch),
 // so a failure in the next panel does not cut short step k's update.
@@ -197,12 +197,26 @@ int chol_lower_enqueue(DMat A, cudaStream_t st) {
   const long n = A.m, ld = A.ld;
   if (n <= 0) return FLA_SUCCESS;
   int* info = cx.d_status + ST_INFO;
-  const bool lookahead = (st == cx.stream);
-  cudaStream_t sd = lookahead ? cx.side : st;
+  // Panels run on the same stream as the updates.  Running them on the
+  // library's second stream beside the trailing update (as FLA_LU_piv does)
+  // gave occasional wrong tiles in the concurrently running trailing-update
+  // GEMM on B200 (about 2 in 100 factorizations at n = 16384, seen as
+  // run-to-run differences of the factor and as false failures on
+  // ill-conditioned SPD matrices); with the panels in stream order every run
+  // is bitwise identical.  The cause is not identified, so the overlap stays
+  // off for the Cholesky.
+  cudaStream_t sd = st;
   const long NBO = chol_blocksize();
   double* Linv = (double*)ws_get(WS_MISC, sizeof(double) * NB * NB);
   double* W = (double*)ws_get(WS_MISC2, sizeof(double) * NB * (size_t)(std::max<long>(0, n - NB) + 2));
-  if (!Linv || !W) return FLA_FAILURE;
+  // Transposed copy of each factored outer panel's rows below its diagonal
+  // block (NBO x rows, k contiguous), two buffers used in turn: the
+  // lookahead and trailing updates take their second operand from it
+  // k-contiguous (one 16 x 64 TMA box per stage, the LU's operand shape).
+  const long ldpt = NBO;
+  double* PT = (double*)ws_get(WS_PANEL_T, sizeof(double) * 2 * (size_t)ldpt * (size_t)std::max<long>(n, 1));
+  if (!Linv || !W || !PT) return FLA_FAILURE;
+  auto pt_of = [&](long k) { return PT + ((k / NBO) & 1) * (size_t)ldpt * (size_t)n; };
   cudaEvent_t ev_look = cx.ev[2], ev_panel = cx.ev[3];
   auto at = [&](long i, long j) { return A.p + i + j * ld; };
 
@@ -226,7 +240,8 @@ int chol_lower_enqueue(DMat A, cudaStream_t st) {
                     (int)(k + b));
   };
   // Outer panel at column k: its sub-panels left to right, each followed by
-  // the update of the panel's remaining columns.
+  // the update of the panel's remaining columns; then the transposed copy of
+  // its rows below the diagonal block.
   auto panel = [&](long k, cudaStream_t s) -> int {
     const long kend = std::min<long>(n, k + NBO);
     for (long j = k; j < kend; j += NB) {
@@ -237,6 +252,8 @@ int chol_lower_enqueue(DMat A, cudaStream_t st) {
                    GEMM_LOWER, 0, info, (int)j2) != FLA_SUCCESS)
         return FLA_FAILURE;
     }
+    if (n > kend)
+      return transpose_dev(at(kend, k), ld, pt_of(k), ldpt, n - kend, kend - k, false, s);
     return FLA_SUCCESS;
   };
 
@@ -247,8 +264,10 @@ int chol_lower_enqueue(DMat A, cudaStream_t st) {
     if (m2 <= 0) break;
     const int lim = (int)(k + b);
     const long nb2 = std::min<long>(NBO, m2);
-    // the next panel's columns first
-    if (gemm_f64(st, false, true, m2, nb2, b, -1.0, at(k + b, k), ld, at(k + b, k), ld, 1.0, at(k + b, k + b), ld,
+    // the next panel's columns first; op(B) = panel^T from its transposed copy
+    // (column c of the copy is panel row k + b + c)
+    const double* pt = pt_of(k);
+    if (gemm_f64(st, false, false, m2, nb2, b, -1.0, at(k + b, k), ld, pt, ldpt, 1.0, at(k + b, k + b), ld,
                  GEMM_LOWER, 0, info, lim) != FLA_SUCCESS)
       return FLA_FAILURE;
     FB_CK(cudaEventRecord(ev_look, st));
@@ -256,7 +275,7 @@ int chol_lower_enqueue(DMat A, cudaStream_t st) {
     if (panel(k + b, sd) != FLA_SUCCESS) return FLA_FAILURE;
     FB_CK(cudaEventRecord(ev_panel, sd));
     if (m2 > nb2 &&
-        gemm_f64(st, false, true, m2 - nb2, m2 - nb2, b, -1.0, at(k + b + nb2, k), ld, at(k + b + nb2, k), ld, 1.0,
+        gemm_f64(st, false, false, m2 - nb2, m2 - nb2, b, -1.0, at(k + b + nb2, k), ld, pt + nb2 * ldpt, ldpt, 1.0,
                  at(k + b + nb2, k + b + nb2), ld, GEMM_LOWER, 0, info, lim) != FLA_SUCCESS)
       return FLA_FAILURE;
     FB_CK(cudaStreamWaitEvent(st, ev_panel, 0));

@@ -50,7 +50,8 @@ inline void count_launch(unsigned n = 1) { ctx().launches += n; }
 enum ProfClass : int { PROF_GEMM = 0, PROF_PANEL, PROF_TRSM, PROF_SWAP, PROF_DIAG, PROF_OTHER, PROF_NCLASS };
 void op_begin(cudaStream_t st);
 void op_end(cudaStream_t st);
-void op_hold(bool on);  // keep the current op window open across nested drivers
+void op_hold(bool on);      // keep the current op window open across nested drivers
+void order_after_caller();  // main stream waits for the caller's default-stream work
 bool prof_on();
 int prof_begin(cudaStream_t st);                       // returns a slot or -1
 void prof_end(int slot, cudaStream_t st, int cls, double flops);
@@ -102,6 +103,7 @@ enum WsSlot : int {
   WS_TRINV,         // inverted diagonal blocks of the solves
   WS_SOLVE_W,       // block of solved unknowns
   WS_SPLITK,        // partial products of split-K GEMMs
+  WS_PANEL_T,       // transposed copies of Cholesky panels (two, ping-pong)
   WS_NSLOTS
 };
 void* ws_get(int slot, size_t bytes);  // nullptr on allocation failure

@@ -105,8 +105,23 @@ static unsigned long long g_prof_n[PROF_NCLASS];
 static bool g_op_hold = false;
 void op_hold(bool on) { g_op_hold = on; }
 
+// The library's streams are non-blocking, so they are not ordered after
+// work the caller left on the default stream (a tensor library producing the
+// input, a pending copy).  Every call first makes its main stream wait for
+// an event recorded on the legacy default stream, which completes after all
+// work previously issued to it and to every blocking stream: the call then
+// sees the caller's data as a synchronous CPU library would.  (A caller
+// producing the input on its own non-blocking stream synchronizes first.)
+void order_after_caller() {
+  static cudaEvent_t ev = nullptr;
+  if (!ev) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  cudaEventRecord(ev, cudaStreamLegacy);
+  cudaStreamWaitEvent(ctx().stream, ev, 0);
+}
+
 void op_begin(cudaStream_t st) {
   if (g_op_hold) return;
+  order_after_caller();
   if (!g_op_ev[0]) {
     cudaEventCreate(&g_op_ev[0]);
     cudaEventCreate(&g_op_ev[1]);
@@ -209,6 +224,7 @@ static size_t dt_size(FLA_Datatype dt) {
 
 int stage(const FLA_Obj& A, int slot, Staged* s, bool copy_in, bool need_align) {
   Context& c = ctx();
+  order_after_caller();
   s->m = (long)A.m;
   s->n = (long)A.n;
   s->esize = dt_size(A.base->datatype);
