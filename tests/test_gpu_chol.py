@@ -108,3 +108,25 @@ def test_dpotrf_lapack_abi(cuda, flame, golden):
     n = C.c_int(b.shape[0])
     flame.lib().dpotrf_(C.c_char_p(b"L"), C.byref(n), b.ctypes.data_as(C.c_void_p), C.byref(n), C.byref(info))
     assert info.value == int(golden["chol_fail_r"]) + 1
+
+
+def test_chol_bitwise_repeatable(cuda, flame):
+    """Five factorizations of one SPD matrix (n = 4096, several outer
+    panels and trailing updates) give bitwise identical factors: no
+    ordering-dependent work between the panel and the updates."""
+    torch = cuda
+    n = 4096
+    g = torch.Generator(device="cuda").manual_seed(3)
+    G = torch.randn((n, n), dtype=torch.float64, device="cuda", generator=g) / n ** 0.5
+    S = G @ G.t() + torch.eye(n, dtype=torch.float64, device="cuda")
+    W = torch.empty_like(S).t()
+    ref = None
+    for _ in range(5):
+        W.copy_(S)
+        torch.cuda.synchronize()
+        assert flame.chol(W) == flame.FLA_SUCCESS
+        L = torch.tril(W)
+        if ref is None:
+            ref = L.clone()
+        else:
+            assert torch.equal(L, ref)

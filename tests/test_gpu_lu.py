@@ -109,3 +109,24 @@ def test_dgetrf_lapack_abi(cuda, flame, golden):
     assert info.value == 0
     assert np.array_equal(ipiv, golden["dgetrf_ipiv"])
     assert rel_fro(a, golden["dgetrf_LU"]) < FACTOR_TOL
+
+
+def test_lu_bitwise_repeatable(cuda, flame):
+    """Five factorizations of one matrix (n = 4096, panels on the second
+    stream beside the trailing updates) give bitwise identical factors and
+    pivots."""
+    torch = cuda
+    n = 4096
+    g = torch.Generator(device="cuda").manual_seed(4)
+    A = torch.rand((n, n), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    W = torch.empty_like(A).t()
+    p = torch.empty(n, dtype=torch.int32, device="cuda")
+    ref = refp = None
+    for _ in range(5):
+        W.copy_(A.t())
+        torch.cuda.synchronize()
+        assert flame.lu_piv(W, p) == flame.FLA_SUCCESS
+        if ref is None:
+            ref, refp = W.clone(), p.clone()
+        else:
+            assert torch.equal(W, ref) and torch.equal(p, refp)
