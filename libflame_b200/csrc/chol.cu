@@ -203,8 +203,11 @@ int chol_lower_enqueue(DMat A, cudaStream_t st) {
   // GEMM on B200 (about 2 in 100 factorizations at n = 16384, seen as
   // run-to-run differences of the factor and as false failures on
   // ill-conditioned SPD matrices); with the panels in stream order every run
-  // is bitwise identical.  The cause is not identified, so the overlap stays
-  // off for the Cholesky.
+  // is bitwise identical.  The wrong tiles came from the GEMM releasing a
+  // k-stage to its TMA refill before a warp's shared-memory loads had
+  // completed (fixed in dgemm_tma_kernel with fences before the release);
+  // the overlap stays off here until the fixed kernel has been run
+  // overlapped on a GPU that showed the failure.
   cudaStream_t sd = st;
   const long NBO = chol_blocksize();
   double* Linv = (double*)ws_get(WS_MISC, sizeof(double) * NB * NB);

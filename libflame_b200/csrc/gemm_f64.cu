@@ -222,6 +222,16 @@ __global__ void __launch_bounds__(Tile<BM_>::THREADS, Tile<BM_>::MINB)
 #pragma unroll
         for (int j = 0; j < 4; ++j) dmma_884(acc[i][j][0], acc[i][j][1], a[i], b[j]);
     }
+    // Release the stage.  Its refill is a TMA write (async proxy) issued as
+    // soon as the last warp arrives, so each lane first waits for its own
+    // shared-memory reads of the stage to complete (CTA fence) and orders
+    // them before async-proxy writes (proxy fence).  Without the fences a
+    // warp's last fragment loads could still be in flight when its arrive
+    // reached the barrier: with other kernels resident on the SM, a few tiles
+    // in 10^8 to 10^9 took one A fragment of one warp (8 rows x 32 columns of
+    // C) from the refilled stage.
+    __threadfence_block();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncwarp();
     if (lane == 0) mbar_arrive(empty0 + 8 * s);
   }
