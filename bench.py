@@ -510,7 +510,7 @@ def run_ours(args, rank, world):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": "FLA_LU_piv n=%d FP64, A iid U(-1,1) seeded, column-major in HBM" % n,
-                       "n": n, "blocksize": 128, "chol_blocksize": 256, "parallelism": "replicas" if world > 1 else "single",
+                       "n": n, "blocksize": 128, "chol_blocksize": 256, "chol_lookahead": True, "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs (2 GiB) larger than L2; the per-step restore of A also flushes L2"},
             "roofline": roofline, "breakdown_ms": breakdown,
             "gpu_launches": launches, "clocks": clocks,

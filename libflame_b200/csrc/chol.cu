@@ -186,8 +186,8 @@ int chol_blocksize() {
 //                  the panel's later columns -= A21 A21^T
 //   then the panel's rows below its diagonal block are copied transposed,
 //   and step k updates A22(:, next panel) -= A21 A21(next rows)^T, factors
-//   the next panel, and updates A22(rest) -= A21 A21^T (lower), all in
-//   stream order.
+//   the next panel on the second stream, and meanwhile updates
+//   A22(rest) -= A21 A21^T (lower) on the main stream.
 // Failure semantics follow FLA_Chol_l_blk_var3: the updates of step k run
 // unless a column before k + b has failed (the guard limit of each launch),
 // so a failure in the next panel does not cut short step k's update.
@@ -197,18 +197,15 @@ int chol_lower_enqueue(DMat A, cudaStream_t st) {
   const long n = A.m, ld = A.ld;
   if (n <= 0) return FLA_SUCCESS;
   int* info = cx.d_status + ST_INFO;
-  // Panels run on the same stream as the updates.  Running them on the
-  // library's second stream beside the trailing update (as FLA_LU_piv does)
-  // gave occasional wrong tiles in the concurrently running trailing-update
-  // GEMM on B200 (about 2 in 100 factorizations at n = 16384, seen as
-  // run-to-run differences of the factor and as false failures on
-  // ill-conditioned SPD matrices); with the panels in stream order every run
-  // is bitwise identical.  The wrong tiles came from the GEMM releasing a
-  // k-stage to its TMA refill before a warp's shared-memory loads had
-  // completed (fixed in dgemm_tma_kernel with fences before the release);
-  // the overlap stays off here until the fixed kernel has been run
-  // overlapped on a GPU that showed the failure.
-  cudaStream_t sd = st;
+  // The next panel is factored on the library's second stream beside the
+  // trailing update (as in FLA_LU_piv); FLA_B200_CHOL_LOOKAHEAD=0 keeps the
+  // panels in stream order.  Only calls on the library's main stream
+  // overlap; a call on another stream runs in that stream's order.
+  static const bool look = [] {
+    const char* e = std::getenv("FLA_B200_CHOL_LOOKAHEAD");
+    return !(e && e[0] == '0');
+  }();
+  cudaStream_t sd = (look && st == cx.stream) ? cx.side : st;
   const long NBO = chol_blocksize();
   double* Linv = (double*)ws_get(WS_MISC, sizeof(double) * NB * NB);
   double* W = (double*)ws_get(WS_MISC2, sizeof(double) * NB * (size_t)(std::max<long>(0, n - NB) + 2));
