@@ -42,6 +42,18 @@ int           FLA_B200_dgemm( int transa, int transb, long m, long n, long k, do
                               const double* A, long lda, const double* B, long ldb,
                               double beta, double* C, long ldc, int lower_only );
 
+/* No counterpart in the reference libflame.  Concurrency self-test of the
+ * FP64 GEMM engine: `iters` times, C := C - A B (m x n x k, beta = 1, the
+ * factorizations' trailing-update shape) on the library's main stream while
+ * its second stream runs Cholesky-panel work (diagonal-block factorization,
+ * triangle inverse, panel GEMMs, transpose), as the lookahead of FLA_Chol
+ * and FLA_LU_piv does; every result is compared bitwise with the update
+ * computed alone and *mismatches receives the number of differing elements
+ * summed over all iterations (0 on a correct GPU).  Allocates its operands
+ * (about 3 m n doubles) and frees them before returning. */
+int           FLA_B200_gemm_concurrency_check( long m, long n, long k, int iters,
+                                               unsigned long long* mismatches );
+
 /* No counterpart in the reference libflame.  LU factorization with partial
  * pivoting of one m x n panel (n <= 128, m >= n) held in device memory (A,
  * column-major, lda >= m; piv receives n relative zero-based pivots, as

@@ -74,6 +74,8 @@ _SIGS = {
     "FLA_B200_dgemm": (C.c_int, [C.c_int, C.c_int, C.c_long, C.c_long, C.c_long, C.c_double,
                                  C.c_void_p, C.c_long, C.c_void_p, C.c_long, C.c_double,
                                  C.c_void_p, C.c_long, C.c_int]),
+    "FLA_B200_gemm_concurrency_check": (C.c_int, [C.c_long, C.c_long, C.c_long, C.c_int,
+                                                  C.POINTER(C.c_ulonglong)]),
     "FLA_B200_LU_piv_solve_mixed": (C.c_int, [FLA_Obj, FLA_Obj, FLA_Obj, C.c_int, C.c_int,
                                               C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "FLA_B200_Chol_solve_mixed": (C.c_int, [C.c_int, FLA_Obj, FLA_Obj, FLA_Obj, C.c_int, C.c_int,

@@ -99,3 +99,22 @@ def test_dgemm_lower_mode_many_tiles(cuda, flame):
     low = torch.tril(torch.ones(n, n, dtype=torch.bool, device="cuda"))
     assert (got[low] - ref[low]).abs().max().item() < 1e-12
     assert torch.equal(got[~low], Cm[~low])
+
+
+def test_gemm_concurrent_with_panel_work(flame):
+    """The trailing-update GEMM with Cholesky-panel kernels beside it on the
+    library's second stream (the factorizations' lookahead): 3000 updates of
+    8192 x 8192 x 128, each bitwise equal to the update computed alone.  A
+    stage-release race in the GEMM's shared-memory pipeline once gave, on
+    some B200s, about one wrong tile per 3000 such updates (8 rows x 32
+    columns fed by one warp's A fragment)."""
+    bad = C.c_ulonglong(12345)
+    rc = flame.lib().FLA_B200_gemm_concurrency_check(8192, 8192, 128, 3000, C.byref(bad))
+    assert rc == flame.FLA_SUCCESS, flame.last_error()
+    assert bad.value == 0
+
+
+def test_gemm_concurrency_check_rejects_bad_arguments(flame):
+    bad = C.c_ulonglong(0)
+    assert flame.lib().FLA_B200_gemm_concurrency_check(0, 8, 8, 1, C.byref(bad)) == flame.FLA_FAILURE
+    assert flame.lib().FLA_B200_gemm_concurrency_check(8, 8, 8, 1, None) == flame.FLA_FAILURE
