@@ -539,7 +539,7 @@ def run_ours(args, rank, world):
                          "path": "dgetrf_ on pinned host buffers (wall clock, includes H2D + D2H)"}
         del pinned, host_src
 
-    # ---- secondary: FP64 FLA_Chol at n=16384 (north-star target)
+    # ---- secondary: FP64 FLA_Chol at n=16384 (target: >= 70 % of the FP64 tensor peak)
     if rank == 0 and not args.no_secondary:
         del src
         G = torch.randn((n, n), dtype=torch.float64, device=dev, generator=g)

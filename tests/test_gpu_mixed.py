@@ -1,7 +1,7 @@
 """Mixed-precision solvers (16-bit tensor-core factorization, FP64
 refinement) against the FP64 oracle.
 
-Bars (north-star: "reach the FP64 form's backward error"): the normwise
+Bars (the mixed solution must reach the FP64 form's backward error): the normwise
 backward error max_c ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) of
 the mixed solution is at most 4x that of the oracle's FP64 LU/Cholesky
 solution on the same system (and below 1e-15 absolute slack), and the
