@@ -494,9 +494,9 @@ def run_ours(args, rank, world):
             "frac": achieved / peak if achieved else None,
             "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul fp64) measured in this run; "
                            "MEASURED_PEAKS.json has no FP64 figure",
-            # DRAM bytes per launch: the ncu capture's bytes per flop (0.0574,
-            # profiles/dgemm_tma_kernel_lu_n6144.md) times this run's average
-            # launch; algorithmic bytes per launch (C read + write) beside it
+            # DRAM bytes per launch: 0.0574 bytes per flop (dram__bytes_read
+            # + write of an ncu capture of this kernel in an n = 6144 LU)
+            # times this run's average launch
             "traffic": 0.0574 * gemm_flops / gemm_n if gemm_n else None,
             "traffic_unit": "bytes per launch (ncu DRAM read + write, scaled per flop from n=6144)",
             "launches_per_step": gemm_n,

@@ -186,6 +186,11 @@ def kernel_launches():
     return int(lib().FLA_B200_kernel_launches())
 
 
+def num_sms():
+    """SM count of the device bound at FLA_Init."""
+    return int(lib().FLA_B200_num_sms())
+
+
 def last_op_ms():
     """Device time of the last factorization/solve call (CUDA events)."""
     return float(lib().FLA_B200_last_op_ms())

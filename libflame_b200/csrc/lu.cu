@@ -136,8 +136,16 @@ __global__ void __launch_bounds__(PANEL_THREADS) lu_panel_kernel(PanelArgs a) {
       if (lane == 0) { s_w = w0; s_r = i0; }
     }
     __syncthreads();
-    const int w = s_w, r = s_r;
+    const int w = s_w;
+    int r = s_r;
     const double* wrow = a.cand_row + ((size_t)par * G + w) * nb;
+    if (r == INT_MAX) {
+      // no orderable candidate (every magnitude NaN): keep row j, as idamax
+      // does when no later entry compares greater than the first; row j was
+      // published by its owner before the barrier
+      r = j;
+      wrow = a.diag_row + par * nb;
+    }
     for (int col = tid; col < nb; col += PANEL_THREADS) su[col] = __ldcg(wrow + col);
     __syncthreads();
     const double piv = su[j];
@@ -773,6 +781,14 @@ extern "C" int FLA_B200_LU_piv_panel_noalloc(int m, int n, double* A, int lda, i
   }
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   noalloc_reset_kernel<<<1, 1, 0, st>>>(s);
+  {
+    const cudaError_t re = cudaGetLastError();
+    if (re != cudaSuccess) {
+      set_last_error(std::string("FLA_B200_LU_piv_panel_noalloc: reset launch failed: ") +
+                     cudaGetErrorString(re));
+      return FLA_FAILURE;
+    }
+  }
   count_launch();
   PanelArgs pa;
   pa.P = A;

@@ -614,8 +614,6 @@ int mixed_solve_dev(bool chol, bool upper, DMat A, DMat B, DMat X, int* d_piv, c
     code = -(cfg.itermax + 1);
   }
   *iter = code;
-  bool fallback = true;
-  (void)fallback;
   // FP64 factorization (in place, or on a copy when A must stay unchanged)
   DMat Af = A;
   if (!overwrite_a) {
@@ -661,8 +659,9 @@ extern "C" {
 // src/map/common/lapacksrc/f2c/dsgesv.c:189-412: same arguments, checks and
 // ITER/INFO conventions; the single-precision factorization is the 16-bit
 // tensor-core LU (format and refinement from FLA_B200_IR_PREC /
-// FLA_B200_IR_SOLVER, default FP16 with equilibration and GMRES-IR).  work
-// and swork are not referenced (the library keeps its own workspace).
+// FLA_B200_IR_SOLVER; by default FP16 with equilibration and the adaptive
+// refinement of FLA_B200_LU_piv_solve_mixed).  work and swork are not
+// referenced (the library keeps its own workspace).
 int dsgesv_(int* n, int* nrhs, double* a, int* lda, int* ipiv, double* b, int* ldb, double* x, int* ldx,
             double* work, float* swork, int* iter, int* info) {
   (void)work;
