@@ -221,6 +221,16 @@ FLA_Error     FLA_Apply_Q_UT( FLA_Side side, FLA_Trans trans, FLA_Direct direct,
 /* src/lapack/util/app/qut/front/flamec/FLA_Apply_Q_UT_create_workspace.c:13-25. */
 FLA_Error     FLA_Apply_Q_UT_create_workspace( FLA_Obj T, FLA_Obj B, FLA_Obj* W );
 
+/* src/lapack/dec/q/qrut/front/flamec/FLA_QR_UT_form_Q.c:13-86.  Q (as many
+ * rows as A) := the first width(Q) columns of H(0) H(1) ... from the factor
+ * in A and T; Q may be A itself (formed in place). */
+FLA_Error     FLA_QR_UT_form_Q( FLA_Obj A, FLA_Obj T, FLA_Obj Q );
+
+/* src/lapack/util/accum/tut/front/flamec/FLA_Accum_T_UT.c:13.  Supported:
+ * FLA_FORWARD, FLA_COLUMNWISE.  T (b x k) := striu(U^T U) + diag(t) per
+ * block of b reflectors stored below the diagonal of A, t libflame's tau. */
+FLA_Error     FLA_Accum_T_UT( FLA_Direct direct, FLA_Store storev, FLA_Obj A, FLA_Obj t, FLA_Obj T );
+
 /* ---- solves ------------------------------------------------------------- */
 /* src/lapack/dec/chol/front/flamec/FLA_Chol_solve.c:13-35: X := inv(A) B
  * with A holding the Cholesky factor from FLA_Chol(uplo, .). */
@@ -228,6 +238,25 @@ FLA_Error     FLA_Chol_solve( FLA_Uplo uplo, FLA_Obj A, FLA_Obj B, FLA_Obj X );
 
 /* src/lapack/dec/lu/piv/front/flamec/FLA_LU_piv_solve.c:13-29. */
 FLA_Error     FLA_LU_piv_solve( FLA_Obj A, FLA_Obj p, FLA_Obj B, FLA_Obj X );
+
+/* src/lapack/dec/q/qrut/front/flamec/FLA_QR_UT_solve.c:13-49: least-squares
+ * X (n x nrhs) := inv(R) (Q^T B)(0:n-1, :) for the m x n (m >= n) factor
+ * from FLA_QR_UT; B is not modified. */
+FLA_Error     FLA_QR_UT_solve( FLA_Obj A, FLA_Obj T, FLA_Obj B, FLA_Obj X );
+
+/* ---- inversion ----------------------------------------------------------- */
+/* src/lapack/inv/tri/front/flamec/FLA_Trinv.c:17-50: the uplo triangle of A
+ * := its inverse (unit: diagonal taken as ones, not referenced).  Returns
+ * FLA_SUCCESS (no singularity check, as the reference's variants). */
+FLA_Error     FLA_Trinv( FLA_Uplo uplo, FLA_Diag diag, FLA_Obj A );
+
+/* src/lapack/misc/ttmm/front/flamec/FLA_Ttmm.c:17-43: lower: tril(A) :=
+ * tril(L^T L), L = tril(A); upper: triu(A) := triu(U U^T). */
+FLA_Error     FLA_Ttmm( FLA_Uplo uplo, FLA_Obj A );
+
+/* src/lapack/inv/spd/front/flamec/FLA_SPDinv.c:15-28: the uplo triangle of
+ * the SPD matrix A := that triangle of inv(A) (Chol, Trinv, Ttmm). */
+FLA_Error     FLA_SPDinv( FLA_Uplo uplo, FLA_Obj A );
 
 /* src/lapack/util/app/piv/front/flamec/FLA_Apply_pivots.c: side FLA_LEFT,
  * trans FLA_NO_TRANSPOSE (P A) or FLA_TRANSPOSE (P^T A). */
@@ -244,6 +273,16 @@ int dpotrf_( char* uplo, int* n, double* a, int* lda, int* info );
 int dgetrf_( int* m, int* n, double* a, int* lda, int* ipiv, int* info );
 /* src/map/lapack2flamec/FLA_geqrf.c:24-88 (tau is LAPACK's tau) */
 int dgeqrf_( int* m, int* n, double* a, int* lda, double* tau, double* work, int* lwork, int* info );
+/* src/map/lapack2flamec/FLA_ormqr.c:35-97: C := op(Q) C or C op(Q), Q from
+ * dgeqrf_'s k reflectors (A, tau); work only answers the size query. */
+int dormqr_( char* side, char* trans, int* m, int* n, int* k, double* a, int* lda, double* tau,
+             double* c, int* ldc, double* work, int* lwork, int* info );
+/* src/map/lapack2flamec/FLA_orgqr.c:30-80: A (m x n) := the first n columns
+ * of Q from dgeqrf_'s first k reflectors in A and tau. */
+int dorgqr_( int* m, int* n, int* k, double* a, int* lda, double* tau, double* work, int* lwork, int* info );
+/* src/map/lapack2flamec/FLA_potri.c:25-56: the uplo triangle of A (dpotrf_'s
+ * factor) := that triangle of inv(A). */
+int dpotri_( char* uplo, int* n, double* a, int* lda, int* info );
 /* src/map/common/lapacksrc/f2c/dpotrs.c, dgetrs.c */
 int dpotrs_( char* uplo, int* n, int* nrhs, double* a, int* lda, double* b, int* ldb, int* info );
 int dgetrs_( char* trans, int* n, int* nrhs, double* a, int* lda, int* ipiv, double* b, int* ldb, int* info );

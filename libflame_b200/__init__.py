@@ -64,6 +64,15 @@ _SIGS = {
     "FLA_Apply_Q_UT": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, FLA_Obj, FLA_Obj, FLA_Obj, FLA_Obj]),
     "FLA_Apply_Q_UT_create_workspace": (C.c_int, [FLA_Obj, FLA_Obj, C.POINTER(FLA_Obj)]),
     "FLA_LU_piv_solve": (C.c_int, [FLA_Obj, FLA_Obj, FLA_Obj, FLA_Obj]),
+    "FLA_QR_UT_solve": (C.c_int, [FLA_Obj, FLA_Obj, FLA_Obj, FLA_Obj]),
+    "FLA_QR_UT_form_Q": (C.c_int, [FLA_Obj, FLA_Obj, FLA_Obj]),
+    "FLA_Accum_T_UT": (C.c_int, [C.c_int, C.c_int, FLA_Obj, FLA_Obj, FLA_Obj]),
+    "FLA_Trinv": (C.c_int, [C.c_int, C.c_int, FLA_Obj]),
+    "FLA_Ttmm": (C.c_int, [C.c_int, FLA_Obj]),
+    "FLA_SPDinv": (C.c_int, [C.c_int, FLA_Obj]),
+    "dormqr_": (C.c_int, [C.c_char_p, C.c_char_p] + [C.c_void_p] * 11),
+    "dorgqr_": (C.c_int, [C.c_void_p] * 9),
+    "dpotri_": (C.c_int, [C.c_char_p] + [C.c_void_p] * 4),
     "FLA_B200_kernel_launches": (C.c_ulonglong, []),
     "FLA_B200_last_error": (C.c_char_p, []),
     "FLA_B200_num_sms": (C.c_int, []),
@@ -329,3 +338,90 @@ def chol_logdet_adjoint(L, Lbar, scale):
 def trsm_llnn_adjoint(L, X, Xbar, Lbar):
     vL, vX, vXb, vLb = View(L), View(X), View(Xbar), View(Lbar)
     return lib().FLA_B200_Trsm_llnn_adjoint(vL.obj, vX.obj, vXb.obj, vLb.obj)
+
+
+def qr_ut_solve(A, T, B, X):
+    """FLA_QR_UT_solve(A, T, B, X): least-squares X from the QR_UT factor."""
+    va, vt, vb, vx = View(A), View(T), View(B), View(X)
+    return lib().FLA_QR_UT_solve(va.obj, vt.obj, vb.obj, vx.obj)
+
+
+def qr_ut_form_q(A, T, Q):
+    """FLA_QR_UT_form_Q(A, T, Q); Q may be A itself (in place)."""
+    va, vt = View(A), View(T)
+    vq = va if Q is A else View(Q)
+    return lib().FLA_QR_UT_form_Q(va.obj, vt.obj, vq.obj)
+
+
+def accum_t_ut(A, t, T):
+    """FLA_Accum_T_UT(FORWARD, COLUMNWISE, A, t, T)."""
+    va, vt, vT = View(A), View(t), View(T)
+    return lib().FLA_Accum_T_UT(FLA_FORWARD, FLA_COLUMNWISE, va.obj, vt.obj, vT.obj)
+
+
+def trinv(A, uplo=FLA_LOWER_TRIANGULAR, diag=FLA_NONUNIT_DIAG):
+    va = View(A)
+    return lib().FLA_Trinv(uplo, diag, va.obj)
+
+
+def ttmm(A, uplo=FLA_LOWER_TRIANGULAR):
+    va = View(A)
+    return lib().FLA_Ttmm(uplo, va.obj)
+
+
+def spdinv(A, uplo=FLA_LOWER_TRIANGULAR):
+    va = View(A)
+    return lib().FLA_SPDinv(uplo, va.obj)
+
+
+def _buf(x):
+    """Raw pointer of a torch tensor or NumPy array (LAPACK entry points)."""
+    return C.c_void_p(x.data_ptr() if hasattr(x, "data_ptr") else x.ctypes.data)
+
+
+def _ld(x):
+    return max(1, x.stride(1) if hasattr(x, "stride") and x.dim() == 2 else x.shape[0])
+
+
+def dormqr(side, trans, a, tau, c):
+    """dormqr_ on column-major buffers (host or device); returns info."""
+    m, n = c.shape
+    k = tau.shape[0]
+    info = C.c_int(0)
+    nw = n if side == "L" else m
+    work = (C.c_double * max(1, nw))()
+    lw = C.c_int(len(work))
+    ints = [C.c_int(v) for v in (m, n, k, _ld(a), _ld(c))]
+    lib().dormqr_(side.encode(), trans.encode(), C.byref(ints[0]), C.byref(ints[1]), C.byref(ints[2]), _buf(a),
+                  C.byref(ints[3]), _buf(tau), _buf(c), C.byref(ints[4]), work, C.byref(lw), C.byref(info))
+    return info.value
+
+
+def dorgqr(a, tau):
+    """dorgqr_ in place on the m x n buffer a with k = len(tau); returns info."""
+    m, n = a.shape
+    k = tau.shape[0]
+    info = C.c_int(0)
+    work = (C.c_double * max(1, n))()
+    ints = [C.c_int(v) for v in (m, n, k, _ld(a), len(work))]
+    lib().dorgqr_(C.byref(ints[0]), C.byref(ints[1]), C.byref(ints[2]), _buf(a), C.byref(ints[3]), _buf(tau),
+                  work, C.byref(ints[4]), C.byref(info))
+    return info.value
+
+
+def dpotri(uplo, a):
+    n = a.shape[0]
+    info = C.c_int(0)
+    ni, ld = C.c_int(n), C.c_int(_ld(a))
+    lib().dpotri_(uplo.encode(), C.byref(ni), _buf(a), C.byref(ld), C.byref(info))
+    return info.value
+
+
+def dgeqrf(a, tau):
+    m, n = a.shape
+    info = C.c_int(0)
+    work = (C.c_double * max(1, n * 32))()
+    ints = [C.c_int(v) for v in (m, n, _ld(a), len(work))]
+    lib().dgeqrf_(C.byref(ints[0]), C.byref(ints[1]), _buf(a), C.byref(ints[2]), _buf(tau), work,
+                  C.byref(ints[3]), C.byref(info))
+    return info.value

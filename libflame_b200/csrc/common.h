@@ -213,6 +213,10 @@ int tri_inverse_lower(const double* L, long ldl, int b, bool unit, double* X, lo
 // Inverses of the 128 x 128 diagonal blocks of an n x n triangle, one
 // launch: block q into X + q*128*128 (ld 128).
 int tri_inverse_blocks(const double* T, long ldt, long n, bool lower, bool unit, double* X, cudaStream_t st);
+// Inverses of the bs x bs (bs <= 128) diagonal blocks, block q into
+// X + q*bs*bs (ld bs), one launch.
+int tri_inverse_blocks_bs(const double* T, long ldt, long n, int bs, bool lower, bool unit, double* X,
+                          cudaStream_t st);
 // X := inv(T), T b x b triangular (lower or upper; unit diagonal if unit).
 int tri_inverse(const double* T, long ldt, int b, bool lower, bool unit, double* X, long ldx, cudaStream_t st);
 // X := X inv(op(T)) ^T row by row: every row x of the m x b block X is

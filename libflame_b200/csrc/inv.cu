@@ -1,0 +1,270 @@
+// Inversion of a symmetric positive definite matrix from its Cholesky
+// factor, and its two building blocks:
+//   FLA_Trinv   T := inv(T) on one triangle      src/lapack/inv/tri/front/flamec/FLA_Trinv.c:17-50
+//   FLA_Ttmm    L := L^T L  (U := U U^T)          src/lapack/misc/ttmm/front/flamec/FLA_Ttmm.c:17-43
+//   FLA_SPDinv  A := inv(A) via Chol, Trinv, Ttmm src/lapack/inv/spd/front/flamec/FLA_SPDinv.c:15-28,
+//                                                 FLA_SPDinv_internal.c:17-38
+//   dpotri_     Trinv + Ttmm on dpotrf_'s factor  src/map/lapack2flamec/FLA_potri.c:25-56
+// Both kernels-level steps are blocked over 128-row blocks with the FP64
+// DMMA GEMM engine doing all the O(n^3) work:
+//   Trinv (lower): X := I; for each block row b: X_b := inv(L_bb) X_b (only
+//   the columns left of the block's end are nonzero), then the rows below
+//   lose L(below, b) X_b — the forward substitution of L X = I restricted to
+//   X's nonzero triangle (n^3/3 flops).  The diagonal blocks' inverses come
+//   from tri_inverse_blocks.
+//   Ttmm (lower): block row I of tril(L^T L) sums only k >= I0, so each block
+//   row is one GEMM W(I0:, I)^T W(I0:, 0:I1) (n^3/3 flops).
+// The upper-triangular forms run on the transposed triangle.
+#include <algorithm>
+#include <cstring>
+
+#include "common.h"
+
+namespace fb {
+
+int set_identity_dev(DMat X, cudaStream_t st);
+
+namespace {
+
+constexpr int TB = 128;
+
+// dst(i, j) := src(i, j) on the lower triangle (i > j, plus i == j when
+// with_diag); with zero_upper the rest of dst is set to 0.
+__global__ void copy_lower_kernel(const double* __restrict__ S, long lds, double* __restrict__ D, long ldd, long n,
+                                  int with_diag, int zero_upper) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * n) return;
+  const long j = idx / n, i = idx - j * n;
+  if (i > j || (with_diag && i == j)) D[i + j * ldd] = S[i + j * lds];
+  else if (zero_upper) D[i + j * ldd] = 0.0;
+}
+
+long even_up(long x) { return (x + 1) & ~1L; }
+
+int copy_lower(const double* S, long lds, double* D, long ldd, long n, bool with_diag, bool zero_upper,
+               cudaStream_t st) {
+  const long total = n * n;
+  if (total <= 0) return FLA_SUCCESS;
+  copy_lower_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(S, lds, D, ldd, n, with_diag ? 1 : 0,
+                                                                     zero_upper ? 1 : 0);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
+}
+
+// Lower triangle of A (n x n) := inv(tril(A)) (unit: the diagonal is taken
+// as ones and left untouched).
+int trinv_lower_dev(DMat A, bool unit, cudaStream_t st) {
+  const long n = A.m;
+  if (n == 0) return FLA_SUCCESS;
+  const long ldx = even_up(n);
+  const long nblk = (n + TB - 1) / TB;
+  double* X = (double*)ws_get(WS_FB, sizeof(double) * (size_t)ldx * (size_t)n);
+  double* Inv = (double*)ws_get(WS_TRINV, sizeof(double) * (size_t)nblk * TB * TB);
+  double* W = (double*)ws_get(WS_SOLVE_W, sizeof(double) * (size_t)TB * (size_t)n);
+  if (!X || !Inv || !W) return FLA_FAILURE;
+  DMat Xm;
+  Xm.p = X;
+  Xm.ld = ldx;
+  Xm.m = Xm.n = n;
+  if (set_identity_dev(Xm, st) != FLA_SUCCESS) return FLA_FAILURE;
+  if (tri_inverse_blocks(A.p, A.ld, n, true, unit, Inv, st) != FLA_SUCCESS) return FLA_FAILURE;
+  for (long bi = 0; bi < nblk; ++bi) {
+    const long jb = bi * TB;
+    const int b = (int)std::min<long>(TB, n - jb);
+    const long c = jb + b;  // X(jb:jb+b, c:) is still zero
+    if (gemm_f64(st, false, false, b, c, b, 1.0, Inv + bi * TB * TB, TB, X + jb, ldx, 0.0, W, TB) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    FB_CK(cudaMemcpy2DAsync(X + jb, sizeof(double) * ldx, W, sizeof(double) * TB, sizeof(double) * b, c,
+                            cudaMemcpyDeviceToDevice, st));
+    const long rest = n - c;
+    if (rest > 0 && gemm_f64(st, false, false, rest, c, b, -1.0, A.p + c + jb * A.ld, A.ld, X + jb, ldx, 1.0,
+                             X + c, ldx) != FLA_SUCCESS)
+      return FLA_FAILURE;
+  }
+  return copy_lower(X, ldx, A.p, A.ld, n, !unit, false, st);
+}
+
+// Lower triangle of A := tril(L^T L), L = tril(A).
+int ttmm_lower_dev(DMat A, cudaStream_t st) {
+  const long n = A.m;
+  if (n == 0) return FLA_SUCCESS;
+  const long ldw = even_up(n);
+  double* W = (double*)ws_get(WS_FB, sizeof(double) * (size_t)ldw * (size_t)n);
+  double* C = (double*)ws_get(WS_MISC2, sizeof(double) * (size_t)ldw * (size_t)n);
+  if (!W || !C) return FLA_FAILURE;
+  if (copy_lower(A.p, A.ld, W, ldw, n, true, true, st) != FLA_SUCCESS) return FLA_FAILURE;
+  for (long i0 = 0; i0 < n; i0 += TB) {
+    const long b = std::min<long>(TB, n - i0), i1 = i0 + b;
+    // C(i0:i1, 0:i1) := W(i0:n, i0:i1)^T W(i0:n, 0:i1)
+    if (gemm_f64(st, true, false, b, i1, n - i0, 1.0, W + i0 + i0 * ldw, ldw, W + i0, ldw, 0.0, C + i0, ldw) !=
+        FLA_SUCCESS)
+      return FLA_FAILURE;
+  }
+  return copy_lower(C, ldw, A.p, A.ld, n, true, false, st);
+}
+
+// The upper forms on the transposed triangle: U^T is lower, inv(U)^T =
+// inv(U^T), and (U U^T) = (U^T)^T (U^T).
+int upper_via_lower(DMat A, int (*op)(DMat, bool, cudaStream_t), bool unit, cudaStream_t st) {
+  const long n = A.m;
+  if (n == 0) return FLA_SUCCESS;
+  const long ldt = even_up(n);
+  double* Tt = (double*)ws_get(WS_REPACK, sizeof(double) * (size_t)ldt * (size_t)n);
+  if (!Tt) return FLA_FAILURE;
+  if (transpose_dev(A.p, A.ld, Tt, ldt, n, n, false, st) != FLA_SUCCESS) return FLA_FAILURE;
+  DMat L;
+  L.p = Tt;
+  L.ld = ldt;
+  L.m = L.n = n;
+  if (op(L, unit, st) != FLA_SUCCESS) return FLA_FAILURE;
+  return transpose_dev(Tt, ldt, A.p, A.ld, n, n, true, st);
+}
+
+int trinv_op(DMat L, bool unit, cudaStream_t st) { return trinv_lower_dev(L, unit, st); }
+int ttmm_op(DMat L, bool, cudaStream_t st) { return ttmm_lower_dev(L, st); }
+
+void ensure_init() {
+  if (!ctx().initialized) FLA_Init();
+}
+
+DMat dm(const Staged& s) {
+  DMat d;
+  d.p = (double*)s.dev;
+  d.ld = s.ld;
+  d.m = s.m;
+  d.n = s.n;
+  return d;
+}
+
+}  // namespace
+
+int trinv_dev(DMat A, bool lower, bool unit, cudaStream_t st) {
+  return lower ? trinv_lower_dev(A, unit, st) : upper_via_lower(A, trinv_op, unit, st);
+}
+
+int ttmm_dev(DMat A, bool lower, cudaStream_t st) {
+  return lower ? ttmm_lower_dev(A, st) : upper_via_lower(A, ttmm_op, false, st);
+}
+
+}  // namespace fb
+
+using namespace fb;
+
+namespace {
+
+bool square_double(const FLA_Obj& A) { return A.base && A.base->datatype == FLA_DOUBLE && A.m == A.n; }
+
+// Stage A, run f on the device operand, copy back.
+template <typename F>
+FLA_Error on_device(const FLA_Obj& A, F f) {
+  Staged s;
+  if (stage(A, WS_STAGE_A, &s) != FLA_SUCCESS) return FLA_FAILURE;
+  cudaStream_t st = ctx().stream;
+  op_begin(st);
+  if (f(dm(s), st) != FLA_SUCCESS) return FLA_FAILURE;
+  op_end(st);
+  if (unstage(s) != FLA_SUCCESS || sync_all() != FLA_SUCCESS) return FLA_FAILURE;
+  return FLA_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+// src/lapack/inv/tri/front/flamec/FLA_Trinv.c:17-50 (+ FLA_Trinv_check).
+// The reference's blocked and unblocked variants return FLA_SUCCESS without
+// a singularity check; a zero on the diagonal yields infinities here too.
+FLA_Error FLA_Trinv(FLA_Uplo uplo, FLA_Diag diag, FLA_Obj A) {
+  ensure_init();
+  FB_REQUIRE(uplo == FLA_LOWER_TRIANGULAR || uplo == FLA_UPPER_TRIANGULAR, "FLA_Trinv", "invalid uplo value");
+  FB_REQUIRE(diag == FLA_NONUNIT_DIAG || diag == FLA_UNIT_DIAG, "FLA_Trinv", "invalid diag value");
+  FB_REQUIRE(square_double(A), "FLA_Trinv", "object must be a square FLA_DOUBLE matrix");
+  if (A.m == 0) return FLA_SUCCESS;
+  // Orders above the reference's blocksize (min of its default M/K/N
+  // blocksizes, 128; FLA_Trinv.c:37-47) take its blocked variant, whose
+  // upper unit-diagonal form passes FLA_NONUNIT_DIAG to its Trsm and Trinv
+  // calls (FLA_Trinv_uu_blk_var3.c:37-53): the result there is the non-unit
+  // inverse, diagonal included.  Reproduced so results match the reference.
+  bool unit = (diag == FLA_UNIT_DIAG);
+  if (uplo == FLA_UPPER_TRIANGULAR && unit && A.m > 128) unit = false;
+  return on_device(A, [&](DMat a, cudaStream_t st) {
+    return trinv_dev(a, uplo == FLA_LOWER_TRIANGULAR, unit, st);
+  });
+}
+
+// src/lapack/misc/ttmm/front/flamec/FLA_Ttmm.c:17-43 (+ FLA_Ttmm_check):
+// lower: tril(A) := tril(L^T L); upper: triu(A) := triu(U U^T).
+FLA_Error FLA_Ttmm(FLA_Uplo uplo, FLA_Obj A) {
+  ensure_init();
+  FB_REQUIRE(uplo == FLA_LOWER_TRIANGULAR || uplo == FLA_UPPER_TRIANGULAR, "FLA_Ttmm", "invalid uplo value");
+  FB_REQUIRE(square_double(A), "FLA_Ttmm", "object must be a square FLA_DOUBLE matrix");
+  if (A.m == 0) return FLA_SUCCESS;
+  return on_device(A, [&](DMat a, cudaStream_t st) { return ttmm_dev(a, uplo == FLA_LOWER_TRIANGULAR, st); });
+}
+
+// src/lapack/inv/spd/front/flamec/FLA_SPDinv.c:15-28 and
+// FLA_SPDinv_internal.c:17-38: Chol, then Trinv and Ttmm on the factor's
+// triangle.  As there, a Cholesky failure is reported through
+// FLA_Check_chol_failure (src/base/flamec/main/FLA_Check.c:803-811), which
+// flags a failing column index > 0 (print + abort at error level >= MIN);
+// the call returns FLA_SUCCESS otherwise.
+FLA_Error FLA_SPDinv(FLA_Uplo uplo, FLA_Obj A) {
+  ensure_init();
+  FB_REQUIRE(uplo == FLA_LOWER_TRIANGULAR || uplo == FLA_UPPER_TRIANGULAR, "FLA_SPDinv", "invalid uplo value");
+  FB_REQUIRE(square_double(A), "FLA_SPDinv", "object must be a square FLA_DOUBLE matrix");
+  if (A.m == 0) return FLA_SUCCESS;
+  const bool lower = (uplo == FLA_LOWER_TRIANGULAR);
+  Staged s;
+  if (stage(A, WS_STAGE_A, &s) != FLA_SUCCESS) return FLA_FAILURE;
+  int info = -1;
+  if ((lower ? chol_lower_dev(dm(s), &info) : chol_upper_dev(dm(s), &info)) != FLA_SUCCESS) return FLA_FAILURE;
+  FB_REQUIRE(!(info > 0), "FLA_SPDinv", "Cholesky factorization failed; matrix not SPD");
+  cudaStream_t st = ctx().stream;
+  op_begin(st);
+  if (trinv_dev(dm(s), lower, false, st) != FLA_SUCCESS) return FLA_FAILURE;
+  if (ttmm_dev(dm(s), lower, st) != FLA_SUCCESS) return FLA_FAILURE;
+  op_end(st);
+  if (unstage(s) != FLA_SUCCESS || sync_all() != FLA_SUCCESS) return FLA_FAILURE;
+  return FLA_SUCCESS;
+}
+
+// src/map/lapack2flamec/FLA_potri.c:25-56 with dpotri_check
+// (src/map/common/lapackcheck/dpotri_check.c): on entry the triangle uplo of
+// A holds dpotrf_'s factor, on exit the same triangle of inv(A).  info = 0
+// (the reference's FLA_Trinv reports no singularity).
+int dpotri_(char* uplo, int* n, double* a, int* lda, int* info) {
+  *info = 0;
+  const bool up = uplo && (uplo[0] == 'U' || uplo[0] == 'u');
+  const bool lo = uplo && (uplo[0] == 'L' || uplo[0] == 'l');
+  if (!up && !lo) *info = -1;
+  else if (*n < 0) *info = -2;
+  else if (*lda < std::max(1, *n)) *info = -4;
+  if (*info != 0) {
+    std::printf("lapack2flame: On entry to %6s, parameter number %2i had an illegal value\n", "DPOTRI", -*info);
+    return FLA_FAILURE;
+  }
+  if (*n == 0) return 0;
+  ensure_init();
+  FLA_Base_obj base;
+  std::memset(&base, 0, sizeof(base));
+  base.datatype = FLA_DOUBLE;
+  base.elemtype = FLA_MATRIX;
+  base.m = base.n = (dim_t)*n;
+  base.rs = 1;
+  base.cs = (dim_t)*lda;
+  base.buffer = a;
+  FLA_Obj A;
+  A.offm = A.offn = 0;
+  A.m = A.n = (dim_t)*n;
+  A.m_inner = A.m;
+  A.n_inner = A.n;
+  A.base = &base;
+  FLA_Error r = on_device(A, [&](DMat d, cudaStream_t st) {
+    if (trinv_dev(d, lo, false, st) != FLA_SUCCESS) return (int)FLA_FAILURE;
+    return ttmm_dev(d, lo, st);
+  });
+  return r == FLA_SUCCESS ? 0 : FLA_FAILURE;
+}
+
+}  // extern "C"

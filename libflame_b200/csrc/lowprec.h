@@ -26,6 +26,11 @@ int lp_gemm(cudaStream_t st, LowPrec prec, long m, long n, long k, float alpha, 
             const uint16_t* B, long ldb, float beta, float* C, long ldc, GemmMode mode = GEMM_FULL,
             long diag_off = 0, const int* guard = nullptr, int guard_limit = 0x7fffffff, long aplane = 0,
             long bplane = 0);
+// The 16-bit case on the tcgen05 tensor cores (tc_gemm.cu): TMA-fed
+// K-major operands, FP32 accumulator in TMEM.
+int tc_gemm16(cudaStream_t st, bool bf16, long m, long n, long k, float alpha, const uint16_t* A, long lda,
+              const uint16_t* B, long ldb, float beta, float* C, long ldc, GemmMode mode, long diag_off,
+              const int* guard, int guard_limit);
 // Element offset into a packed operand buffer (16-bit elements, or floats
 // for LP_TF32X3).
 inline uint16_t* lp_off(uint16_t* base, LowPrec p, size_t elems) {

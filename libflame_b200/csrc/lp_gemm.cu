@@ -20,6 +20,8 @@
 
 #include <algorithm>
 
+#include <string>
+
 #include "common.h"
 #include "lowprec.h"
 
@@ -460,6 +462,13 @@ int lp_gemm(cudaStream_t st, LowPrec prec, long m, long n, long k, float alpha, 
     set_last_error("lp_gemm: packed operands need 16-byte aligned rows");
     return FLA_FAILURE;
   }
+  static const bool use_mma_sync = [] {
+    const char* e = std::getenv("FLA_B200_LP_GEMM");
+    return e && std::string(e) == "mma";
+  }();
+  if (!use_mma_sync && k > 0)
+    return tc_gemm16(st, prec == LP_BF16, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, mode, diag_off, guard,
+                     guard_limit);
   lp_attrs();
   dim3 grid((unsigned)((m + LBM - 1) / LBM), (unsigned)((n + LBN - 1) / LBN));
   const int ps = prof_begin(st);

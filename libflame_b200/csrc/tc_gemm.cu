@@ -1,0 +1,290 @@
+// 16-bit GEMM on the fifth-generation tensor cores (tcgen05) for the
+// mixed-precision factorizations:
+//
+//   C (FP32, column-major) := alpha * A * B^T + beta * C
+//   A: m x k, B: n x k, FP16 or BF16, k contiguous (row r at A + r * lda)
+//
+// One CTA of 128 threads per 128 x TN output tile:
+//   * thread 0 (warp 0) streams the k-blocks of A (128 x 64) and B (TN x 64)
+//     with 2D TMA loads (128-byte swizzle) into an S-stage ring of shared
+//     memory buffers, each stage completing an mbarrier transaction count;
+//   * thread 32 (warp 1) issues tcgen05.mma (M = 128, N = TN, K = 16, FP32
+//     accumulate) into a TN-column TMEM accumulator and releases each stage
+//     with tcgen05.commit on the stage's "empty" mbarrier, then commits a
+//     final "done" mbarrier;
+//   * the four warps read the accumulator (warp w owns TMEM lanes 32w..32w+31,
+//     i.e. tile rows) with tcgen05.ld and write C column by column (32
+//     consecutive rows per store: coalesced).
+// Two CTAs fit on an SM (3 stages x 32 KB of shared memory, 2 x 128 TMEM
+// columns), so one CTA's epilogue overlaps the other's main loop.
+//
+// The shared-memory operand descriptors describe K-major tiles with the
+// 128-byte swizzle (rows of 128 bytes, 8-row atoms 1024 bytes apart); the
+// K = 16 sub-steps of a 64-wide k-block advance the start address by 32
+// bytes inside the swizzle atom.
+//
+// Every mbarrier wait is bounded (kWaitLimitNs); on expiry the kernel
+// records the error in the status block, lets the MMA thread commit what it
+// issued, waits (bounded) for its own TMA loads still in flight, frees its
+// TMEM and returns without storing.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+#include <mutex>
+
+#include "common.h"
+#include "dev_util.cuh"
+#include "lowprec.h"
+
+namespace fb {
+
+namespace {
+
+constexpr int TC_BM = 128;
+constexpr int TC_BK = 64;  // 64 16-bit values = 128 bytes = one swizzle row
+constexpr int TC_THREADS = 128;
+
+template <int TN, int STAGES>
+struct TcCfg {
+  static constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2;
+  static constexpr uint32_t B_BYTES = TN * TC_BK * 2;
+  static constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;
+  static constexpr uint32_t BAR_OFF = STAGES * STAGE_BYTES;
+  // stages, then 2*STAGES+1 mbarriers and the TMEM address slot, plus slack
+  // to align the ring to 1024 bytes (the swizzle atom)
+  static constexpr uint32_t SMEM_BYTES = BAR_OFF + 8 * (2 * STAGES + 1) + 16 + 1024;
+  static constexpr uint32_t TMEM_COLS = TN;  // FP32 accumulator columns (power of 2 >= 32)
+};
+
+// K-major, 128-byte swizzle, 8-row atoms 1024 bytes apart (SBO), version 1.
+__device__ __forceinline__ uint64_t umma_desc_k_sw128(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)(1024u >> 4) << 32) |
+         ((uint64_t)1u << 46) | ((uint64_t)2u << 61);
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_mma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                           uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+// 32 consecutive FP32 accumulator columns of this thread's TMEM lane.
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+template <int TN, int STAGES>
+__global__ void __launch_bounds__(TC_THREADS, 2)
+    tc_gemm16_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB, float* C,
+                     long ldc, int M, int N, int K, float alpha, float beta, uint32_t idesc, int lower,
+                     long diag_off, const int* guard, int guard_limit, int* err) {
+  using Cfg = TcCfg<TN, STAGES>;
+  extern __shared__ uint8_t smem_raw[];
+  const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TN;
+  // tile entirely outside the written triangle: nothing to do (CTA-uniform)
+  if (lower && (long)(m0 + TC_BM - 1) - (long)n0 < diag_off) return;
+  if (guard && *((volatile const int*)guard) < guard_limit) return;
+
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t* gbase = smem_raw + (base - raw);
+  const uint32_t bar0 = base + Cfg::BAR_OFF;  // full[s] = bar0 + 8s, empty[s] = bar0 + 8(S+s), done
+  const uint32_t done_bar = bar0 + 8 * (2 * STAGES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + Cfg::BAR_OFF + 8 * (2 * STAGES + 1));
+  __shared__ int s_abort;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(bar0 + 8 * s, 1);
+      mbar_init(bar0 + 8 * (STAGES + s), 1);
+    }
+    mbar_init(done_bar, 1);
+    fence_barrier_init();
+    s_abort = 0;
+    prefetch_tmap(&mA);
+    prefetch_tmap(&mB);
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(Cfg::TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int nk = (K + TC_BK - 1) / TC_BK;
+
+  if (threadIdx.x == 0) {
+    // ---- TMA producer
+    int issued = 0;
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % STAGES, r = kb / STAGES;
+      if (r > 0 && !mbar_wait(bar0 + 8 * (STAGES + s), (uint32_t)((r - 1) & 1), err, 41)) {
+        s_abort = 1;
+        break;
+      }
+      if (*((volatile int*)&s_abort)) break;
+      const uint32_t sa = base + s * Cfg::STAGE_BYTES, sb = sa + Cfg::A_BYTES;
+      mbar_arrive_expect_tx(bar0 + 8 * s, Cfg::STAGE_BYTES);
+      tma_load_2d(sa, &mA, kb * TC_BK, m0, bar0 + 8 * s);
+      tma_load_2d(sb, &mB, kb * TC_BK, n0, bar0 + 8 * s);
+      issued = kb + 1;
+    }
+    // drain: the last load issued into each stage has landed (bounded)
+    for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; ++kb)
+      mbar_wait(bar0 + 8 * (kb % STAGES), (uint32_t)((kb / STAGES) & 1), err, 42);
+  } else if (threadIdx.x == 32) {
+    // ---- MMA issuer
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % STAGES, r = kb / STAGES;
+      if (!mbar_wait(bar0 + 8 * s, (uint32_t)(r & 1), err, 43)) {
+        s_abort = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t sa = base + s * Cfg::STAGE_BYTES, sb = sa + Cfg::A_BYTES;
+#pragma unroll
+      for (int k = 0; k < TC_BK / 16; ++k)
+        tc_mma_f16(tmem, umma_desc_k_sw128(sa + 32 * k), umma_desc_k_sw128(sb + 32 * k), idesc,
+                   (kb > 0 || k > 0) ? 1u : 0u);
+      tc_commit(bar0 + 8 * (STAGES + s));  // stage s free once these MMAs are done
+    }
+    tc_commit(done_bar);  // every MMA issued above has completed
+  }
+  // ---- epilogue: all four warps
+  const bool got = mbar_wait(done_bar, 0, err, 44);
+  tc_fence_after();
+  const bool store = got && nk > 0 && !*((volatile int*)&s_abort);
+  const int row = m0 + warp * 32 + lane;
+  const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+  for (int c0 = 0; c0 < TN; c0 += 32) {
+    if (!__all_sync(0xffffffffu, store ? 1 : 0)) break;
+    if (n0 + c0 >= N) break;
+    float v[32];
+    tc_ld32(tl + c0, v);
+    if (row < M) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const int col = n0 + c0 + j;
+        if (col < N && (!lower || (long)row - (long)col >= diag_off)) {
+          float* cp = C + row + (long)col * ldc;
+          *cp = (beta == 0.f) ? alpha * v[j] : fmaf(alpha, v[j], beta * *cp);
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::TMEM_COLS)
+                 : "memory");
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 g_enc16 = nullptr;
+std::once_flag g_enc16_once;
+
+bool get_enc16() {
+  std::call_once(g_enc16_once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_enc16 = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  });
+  return g_enc16 != nullptr;
+}
+
+// rows x kdim 16-bit operand, k contiguous (row pitch ld elements), box of
+// box_rows rows x 64 k-values, 128-byte swizzle, zero fill out of bounds.
+bool make_map16(CUtensorMap* map, const uint16_t* p, long rows, long kdim, long ld, int box_rows) {
+  if (!get_enc16()) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)(kdim > 0 ? kdim : 1), (cuuint64_t)(rows > 0 ? rows : 1)};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  return g_enc16(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<uint16_t*>(p), dims, strides, box, estr,
+                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+constexpr int TC_TN = 128;
+constexpr int TC_STAGES = 3;
+
+}  // namespace
+
+// C := alpha A B^T + beta C on the tcgen05 tensor cores (see the top of
+// this file); A, B packed 16-bit, k contiguous, lda / ldb multiples of 8 and
+// 16-byte aligned bases (the TMA rules).  GEMM_LOWER writes i - j >= diag_off
+// only and skips tiles with nothing to write.
+int tc_gemm16(cudaStream_t st, bool bf16, long m, long n, long k, float alpha, const uint16_t* A, long lda,
+              const uint16_t* B, long ldb, float beta, float* C, long ldc, GemmMode mode, long diag_off,
+              const int* guard, int guard_limit) {
+  using Cfg = TcCfg<TC_TN, TC_STAGES>;
+  if (m <= 0 || n <= 0) return FLA_SUCCESS;
+  if (k <= 0) {
+    set_last_error("tc_gemm16: k must be positive");
+    return FLA_FAILURE;
+  }
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(tc_gemm16_kernel<TC_TN, TC_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)Cfg::SMEM_BYTES);
+    attr = true;
+  }
+  CUtensorMap mA, mB;
+  if (!make_map16(&mA, A, m, k, lda, TC_BM) || !make_map16(&mB, B, n, k, ldb, TC_TN)) {
+    set_last_error("tc_gemm16: cuTensorMapEncodeTiled failed");
+    return FLA_FAILURE;
+  }
+  // instruction descriptor: FP32 accumulator, A/B FP16 (0) or BF16 (1),
+  // both K-major, N = TN, M = 128
+  const uint32_t fmt = bf16 ? 1u : 0u;
+  const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(TC_TN >> 3) << 17) |
+                         ((uint32_t)(TC_BM >> 4) << 24);
+  dim3 grid((unsigned)((m + TC_BM - 1) / TC_BM), (unsigned)((n + TC_TN - 1) / TC_TN));
+  const int ps = prof_begin(st);
+  tc_gemm16_kernel<TC_TN, TC_STAGES><<<grid, TC_THREADS, Cfg::SMEM_BYTES, st>>>(
+      mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, idesc, mode == GEMM_LOWER ? 1 : 0, diag_off, guard,
+      guard_limit, ctx().d_status + ST_ERROR);
+  prof_end(ps, st, PROF_GEMM,
+           mode == GEMM_LOWER && m == n ? (double)m * (double)(m + 1) * (double)k : 2.0 * m * (double)n * k);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
+}
+
+}  // namespace fb

@@ -110,20 +110,20 @@ __global__ void __launch_bounds__(THREADS) trsm_tile_kernel(const double* __rest
 // so the b steps cost only warp-level latency.
 constexpr int INV_WARPS = 16;
 constexpr size_t INV_SMEM = (size_t)(TB * LDT + TB) * sizeof(double);
-// Batched over the diagonal blocks of an n x n triangle: blockIdx.y = block
-// index q, T_q = T + q*TB*(1 + ldt), X_q = X + q * xstride; with gridDim.y
-// = 1 and n = b, the single b x b block.
+// Batched over the diagonal blocks of order bs (<= TB) of an n x n
+// triangle: blockIdx.y = block index q, T_q = T + q*bs*(1 + ldt), X_q = X +
+// q * xstride; with gridDim.y = 1 and n = b, the single b x b block.
 template <bool LOWER, bool UNIT>
 __global__ void __launch_bounds__(INV_WARPS * 32) tri_inv_kernel(const double* __restrict__ T, long ldt,
                                                                  double* __restrict__ X, long ldx, int n,
-                                                                 long xstride) {
+                                                                 long xstride, int bs = TB) {
   extern __shared__ double sm[];
   double* ST = sm;             // stored triangle, ST[r + c*LDT]
   double* sd = ST + TB * LDT;  // reciprocal diagonal
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int q = blockIdx.y;
-  const int b = min(TB, n - q * TB);
-  T += (long)q * TB * (1 + ldt);
+  const int b = min(bs, n - q * bs);
+  T += (long)q * bs * (1 + ldt);
   X += (long)q * xstride;
   load_block_f64<INV_WARPS * 32, true>(T, ldt, b, ST, LDT, [](int r, int c) { return LOWER ? (r >= c) : (r <= c); });
   __syncthreads();
@@ -328,6 +328,30 @@ int tri_inverse_blocks(const double* T, long ldt, long n, bool lower, bool unit,
     else tri_inv_kernel<false, false><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, TB, (int)n, xs);
   }
   prof_end(ps, st, PROF_TRSM, (double)n * TB * TB / 3.0);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
+}
+
+// Inverses of the bs x bs diagonal blocks (bs <= 128) of the n x n
+// triangle T in one launch: block q (order min(bs, n - bs q)) into
+// X + q * bs * bs, ld bs.
+int tri_inverse_blocks_bs(const double* T, long ldt, long n, int bs, bool lower, bool unit, double* X,
+                          cudaStream_t st) {
+  if (n <= 0) return FLA_SUCCESS;
+  set_attrs();
+  const long nblk = (n + bs - 1) / bs;
+  dim3 grid((unsigned)((bs + INV_WARPS - 1) / INV_WARPS), (unsigned)nblk);
+  const long xs = (long)bs * bs;
+  const int ps = prof_begin(st);
+  if (lower) {
+    if (unit) tri_inv_kernel<true, true><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, bs, (int)n, xs, bs);
+    else tri_inv_kernel<true, false><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, bs, (int)n, xs, bs);
+  } else {
+    if (unit) tri_inv_kernel<false, true><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, bs, (int)n, xs, bs);
+    else tri_inv_kernel<false, false><<<grid, INV_WARPS * 32, INV_SMEM, st>>>(T, ldt, X, bs, (int)n, xs, bs);
+  }
+  prof_end(ps, st, PROF_TRSM, (double)n * bs * bs / 3.0);
   count_launch();
   FB_CK(cudaGetLastError());
   return FLA_SUCCESS;

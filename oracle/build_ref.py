@@ -10,6 +10,12 @@ Inputs : the reference source tree (default /root/reference, read-only) and
 Outputs: oracle/_ref/libflame_ref.so        (flat FLA_* + lapack2flame, serial)
          oracle/_ref/libflame_ref_smp.so    (same + SuperMatrix/OpenMP, for the
                                              multi-threaded CPU baseline)
+         oracle/_ref/libflame_ref_openblas.so (--openblas: the serial objects
+                                             without the built-in f2c BLAS, their
+                                             BLAS references renamed to SciPy's
+                                             bundled LP64 OpenBLAS, whose
+                                             exports carry a scipy_ prefix: the
+                                             fast multi-threaded CPU baseline)
 Objects go to oracle/_ref/obj*/.  Nothing is written into the reference tree.
 
 Which reference sources are compiled: every .c under the directories listed
@@ -105,6 +111,56 @@ def build(ref, out, smp, f2c_list, jobs):
     return lib
 
 
+def openblas_lib():
+    """SciPy's bundled OpenBLAS (LP64, Fortran symbols prefixed scipy_)."""
+    import glob
+    import scipy
+    d = os.path.realpath(os.path.join(os.path.dirname(scipy.__file__), "..", "scipy.libs"))
+    libs = sorted(glob.glob(os.path.join(d, "libscipy_openblas*.so")))
+    if not libs:
+        raise SystemExit("SciPy's bundled OpenBLAS not found under " + d)
+    return libs[0]
+
+
+def build_openblas(ref, out):
+    """Relink the serial objects, minus src/flablas (the built-in BLAS; only
+    its lsame.c reads FLA_ENABLE_BUILTIN_BLAS; its f2c runtime helpers under
+    f2c/other/util stay), against OpenBLAS: every
+    symbol the objects reference but do not define and that OpenBLAS exports
+    as scipy_<name> is renamed to it (objcopy --redefine-syms on one
+    relocatable object)."""
+    ob = openblas_lib()
+    objdir = os.path.join(out, "obj_serial")
+    objs = []
+    for root, _, fnames in os.walk(objdir):
+        rel = os.path.relpath(root, objdir)
+        # keep the f2c runtime helpers (complex conjugate / imaginary part)
+        if rel.startswith(os.path.join("src", "flablas")) and \
+                not rel.startswith(os.path.join("src", "flablas", "f2c", "other", "util")):
+            continue
+        objs += [os.path.join(root, f) for f in fnames if f.endswith(".o")]
+    rsp = os.path.join(out, "objs_openblas.rsp")
+    with open(rsp, "w") as f:
+        f.write("\n".join(sorted(objs)))
+    combined = os.path.join(out, "libflame_ref_openblas.o")
+    subprocess.run(["ld", "-r", "-o", combined, "@" + rsp], check=True)
+    undef = subprocess.run(["nm", "-u", combined], capture_output=True, text=True, check=True).stdout.split()
+    undef = {u for u in undef if u not in ("U", "w")}
+    exported = subprocess.run(["nm", "-D", "--defined-only", ob], capture_output=True, text=True,
+                              check=True).stdout.split()
+    exported = {e for e in exported if e.startswith("scipy_")}
+    pairs = sorted((u, "scipy_" + u) for u in undef if "scipy_" + u in exported)
+    mp = os.path.join(out, "openblas_redefine.txt")
+    with open(mp, "w") as f:
+        f.write("".join("%s %s\n" % p for p in pairs))
+    subprocess.run(["objcopy", "--redefine-syms=" + mp, combined], check=True)
+    lib = os.path.join(out, "libflame_ref_openblas.so")
+    subprocess.run(["gcc", "-shared", "-o", lib, combined, ob, "-Wl,-rpath," + os.path.dirname(ob), "-lm"],
+                   check=True)
+    print("renamed %d BLAS/LAPACK references to OpenBLAS" % len(pairs))
+    return lib
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=os.environ.get("LIBFLAME_REF_DIR") or DEFAULT_REF,
@@ -113,6 +169,8 @@ def main():
                     help="exit quietly when the reference tree is absent")
     ap.add_argument("--out", default=os.path.join(HERE, "_ref"))
     ap.add_argument("--smp", action="store_true", help="also build the SuperMatrix/OpenMP library")
+    ap.add_argument("--openblas", action="store_true",
+                    help="also build libflame_ref_openblas.so (reference over SciPy's OpenBLAS)")
     ap.add_argument("-j", type=int, default=os.cpu_count() or 4)
     a = ap.parse_args()
     if not os.path.isdir(os.path.join(a.ref, "src")):
@@ -126,6 +184,8 @@ def main():
     print(build(a.ref, a.out, False, f2c_list, a.j))
     if a.smp:
         print(build(a.ref, a.out, True, f2c_list, a.j))
+    if a.openblas:
+        print(build_openblas(a.ref, a.out))
 
 
 if __name__ == "__main__":

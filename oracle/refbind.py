@@ -40,10 +40,17 @@ class FLA_Obj(C.Structure):
 _lib = {}
 
 
-def lib(smp=False):
-    key = "smp" if smp else "serial"
+LIB_FILES = {"serial": "libflame_ref.so", "smp": "libflame_ref_smp.so",
+             "openblas": "libflame_ref_openblas.so"}
+
+
+def lib(smp=False, kind=None):
+    """The reference library: "serial" (f2c built-in BLAS, the parity
+    oracle), "smp" (+ SuperMatrix/OpenMP) or "openblas" (flat FLA_* over
+    SciPy's bundled OpenBLAS, the fast CPU baseline)."""
+    key = kind or ("smp" if smp else "serial")
     if key not in _lib:
-        path = os.path.join(REF_DIR, "libflame_ref_smp.so" if smp else "libflame_ref.so")
+        path = os.path.join(REF_DIR, LIB_FILES[key])
         if not os.path.exists(path):
             raise FileNotFoundError(path + " missing: run python oracle/build_ref.py")
         L = C.CDLL(path)
@@ -53,7 +60,8 @@ def lib(smp=False):
                      "FLA_Chol_solve", "FLA_LU_piv_solve", "FLA_Apply_pivots",
                      "FLA_Shift_pivots_to", "FLA_Obj_create_without_buffer",
                      "FLA_Obj_attach_buffer", "FLA_Obj_free_without_buffer",
-                     "FLA_Trsm", "FLA_Set"]:
+                     "FLA_Trsm", "FLA_Set", "FLA_QR_UT_solve", "FLA_QR_UT_form_Q",
+                     "FLA_SPDinv", "FLA_Trinv", "FLA_Ttmm", "FLA_Accum_T_UT"]:
             getattr(L, name).restype = C.c_int
         _lib[key] = L
     return _lib[key]
@@ -85,20 +93,20 @@ def _dt(a):
     return (np.float32, FLA_FLOAT) if np.asarray(a).dtype == np.float32 else (np.float64, FLA_DOUBLE)
 
 
-def chol(A, uplo=FLA_LOWER_TRIANGULAR, smp=False):
+def chol(A, uplo=FLA_LOWER_TRIANGULAR, smp=False, kind=None):
     """FLA_Chol (src/lapack/dec/chol/front/flamec/FLA_Chol.c:16-29).
     Returns (factored copy of A, return value)."""
-    L = lib(smp)
+    L = lib(smp, kind)
     npdt, dt = _dt(A)
     M = _Mat(L, A, npdt, dt)
     r = L.FLA_Chol(uplo, M.obj)
     return M.a, r
 
 
-def lu_piv(A, smp=False):
+def lu_piv(A, smp=False, kind=None):
     """FLA_LU_piv (src/lapack/dec/lu/piv/front/flamec/FLA_LU_piv.c:16-33).
     Returns (LU, relative zero-based pivots, return value)."""
-    L = lib(smp)
+    L = lib(smp, kind)
     npdt, dt = _dt(A)
     M = _Mat(L, A, npdt, dt)
     k = min(M.a.shape)
@@ -107,10 +115,10 @@ def lu_piv(A, smp=False):
     return M.a, P.a.ravel().copy(), r
 
 
-def qr_ut(A, b_alg=None):
+def qr_ut(A, b_alg=None, kind=None):
     """FLA_QR_UT_create_T + FLA_QR_UT (src/lapack/dec/q/qrut/front/flamec/
     FLA_QR_UT_create_T.c:13-51, FLA_QR_UT.c:15-28).  Returns (A, T, rval)."""
-    L = lib()
+    L = lib(kind=kind)
     M = _Mat(L, A)
     m, n = M.a.shape
     if b_alg is None:
@@ -163,6 +171,59 @@ def apply_pivots(p, A, trans=FLA_NO_TRANSPOSE):
     return M.a, r
 
 
+def qr_ut_solve(QR, T, B):
+    """FLA_QR_UT_solve (src/lapack/dec/q/qrut/front/flamec/FLA_QR_UT_solve.c:13-49)."""
+    L = lib()
+    MA, MT, MB = _Mat(L, QR), _Mat(L, T), _Mat(L, B)
+    MX = _Mat(L, np.zeros((MA.a.shape[1], MB.a.shape[1])))
+    r = L.FLA_QR_UT_solve(MA.obj, MT.obj, MB.obj, MX.obj)
+    return MX.a, r
+
+
+def qr_ut_form_q(QR, T, ncols):
+    """FLA_QR_UT_form_Q (src/lapack/dec/q/qrut/front/flamec/FLA_QR_UT_form_Q.c:13-86)
+    into a separate m x ncols Q."""
+    L = lib()
+    MA, MT = _Mat(L, QR), _Mat(L, T)
+    MQ = _Mat(L, np.zeros((MA.a.shape[0], ncols)))
+    r = L.FLA_QR_UT_form_Q(MA.obj, MT.obj, MQ.obj)
+    return MQ.a, r
+
+
+def accum_t_ut(QR, t, b):
+    """FLA_Accum_T_UT(FORWARD, COLUMNWISE) (src/lapack/util/accum/tut/front/flamec/FLA_Accum_T_UT.c:13)."""
+    L = lib()
+    MA = _Mat(L, QR)
+    Mt = _Mat(L, np.asarray(t, dtype=np.float64))
+    MT = _Mat(L, np.zeros((b, min(MA.a.shape))))
+    r = L.FLA_Accum_T_UT(FLA_FORWARD, FLA_COLUMNWISE, MA.obj, Mt.obj, MT.obj)
+    return MT.a, r
+
+
+def spdinv(A, uplo=FLA_LOWER_TRIANGULAR):
+    """FLA_SPDinv (src/lapack/inv/spd/front/flamec/FLA_SPDinv.c:15-28)."""
+    L = lib()
+    M = _Mat(L, A)
+    r = L.FLA_SPDinv(uplo, M.obj)
+    return M.a, r
+
+
+def trinv(A, uplo=FLA_LOWER_TRIANGULAR, diag=FLA_NONUNIT_DIAG):
+    """FLA_Trinv (src/lapack/inv/tri/front/flamec/FLA_Trinv.c:17-50)."""
+    L = lib()
+    M = _Mat(L, A)
+    r = L.FLA_Trinv(uplo, diag, M.obj)
+    return M.a, r
+
+
+def ttmm(A, uplo=FLA_LOWER_TRIANGULAR):
+    """FLA_Ttmm (src/lapack/misc/ttmm/front/flamec/FLA_Ttmm.c:17-43)."""
+    L = lib()
+    M = _Mat(L, A)
+    r = L.FLA_Ttmm(uplo, M.obj)
+    return M.a, r
+
+
 # ---- LAPACK ABI through lapack2flame / f2c drivers ------------------------
 
 def _ip(x):
@@ -203,21 +264,30 @@ def dgeqrf(A):
     return a, tau, info.value
 
 
-def dposv(A, B, uplo="L"):
-    L = lib()
+last_secs = 0.0  # seconds of the last dsposv / dsgesv / dposv / dgesv call itself
+
+
+def dposv(A, B, uplo="L", kind=None):
+    global last_secs
+    import time
+    L = lib(kind=kind)
     a = np.array(A, dtype=np.float64, order="F", copy=True)
     b = np.array(B, dtype=np.float64, order="F", copy=True)
     if b.ndim == 1:
         b = b.reshape(-1, 1, order="F")
     n, nrhs = b.shape
     info = C.c_int(0)
+    t0 = time.perf_counter()
     L.dposv_(C.c_char_p(uplo.encode()), _ip(n), _ip(nrhs), a.ctypes.data_as(C.c_void_p),
              _ip(max(n, 1)), b.ctypes.data_as(C.c_void_p), _ip(max(n, 1)), C.byref(info))
+    last_secs = time.perf_counter() - t0
     return a, b, info.value
 
 
-def dgesv(A, B):
-    L = lib()
+def dgesv(A, B, kind=None):
+    global last_secs
+    import time
+    L = lib(kind=kind)
     a = np.array(A, dtype=np.float64, order="F", copy=True)
     b = np.array(B, dtype=np.float64, order="F", copy=True)
     if b.ndim == 1:
@@ -225,16 +295,20 @@ def dgesv(A, B):
     n, nrhs = b.shape
     ipiv = np.zeros(n, dtype=np.int32)
     info = C.c_int(0)
+    t0 = time.perf_counter()
     L.dgesv_(_ip(n), _ip(nrhs), a.ctypes.data_as(C.c_void_p), _ip(max(n, 1)),
              ipiv.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p), _ip(max(n, 1)),
              C.byref(info))
+    last_secs = time.perf_counter() - t0
     return a, ipiv, b, info.value
 
 
-def dsposv(A, B, uplo="L"):
+def dsposv(A, B, uplo="L", kind=None):
     """The reference's FP32-factor/FP64-refine driver
     (src/map/common/lapacksrc/f2c/dsposv.c:250-413)."""
-    L = lib()
+    global last_secs
+    import time
+    L = lib(kind=kind)
     a = np.array(A, dtype=np.float64, order="F", copy=True)
     b = np.array(B, dtype=np.float64, order="F", copy=True)
     if b.ndim == 1:
@@ -245,16 +319,20 @@ def dsposv(A, B, uplo="L"):
     swork = np.zeros(n * (n + nrhs), dtype=np.float32)
     it = C.c_int(0)
     info = C.c_int(0)
+    t0 = time.perf_counter()
     L.dsposv_(C.c_char_p(uplo.encode()), _ip(n), _ip(nrhs), a.ctypes.data_as(C.c_void_p), _ip(n),
               b.ctypes.data_as(C.c_void_p), _ip(n), x.ctypes.data_as(C.c_void_p), _ip(n),
               work.ctypes.data_as(C.c_void_p), swork.ctypes.data_as(C.c_void_p),
               C.byref(it), C.byref(info))
+    last_secs = time.perf_counter() - t0
     return x, it.value, info.value
 
 
-def dsgesv(A, B):
+def dsgesv(A, B, kind=None):
     """src/map/common/lapacksrc/f2c/dsgesv.c:246-405."""
-    L = lib()
+    global last_secs
+    import time
+    L = lib(kind=kind)
     a = np.array(A, dtype=np.float64, order="F", copy=True)
     b = np.array(B, dtype=np.float64, order="F", copy=True)
     if b.ndim == 1:
@@ -266,10 +344,12 @@ def dsgesv(A, B):
     swork = np.zeros(n * (n + nrhs), dtype=np.float32)
     it = C.c_int(0)
     info = C.c_int(0)
+    t0 = time.perf_counter()
     L.dsgesv_(_ip(n), _ip(nrhs), a.ctypes.data_as(C.c_void_p), _ip(n),
               ipiv.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p), _ip(n),
               x.ctypes.data_as(C.c_void_p), _ip(n), work.ctypes.data_as(C.c_void_p),
               swork.ctypes.data_as(C.c_void_p), C.byref(it), C.byref(info))
+    last_secs = time.perf_counter() - t0
     return x, it.value, info.value
 
 
@@ -317,3 +397,74 @@ def lu_piv_flash(A, nthreads, block=256):
 def chol_flash(A, nthreads, block=256):
     a, _, r, dt = _flash_run("chol", A, nthreads, block)
     return a, r, dt
+
+
+def dormqr(side, trans, QR, tau, Cm):
+    """dormqr_ (src/map/lapack2flamec/FLA_ormqr.c:35-97)."""
+    L = lib()
+    a = np.array(QR, dtype=np.float64, order="F", copy=True)
+    c = np.array(Cm, dtype=np.float64, order="F", copy=True)
+    t = np.array(tau, dtype=np.float64, copy=True)
+    m, n = c.shape
+    k = len(t)
+    nw = n if side == "L" else m
+    work = np.zeros(max(1, nw) * 64)
+    info = C.c_int(0)
+    L.dormqr_(C.c_char_p(side.encode()), C.c_char_p(trans.encode()), _ip(m), _ip(n), _ip(k),
+              a.ctypes.data_as(C.c_void_p), _ip(max(a.shape[0], 1)), t.ctypes.data_as(C.c_void_p),
+              c.ctypes.data_as(C.c_void_p), _ip(max(m, 1)), work.ctypes.data_as(C.c_void_p),
+              _ip(len(work)), C.byref(info))
+    return c, info.value
+
+
+def dorgqr(QR, tau, n):
+    """dorgqr_ (src/map/lapack2flamec/FLA_orgqr.c:30-80) on the first n columns."""
+    L = lib()
+    a = np.array(QR[:, :n], dtype=np.float64, order="F", copy=True)
+    t = np.array(tau, dtype=np.float64, copy=True)
+    m = a.shape[0]
+    k = len(t)
+    work = np.zeros(max(1, n) * 64)
+    info = C.c_int(0)
+    L.dorgqr_(_ip(m), _ip(n), _ip(k), a.ctypes.data_as(C.c_void_p), _ip(max(m, 1)),
+              t.ctypes.data_as(C.c_void_p), work.ctypes.data_as(C.c_void_p), _ip(len(work)), C.byref(info))
+    return a, info.value
+
+
+def dpotri(Afac, uplo="L"):
+    """dpotri_ (src/map/lapack2flamec/FLA_potri.c:25-56)."""
+    L = lib()
+    a = np.array(Afac, dtype=np.float64, order="F", copy=True)
+    n = a.shape[0]
+    info = C.c_int(0)
+    L.dpotri_(C.c_char_p(uplo.encode()), _ip(n), a.ctypes.data_as(C.c_void_p), _ip(max(n, 1)), C.byref(info))
+    return a, info.value
+
+
+def openblas_threads(n):
+    """Thread count of the OpenBLAS behind the "openblas" build."""
+    L = lib(kind="openblas")
+    f = getattr(L, "scipy_openblas_set_num_threads", None)
+    if f is None:
+        import glob
+        import scipy
+        d = os.path.realpath(os.path.join(os.path.dirname(scipy.__file__), "..", "scipy.libs"))
+        f = C.CDLL(sorted(glob.glob(os.path.join(d, "libscipy_openblas*.so")))[0]).scipy_openblas_set_num_threads
+    f(int(n))
+
+
+def timed_call(op, A, kind="openblas"):
+    """Seconds taken by one reference FLA_LU_piv (op "lu") or lower FLA_Chol
+    (op "chol") on a copy of A, the copy into the reference's buffer
+    excluded.  Returns (seconds, return value)."""
+    import time
+    L = lib(kind=kind)
+    M = _Mat(L, A)
+    if op == "lu":
+        P = _Mat(L, np.zeros(min(M.a.shape), dtype=np.int32), np.int32, FLA_INT)
+        t0 = time.perf_counter()
+        r = L.FLA_LU_piv(M.obj, P.obj)
+    else:
+        t0 = time.perf_counter()
+        r = L.FLA_Chol(FLA_LOWER_TRIANGULAR, M.obj)
+    return time.perf_counter() - t0, r

@@ -111,6 +111,40 @@ def main():
     A = rng.uniform(-1, 1, (100, 100))
     x, it, info = R.dsgesv(A, B)
     out["dsgesv_A"], out["dsgesv_B"], out["dsgesv_X"], out["dsgesv_iter"] = A, B, x, np.array(it)
+    # the steps after QR: least squares, explicit Q, LAPACK ormqr / orgqr
+    for (m, n) in [(90, 40), (170, 130)]:
+        A = rng.standard_normal((m, n))
+        QR, T, _ = R.qr_ut(A)
+        B = rng.standard_normal((m, 3))
+        X, _ = R.qr_ut_solve(QR, T, B)
+        Q, _ = R.qr_ut_form_q(QR, T, n)
+        key = "qrx_%dx%d" % (m, n)
+        out[key + "_A"], out[key + "_B"], out[key + "_X"], out[key + "_Q"] = A, B, X, Q
+        a, tau, _ = R.dgeqrf(A)
+        CL = rng.standard_normal((m, 5))
+        CR = rng.standard_normal((4, m))
+        out[key + "_CL"], out[key + "_CR"] = CL, CR
+        for side, trans, Cm in [("L", "T", CL), ("L", "N", CL), ("R", "N", CR), ("R", "T", CR)]:
+            c, info = R.dormqr(side, trans, a, tau, Cm)
+            out[key + "_ormqr_%s%s" % (side, trans)] = c
+        q, info = R.dorgqr(a, tau, n)
+        out[key + "_orgqr"] = q
+        Tt, _ = R.accum_t_ut(a, 1.0 / tau, min(32, n))
+        out[key + "_accumT"] = Tt
+    # inversion: FLA_SPDinv, FLA_Trinv, FLA_Ttmm, dpotri_
+    for n in [50, 140]:
+        A = spd(rng, n)
+        out["spdinv_%d_A" % n] = A
+        out["spdinv_%d_L" % n], _ = R.spdinv(A, R.FLA_LOWER_TRIANGULAR)
+        out["spdinv_%d_U" % n], _ = R.spdinv(A, R.FLA_UPPER_TRIANGULAR)
+        Lf, _ = R.chol(A)
+        out["dpotri_%d_L" % n], _ = R.dpotri(Lf, "L")
+        M = rng.uniform(-1, 1, (n, n)) + 4 * np.eye(n)
+        out["trinv_%d_M" % n] = M
+        for uplo, ul in [(R.FLA_LOWER_TRIANGULAR, "l"), (R.FLA_UPPER_TRIANGULAR, "u")]:
+            for diag, dg in [(R.FLA_NONUNIT_DIAG, "n"), (R.FLA_UNIT_DIAG, "u")]:
+                out["trinv_%d_%s%s" % (n, ul, dg)], _ = R.trinv(M, uplo, diag)
+            out["ttmm_%d_%s" % (n, ul)], _ = R.ttmm(M, uplo)
     path = os.path.join(HERE, "reference_small.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes,", len(out), "arrays")

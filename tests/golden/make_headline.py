@@ -4,10 +4,18 @@ FLA_LU_piv, FLA_QR_UT and FLA_Apply_Q_UT over the reference's built-in f2c
 BLAS, single thread) on the seeded inputs of tests/golden/headline.py.
 
     python tests/golden/make_headline.py lu|chol|qr
+    python tests/golden/make_headline.py spread
 
-Each run takes minutes of one CPU core (the reference's f2c BLAS runs at a
-few GFLOP/s) and writes tests/golden/headline_<op>.npz.  See headline.py
-for what the records hold and how the GPU test uses them.
+Each of the first three takes minutes of one CPU core (the reference's f2c
+BLAS runs at a few GFLOP/s) and writes tests/golden/headline_<op>.npz.  See
+headline.py for what the records hold and how the GPU test uses them.
+
+"spread" adds to each record how far the same reference, built over
+OpenBLAS instead of its f2c BLAS (oracle/_ref/libflame_ref_openblas.so,
+all host threads), lands from it on the same input: the relative Frobenius
+difference of the two factors (from the sketches) and the OpenBLAS build's
+backward error.  Two correct FP64 builds of the reference differ by this
+much only through the order of their floating-point operations.
 """
 import os
 import sys
@@ -79,5 +87,43 @@ def make_qr():
     print("qr: r=%d be=%.4f %.0fs" % (r, be, secs))
 
 
+def _add(name, **kw):
+    path = os.path.join(HERE, "headline_%s.npz" % name)
+    rec = dict(np.load(path))
+    rec.update({k: np.array(v) for k, v in kw.items()})
+    np.savez_compressed(path, **rec)
+
+
+def make_spread():
+    import torch
+    R.openblas_threads(os.cpu_count() or 1)
+    rec = np.load(os.path.join(HERE, "headline_lu.npz"))
+    A = H.lu_input()
+    LU, p, r = R.lu_piv(A, kind="openblas")
+    rel = H.sketch_rel_diff(H.sketches(torch, torch.from_numpy(LU), "cpu"), (rec["sk_l"], rec["sk_r"]))
+    be = H.lu_backward_error(torch, torch.from_numpy(A), torch.from_numpy(LU), p, "cpu")
+    _add("lu", spread=rel, spread_pivots_identical=bool(np.array_equal(p, rec["p"])), spread_be=be)
+    print("lu spread %.3e (pivots identical %s), OpenBLAS build be %.4f" % (rel, np.array_equal(p, rec["p"]), be))
+    del A, LU
+    rec = np.load(os.path.join(HERE, "headline_chol.npz"))
+    G = H.chol_factor_input()
+    A = H.chol_input_torch(torch, G, "cpu").numpy()
+    del G
+    Lf, r = R.chol(A, kind="openblas")
+    Lt = torch.tril(torch.from_numpy(Lf))
+    rel = H.sketch_rel_diff(H.sketches(torch, Lt, "cpu"), (rec["sk_l"], rec["sk_r"]))
+    be = H.chol_backward_error(torch, torch.from_numpy(A), Lt)
+    _add("chol", spread=rel, spread_be=be)
+    print("chol spread %.3e, OpenBLAS build be %.4f" % (rel, be))
+    del A, Lf, Lt
+    rec = np.load(os.path.join(HERE, "headline_qr.npz"))
+    A, B = H.qr_input()
+    QR, T, r = R.qr_ut(A, kind="openblas")
+    rel = H.sketch_rel_diff(H.sketches(torch, torch.from_numpy(QR), "cpu"), (rec["sk_l"], rec["sk_r"]))
+    be = H.qr_backward_error(torch, torch.from_numpy(A), torch.from_numpy(QR), torch.from_numpy(T), "cpu")
+    _add("qr", spread=rel, spread_be=be)
+    print("qr spread %.3e, OpenBLAS build be %.4f" % (rel, be))
+
+
 if __name__ == "__main__":
-    {"lu": make_lu, "chol": make_chol, "qr": make_qr}[sys.argv[1]]()
+    {"lu": make_lu, "chol": make_chol, "qr": make_qr, "spread": make_spread}[sys.argv[1]]()

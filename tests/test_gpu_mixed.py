@@ -37,7 +37,8 @@ def backward_error(A, X, B):
 
 
 @pytest.mark.parametrize("prec,name", [(0, "bfloat16"), (1, "float16"), (2, None)])
-@pytest.mark.parametrize("m,n,k", [(300, 200, 128), (1000, 700, 256), (64, 64, 40)])
+@pytest.mark.parametrize("m,n,k", [(300, 200, 128), (1000, 700, 256), (64, 64, 40), (2049, 513, 1000),
+                                   (128, 128, 64), (257, 129, 8)])
 def test_lp_gemm_matches_rounded_product(cuda, flame, prec, name, m, n, k):
     torch = cuda
     g = torch.Generator(device="cuda").manual_seed(m + n + k + prec)
