@@ -518,7 +518,7 @@ def chol_n1024_section(torch, dev, F, peak, reps=60):
     n = 1024
     G = np.random.default_rng(1024).standard_normal((n, n))
     src = torch.from_numpy(G @ G.T / n + np.eye(n)).to(dev)  # symmetric: either order
-    work = torch.empty_like(src)
+    work = torch.empty((n, n), dtype=torch.float64, device=dev).t()  # column-major
     flush = torch.empty(32 * 1024 * 1024, dtype=torch.float64, device=dev)
     vW = F.View(work)
     L = F.lib()

@@ -77,7 +77,8 @@ int           FLA_B200_LU_piv_panel_noalloc( int m, int n, double* A, int lda, i
  * trailing updates with FP32 accumulation, panels in FP64) and FP64
  * iterative refinement restores FP64 accuracy; A is left unchanged.
  * prec: 0 BF16, 1 FP16 with power-of-two equilibration, 2 3xTF32
- * (FP32-accurate), -1 the library default (FLA_B200_IR_PREC, else FP16).
+ * (FP32-accurate), 3 FP16 hi/lo split (FP32-accurate, on the 16-bit
+ * tensor cores), -1 the library default (FLA_B200_IR_PREC, else FP16).
  * solver: 0 classic refinement (dsgesv_'s), 1 GMRES-IR (GMRES in FP64
  * preconditioned by the low-precision factors, for ill-conditioned A),
  * 2 adaptive (classic refinement while each step cuts the backward error
@@ -94,10 +95,11 @@ FLA_Error     FLA_B200_LU_piv_solve_mixed( FLA_Obj A, FLA_Obj B, FLA_Obj X, int 
 FLA_Error     FLA_B200_Chol_solve_mixed( FLA_Uplo uplo, FLA_Obj A, FLA_Obj B, FLA_Obj X, int prec,
                                          int solver, int* iter, int* inner );
 
-/* The 16-bit tensor-core GEMM of the mixed-precision factorizations on
- * device buffers: C (FP32, column-major) := alpha A B^T + beta C, A m x k
- * and B n x k FP32 column-major, rounded to prec (0 BF16, 1 FP16),
- * accumulated in FP32. */
+/* The tensor-core GEMM of the mixed-precision factorizations on device
+ * buffers: C (FP32, column-major) := alpha A B^T + beta C, A m x k and B
+ * n x k FP32 column-major, rounded to prec (0 BF16, 1 FP16: tcgen05 with an
+ * FP32 TMEM accumulator; 2 3xTF32; 3 FP16 hi/lo split, three tcgen05
+ * products, FP32-accurate), accumulated in FP32. */
 int           FLA_B200_lp_gemm( int prec, long m, long n, long k, float alpha, const float* A, long lda,
                                 const float* B, long ldb, float beta, float* C, long ldc );
 

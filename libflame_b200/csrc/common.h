@@ -104,6 +104,7 @@ enum WsSlot : int {
   WS_SOLVE_W,       // block of solved unknowns
   WS_SPLITK,        // partial products of split-K GEMMs
   WS_PANEL_T,       // transposed copies of Cholesky panels (two, ping-pong)
+  WS_SWEEP,         // ready flags of the one-launch triangular sweeps
   WS_NSLOTS
 };
 void* ws_get(int slot, size_t bytes);  // nullptr on allocation failure

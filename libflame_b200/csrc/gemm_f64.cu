@@ -38,17 +38,21 @@ namespace {
 constexpr int BN = 64, BK = 16;
 
 // Tile shapes: BM = 128 (8 warps, 4 stages, 2 CTAs per SM) or BM = 64
-// (4 warps, 3 stages, 4 CTAs per SM).  Each warp owns a 32 x 32 sub-tile.
-template <int BM_>
+// (4 warps, 3 stages, 4 CTAs per SM), BN = 64; and 128 x 32 (4 warps) for
+// products with at most 32 columns (the refinement residual B - A X).  Each
+// warp owns a 32 x 32 sub-tile.
+template <int BM_, int BN_ = BN>
 struct Tile {
   static constexpr int BM = BM_;
-  static constexpr int WM = BM / 32;                 // warps along m (2 along n)
-  static constexpr int WARPS = WM * 2;
+  static constexpr int BNT = BN_;
+  static constexpr int WM = BM / 32;                 // warps along m
+  static constexpr int WN = BN_ / 32;                // warps along n
+  static constexpr int WARPS = WM * WN;
   static constexpr int THREADS = WARPS * 32;
   static constexpr int STAGES = BM == 128 ? 4 : 3;
   static constexpr int MINB = BM == 128 ? 2 : 4;      // CTAs per SM
   static constexpr int A_STAGE_BYTES = BM * BK * 8;
-  static constexpr int B_STAGE_BYTES = BN * BK * 8;
+  static constexpr int B_STAGE_BYTES = BN_ * BK * 8;
   static constexpr int STAGE_BYTES = A_STAGE_BYTES + B_STAGE_BYTES;
   static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 2048 /*align*/ + 256 /*barriers*/;
 };
@@ -89,13 +93,14 @@ __device__ __forceinline__ double lds_f64(uint32_t addr) {
   return v;
 }
 
-template <bool A_K, bool B_K, int BM_>
-__global__ void __launch_bounds__(Tile<BM_>::THREADS, Tile<BM_>::MINB)
+template <bool A_K, bool B_K, int BM_, int BN_ = BN>
+__global__ void __launch_bounds__(Tile<BM_, BN_>::THREADS, Tile<BM_, BN_>::MINB)
     dgemm_tma_kernel(const __grid_constant__ CUtensorMap mapA,
                      const __grid_constant__ CUtensorMap mapB, double* __restrict__ C, long ldc,
                      int M, int N, int K, double alpha, double beta, int mode, long diag_off,
                      int* err, const int* guard, int guard_limit, int k_chunk, long c_zstride) {
-  using TC = Tile<BM_>;
+  using TC = Tile<BM_, BN_>;
+  constexpr int BN = TC::BNT;  // shadows the default 64 for this instantiation
   constexpr int BM = TC::BM, STAGES = TC::STAGES, THREADS = TC::THREADS, CONSUMER_WARPS = TC::WARPS;
   constexpr int A_STAGE_BYTES = TC::A_STAGE_BYTES, STAGE_BYTES = TC::STAGE_BYTES;
   extern __shared__ unsigned char smem_raw[];
@@ -368,22 +373,21 @@ bool make_map(CUtensorMap* map, const double* p, long rows, long cols, long ld, 
   return r == CUDA_SUCCESS;
 }
 
-template <bool A_K, bool B_K, int BM_>
+template <bool A_K, bool B_K, int BM_, int BN_>
 void set_attrs() {
   static bool done = false;
   if (!done) {
-    cudaFuncSetAttribute(dgemm_tma_kernel<A_K, B_K, BM_>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         Tile<BM_>::SMEM_BYTES);
+    cudaFuncSetAttribute(dgemm_tma_kernel<A_K, B_K, BM_, BN_>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         Tile<BM_, BN_>::SMEM_BYTES);
     done = true;
   }
 }
-
-template <bool A_K, bool B_K, int BM_>
+template <bool A_K, bool B_K, int BM_, int BN_ = BN>
 void launch(dim3 grid, cudaStream_t st, const CUtensorMap& mA, const CUtensorMap& mB, double* C, long ldc, long m,
             long n, long k, double alpha, double beta, GemmMode mode, long diag_off, int* err, const int* guard,
             int guard_limit, int k_chunk, long c_zstride) {
-  set_attrs<A_K, B_K, BM_>();
-  dgemm_tma_kernel<A_K, B_K, BM_><<<grid, Tile<BM_>::THREADS, Tile<BM_>::SMEM_BYTES, st>>>(
+  set_attrs<A_K, B_K, BM_, BN_>();
+  dgemm_tma_kernel<A_K, B_K, BM_, BN_><<<grid, Tile<BM_, BN_>::THREADS, Tile<BM_, BN_>::SMEM_BYTES, st>>>(
       mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, mode, diag_off, err, guard, guard_limit, k_chunk,
       c_zstride);
 }
@@ -443,14 +447,18 @@ int gemm_f64(cudaStream_t st, bool ta, bool tb, long m, long n, long k, double a
   // B operand: op(B) is k x n.  tb = false: stored k x n, k contiguous.
   //            tb = true: stored n x k, n contiguous.
   CUtensorMap mA, mB;
-  const int BMv = tile_bm();
+  // products with at most 32 columns and a long k (the refinement residual
+  // R = B - A X): 128 x 32 tiles, k split to fill the GPU
+  const bool narrow = (n <= 32 && mode == GEMM_FULL && !guard && k >= 2048);
+  const int BMv = narrow ? 128 : tile_bm();
+  const int BNv = narrow ? 32 : BN;
   bool okA = ta ? make_map(&mA, A, k, m, lda, 16, BMv) : make_map(&mA, A, m, k, lda, 16, BK);
-  bool okB = tb ? make_map(&mB, B, n, k, ldb, 16, BK) : make_map(&mB, B, k, n, ldb, 16, BN);
+  bool okB = tb ? make_map(&mB, B, n, k, ldb, 16, BK) : make_map(&mB, B, k, n, ldb, 16, BNv);
   if (!okA || !okB) {
     set_last_error("gemm_f64: cuTensorMapEncodeTiled failed");
     return FLA_FAILURE;
   }
-  dim3 grid((unsigned)((m + BMv - 1) / BMv), (unsigned)((n + BN - 1) / BN));
+  dim3 grid((unsigned)((m + BMv - 1) / BMv), (unsigned)((n + BNv - 1) / BNv));
   int* err = ctx().d_status + ST_ERROR;
   // Split K when the output has too few tiles to occupy the GPU and K is
   // long (the W = U^T B products of the QR updates and of FLA_Apply_Q_UT):
@@ -460,8 +468,8 @@ int gemm_f64(cudaStream_t st, bool ta, bool tb, long m, long n, long k, double a
   const int sms = ctx().num_sms;
   long S = 1, kc = 0, ldp = 0, zs = 0;
   double* Pz = nullptr;
-  if (mode == GEMM_FULL && !guard && tiles * 2 <= sms && k >= 2048) {
-    S = std::min<long>(std::min<long>((2L * sms + tiles - 1) / tiles, k / 512), 64);
+  if (mode == GEMM_FULL && !guard && (tiles * 2 <= sms || narrow) && k >= 2048) {
+    S = std::min<long>(std::min<long>(((narrow ? 4L : 2L) * sms + tiles - 1) / tiles, k / 512), 64);
     if (S > 1) {
       kc = ((k + S - 1) / S + BK - 1) / BK * BK;
       S = (k + kc - 1) / kc;
@@ -477,10 +485,12 @@ int gemm_f64(cudaStream_t st, bool ta, bool tb, long m, long n, long k, double a
   const double al = S > 1 ? 1.0 : alpha, be = S > 1 ? 0.0 : beta;
   const int pslot = prof_begin(st);
 #define FB_GEMM_LAUNCH(AK, BK_)                                                                                  \
-  (BMv == 64 ? launch<AK, BK_, 64>(grid, st, mA, mB, Cl, ldcl, m, n, k, al, be, mode, diag_off, err, guard,     \
-                                   guard_limit, (int)kc, zs)                                                    \
-             : launch<AK, BK_, 128>(grid, st, mA, mB, Cl, ldcl, m, n, k, al, be, mode, diag_off, err, guard,    \
-                                    guard_limit, (int)kc, zs))
+  (narrow ? launch<AK, BK_, 128, 32>(grid, st, mA, mB, Cl, ldcl, m, n, k, al, be, mode, diag_off, err, guard,   \
+                                     guard_limit, (int)kc, zs)                                                  \
+   : BMv == 64 ? launch<AK, BK_, 64>(grid, st, mA, mB, Cl, ldcl, m, n, k, al, be, mode, diag_off, err, guard,   \
+                                     guard_limit, (int)kc, zs)                                                  \
+               : launch<AK, BK_, 128>(grid, st, mA, mB, Cl, ldcl, m, n, k, al, be, mode, diag_off, err, guard,  \
+                                      guard_limit, (int)kc, zs))
   if (ta && !tb) FB_GEMM_LAUNCH(true, true);
   else if (ta && tb) FB_GEMM_LAUNCH(true, false);
   else if (!ta && !tb) FB_GEMM_LAUNCH(false, true);

@@ -167,10 +167,12 @@ __global__ void __launch_bounds__(LTHREADS) lp_gemm_kernel(const uint16_t* __res
 }
 
 // dst[r * ldd + kk] := src(r, kk), src(r, kk) at src[r * rs + kk * cs]
-template <typename TS, bool FP16>
+// MODE 0: BF16; 1: FP16; 2: FP16 hi plane at dst and lo plane (the
+// remainder times 2^11) at dst + plane.
+template <typename TS, int MODE>
 __global__ void __launch_bounds__(256) pack16_kernel(const TS* __restrict__ src, long rs, long cs,
                                                      uint16_t* __restrict__ dst, long ldd, int rows, int kdim,
-                                                     float scale) {
+                                                     float scale, long plane) {
   __shared__ float tile[32][33];
   const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
@@ -191,9 +193,13 @@ __global__ void __launch_bounds__(256) pack16_kernel(const TS* __restrict__ src,
     if (r < rows && k < kpad) {
       const float v = tile[tx][yy];
       uint16_t h;
-      if (FP16) {
+      if (MODE >= 1) {
         __half hv = __float2half_rn(v);
         h = *reinterpret_cast<uint16_t*>(&hv);
+        if (MODE == 2) {
+          __half lv = __float2half_rn((v - __half2float(hv)) * 2048.0f);
+          dst[plane + (long)r * ldd + k] = *reinterpret_cast<uint16_t*>(&lv);
+        }
       } else {
         __nv_bfloat16 bv = __float2bfloat16_rn(v);
         h = *reinterpret_cast<uint16_t*>(&bv);
@@ -466,9 +472,9 @@ int lp_gemm(cudaStream_t st, LowPrec prec, long m, long n, long k, float alpha, 
     const char* e = std::getenv("FLA_B200_LP_GEMM");
     return e && std::string(e) == "mma";
   }();
-  if (!use_mma_sync && k > 0)
-    return tc_gemm16(st, prec == LP_BF16, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, mode, diag_off, guard,
-                     guard_limit);
+  if (prec == LP_FP16X3 || (!use_mma_sync && k > 0))
+    return tc_gemm16(st, prec == LP_BF16, prec == LP_FP16X3, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, mode,
+                     diag_off, guard, guard_limit, aplane, bplane);
   lp_attrs();
   dim3 grid((unsigned)((m + LBM - 1) / LBM), (unsigned)((n + LBN - 1) / LBN));
   const int ps = prof_begin(st);
@@ -498,10 +504,12 @@ int pack16(cudaStream_t st, LowPrec prec, const TS* src, long rs, long cs, uint1
     return FLA_SUCCESS;
   }
   dim3 grid((unsigned)((rows + 31) / 32), (unsigned)((((kdim + 7) & ~7L) + 31) / 32));
-  if (prec == LP_FP16)
-    pack16_kernel<TS, true><<<grid, 256, 0, st>>>(src, rs, cs, dst, ldd, (int)rows, (int)kdim, scale);
+  if (prec == LP_FP16X3)
+    pack16_kernel<TS, 2><<<grid, 256, 0, st>>>(src, rs, cs, dst, ldd, (int)rows, (int)kdim, scale, plane);
+  else if (prec == LP_FP16)
+    pack16_kernel<TS, 1><<<grid, 256, 0, st>>>(src, rs, cs, dst, ldd, (int)rows, (int)kdim, scale, 0);
   else
-    pack16_kernel<TS, false><<<grid, 256, 0, st>>>(src, rs, cs, dst, ldd, (int)rows, (int)kdim, scale);
+    pack16_kernel<TS, 0><<<grid, 256, 0, st>>>(src, rs, cs, dst, ldd, (int)rows, (int)kdim, scale, 0);
   count_launch();
   FB_CK(cudaGetLastError());
   return FLA_SUCCESS;
@@ -539,12 +547,13 @@ int sgemm(cudaStream_t st, bool ta, bool tb, long m, long n, long k, float alpha
 
 // Direct entry to the 16-bit tensor-core GEMM for tests: C (FP32, ld ldc)
 // := alpha * A * B^T + beta * C with A (m x k) and B (n x k) given in FP32
-// column-major and packed here.  prec: 0 = BF16, 1 = FP16, 2 = 3xTF32.
+// column-major and packed here.  prec: 0 = BF16, 1 = FP16, 2 = 3xTF32,
+// 3 = split FP16 (FP32-accurate).
 extern "C" int FLA_B200_lp_gemm(int prec, long m, long n, long k, float alpha, const float* A, long lda,
                                 const float* B, long ldb, float beta, float* C, long ldc) {
   using namespace fb;
   if (!ctx().initialized) FLA_Init();
-  const LowPrec p = prec == 2 ? LP_TF32X3 : (prec == 1 ? LP_FP16 : LP_BF16);
+  const LowPrec p = prec == 3 ? LP_FP16X3 : prec == 2 ? LP_TF32X3 : (prec == 1 ? LP_FP16 : LP_BF16);
   const long kp = (k + 7) & ~7L;
   uint16_t* pa = (uint16_t*)ws_get(WS_MISC, lp_packed_bytes(p, m, kp));
   uint16_t* pb = (uint16_t*)ws_get(WS_MISC2, lp_packed_bytes(p, n, kp));

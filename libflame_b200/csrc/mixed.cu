@@ -36,6 +36,7 @@
 #include <vector>
 
 #include "common.h"
+#include "dev_util.cuh"
 #include "lowprec.h"
 #include "mixed.h"
 
@@ -44,6 +45,7 @@ namespace fb {
 namespace {
 
 constexpr int MB = 128;  // block size of the low-precision factorizations
+constexpr int NBO = 256;  // outer block of the low-precision Cholesky (depth of its updates)
 
 // AT[j + i * ldt] = (float)(A[i + j * lda] * sr[i] * sc[j])   (A m x n)
 __global__ void transpose_scale_kernel(const double* __restrict__ A, long lda, float* __restrict__ AT, long ldt,
@@ -253,30 +255,8 @@ __global__ void gather_rows_kernel(const double* __restrict__ R, long ldr, const
   }
 }
 
-// One block step of a blocked triangular sweep with inverted diagonal blocks
-// (FP32, nr <= 32 right-hand sides), 128 rows per CTA:
-//   Y(r, :) -= op(F)(r, b0 : b0+w) X(b0 : b0+w, :)     r in [r_lo, r_hi)
-// and the CTA whose rows are the next diagonal block [own_lo, own_lo+wn)
-// finishes that block in place: X(own_lo + i, :) = sum_k op(Inv)(i, k) Y(own_lo + k, :).
-// The solved block of this step was written by the previous launch (or by
-// the prologue launch, w = 0), so the inverse multiply is done once per
-// block rather than by every CTA, and X and Y are separate buffers: no CTA
-// reads rows another CTA of the same launch writes.
-// op(Inv)(i, k) = Inv[k + i * 128] when TI (else Inv[i + k * 128]);
-// op(F)(r, b0 + k) = F[(b0 + k) + r * ldf] when TF (else F[r + (b0 + k) * ldf]).
-// 32-column slab of a 128-row operand, 16 values per thread: all loads are
-// issued before any is used, so one slab costs one memory latency.
-// ROWMAJ: element (i, k) at P[k + i * ld] (else P[i + k * ld]); rows i < mi,
-// columns k < mk are read, the rest are zero.
-template <bool ROWMAJ>
-__device__ __forceinline__ void slab_load(const float* __restrict__ P, long ld, int mi, int mk, float (&v)[16]) {
-#pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    const int e = threadIdx.x + j * 256;
-    const int i = ROWMAJ ? (e >> 5) : (e & 127), k = ROWMAJ ? (e & 31) : (e >> 7);
-    v[j] = (i < mi && k < mk) ? (ROWMAJ ? P[(long)k + (long)i * ld] : P[(long)i + (long)k * ld]) : 0.f;
-  }
-}
+// Building blocks of the blocked triangular sweeps (FP32, 128-row blocks,
+// nr <= 32 right-hand sides) of the correction solves.
 // 128 x 128 block of op(P) into registers, 16 float4 per thread, every load
 // in flight at once.  ROWMAJ: element (i, k) at P[k + i * ld], else
 // P[i + k * ld]; the contiguous index runs in float4 steps (the caller
@@ -344,75 +324,108 @@ __device__ __forceinline__ void block_fma(const float* sF, const float (*sX)[36]
 
 constexpr int SOLVE_SMEM = (128 * 36 + 128 * 129) * 4;
 
-template <bool TI, bool TF>
-__global__ void __launch_bounds__(256) solve_step_kernel(const float* __restrict__ F, long ldf,
-                                                         const float* __restrict__ Inv, float* __restrict__ X,
-                                                         float* __restrict__ Y, long ldy, int nr, int b0, int w,
-                                                         int r_lo, int r_hi, int own_lo, int wn) {
+__device__ __forceinline__ int ld_acquire_flag(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_flag(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Whole blocked triangular sweep in one cooperative launch (FP32, nr <= 32
+// right-hand sides, 128-row blocks):
+//   X_i := op(Inv_i) (Y_i - sum_j op(F)(block i, block j) X_j)
+// over the blocks j solved before i (j < i forward, j > i backward).  CTA g
+// owns the blocks solved g-th, (g + G)-th, ... (G = gridDim.x); for each it
+// accumulates the contributions of the earlier blocks as they are published
+// (the next op(F) block is loaded before waiting on the previous X block),
+// then applies the inverse and publishes its own block: X stores, a fence,
+// and flags[i] := epoch.  Every block depends only on blocks solved earlier
+// and every CTA takes its blocks in solve order, so with all CTAs resident
+// (cooperative launch) the sweep cannot deadlock; each wait is bounded.
+// X blocks of other CTAs are read through L2 (ld.global.cg): they were
+// written during this launch.
+// op(Inv)(i, k) = Inv[k + i * 128] when TI (else Inv[i + k * 128]);
+// op(F)(r, c) = F[c + r * ldf] when TF (else F[r + c * ldf]).
+template <bool TI, bool TF, bool BWD>
+__global__ void __launch_bounds__(256) solve_sweep_kernel(const float* __restrict__ F, long ldf,
+                                                          const float* __restrict__ Inv, float* X,
+                                                          const float* __restrict__ Y, long ldy, int n, int nr,
+                                                          int nblk, int* flags, int epoch, int* err) {
   extern __shared__ __align__(16) float sm_solve[];
-  float (*sX)[36] = reinterpret_cast<float (*)[36]>(sm_solve);  // X(b0 : b0+w, :), then the owner's rows
-  float* sF = sm_solve + 128 * 36;                              // op(F) block, then op(Inv)
+  float (*sX)[36] = reinterpret_cast<float (*)[36]>(sm_solve);
+  float* sF = sm_solve + 128 * 36;
+  __shared__ int s_ok;
   const int tid = threadIdx.x;
   const int rg = tid & 31, cg = tid >> 5;
-  const int r0 = r_lo + blockIdx.x * 128;
-  const bool owner = (r0 == own_lo);
-  // the whole op(F) block (rows r0.., columns b0..b0+w) in flight first
-  float4 v[16];
-  const float* Fb = TF ? F + b0 + (long)r0 * ldf : F + r0 + (long)b0 * ldf;
-  if (w > 0) block_load<TF>(Fb, ldf, r_hi - r0, w, v);
-  {
-    // X block: element (k, c) at X[b0 + k + c * ldy]
-    float xv[16];
-    slab_load<false>(X + b0, ldy, w, nr, xv);
+  for (int q = blockIdx.x; q < nblk; q += gridDim.x) {
+    const int bi = BWD ? nblk - 1 - q : q;
+    const int r0 = bi * 128, wn = min(128, n - r0);
+    float acc[4][4];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int e = tid + j * 256;
-      sX[e & 127][e >> 7] = xv[j];
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
+    for (int t = 0; t < q; ++t) {
+      const int bj = BWD ? nblk - 1 - t : t;
+      const int c0 = bj * 128, w = min(128, n - c0);
+      float4 v[16];
+      block_load<TF>(TF ? F + c0 + (long)r0 * ldf : F + r0 + (long)c0 * ldf, ldf, wn, w, v);
+      if (tid == 0) {
+        int ok = 1;
+        if (ld_acquire_flag(flags + bj) < epoch) {
+          const unsigned long long t0 = globaltimer_ns();
+          while (ld_acquire_flag(flags + bj) < epoch) {
+            if (*((volatile int*)err) != 0 || globaltimer_ns() - t0 > kWaitLimitNs) {
+              atomicExch(err, 51);
+              ok = 0;
+              break;
+            }
+          }
+        }
+        s_ok = ok;
+      }
+      __syncthreads();
+      if (!s_ok) return;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int e = tid + j * 256;
+        const int k = e & 127, c = e >> 7;
+        sX[k][c] = (k < w && c < nr) ? __ldcg(X + (long)(c0 + k) + (long)c * ldy) : 0.f;
+      }
+      block_store<TF>(sF, v);
+      __syncthreads();
+      block_fma(sF, sX, w, rg, cg, acc);
+      __syncthreads();
     }
-  }
-  if (w > 0) block_store<TF>(sF, v);
-  // the owner's inverse block loads overlap the update
-  if (owner) block_load<TI>(Inv, 128, wn, wn, v);
-  __syncthreads();
-  float acc[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
-  block_fma(sF, sX, w, rg, cg, acc);
-  if (!owner) {
+    // X_i := op(Inv_i) (Y_i - acc)
+    float4 v[16];
+    block_load<TI>(Inv + (long)bi * 128 * 128, 128, wn, wn, v);
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
-      const int r = r0 + rg + 32 * a;
-      if (r < r_hi)
+      const int i = rg + 32 * a;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int c = 4 * cg + b;
+        sX[i][c] = (i < wn && c < nr) ? Y[(long)(r0 + i) + (long)c * ldy] - acc[a][b] : 0.f;
+        acc[a][b] = 0.f;
+      }
+    }
+    block_store<TI>(sF, v);
+    __syncthreads();
+    block_fma(sF, sX, wn, rg, cg, acc);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int i = rg + 32 * a;
+      if (i < wn)
 #pragma unroll
         for (int b = 0; b < 4; ++b)
-          if (4 * cg + b < nr) Y[(long)r + (long)(4 * cg + b) * ldy] -= acc[a][b];
+          if (4 * cg + b < nr) __stcg(X + (long)(r0 + i) + (long)(4 * cg + b) * ldy, acc[a][b]);
     }
-    return;
-  }
-  // owner: the next diagonal block, updated, into sX; then X := op(Inv) sX
-  __syncthreads();
-#pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int i = rg + 32 * a;
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int c = 4 * cg + b;
-      sX[i][c] = (i < wn && c < nr) ? Y[(long)(r0 + i) + (long)c * ldy] - acc[a][b] : 0.f;
-      acc[a][b] = 0.f;
-    }
-  }
-  block_store<TI>(sF, v);
-  __syncthreads();
-  block_fma(sF, sX, wn, rg, cg, acc);
-#pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int i = rg + 32 * a;
-    if (i < wn)
-#pragma unroll
-      for (int b = 0; b < 4; ++b)
-        if (4 * cg + b < nr) X[(long)(r0 + i) + (long)(4 * cg + b) * ldy] = acc[a][b];
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) st_release_flag(flags + bi, epoch);
   }
 }
 
@@ -430,7 +443,10 @@ struct LpWork {
   uint16_t* PB = nullptr;   // packed B-operand (n x MB)
   uint16_t* PC = nullptr;   // packed operand of the side stream (n x MB)
   uint16_t* PX = nullptr;   // packed inverse block (MB x MB)
-  long plane = 0, planeX = 0;  // LP_TF32X3: float offset of the lo planes
+  uint16_t* PD = nullptr;   // Cholesky: packed sub-panel of the side stream (n x MB)
+  uint16_t* PW[2] = {nullptr, nullptr};  // Cholesky: packed outer panels (n x NBO), ping-pong
+  long plane = 0, planeX = 0;  // lo-plane offsets (LP_TF32X3: floats; LP_FP16X3: 16-bit elements)
+  long planeW = 0;
   double* P64 = nullptr;    // FP64 panel (MB x n)
   double* X64 = nullptr;    // FP64 inverse blocks (2 x MB x MB)
 };
@@ -440,12 +456,17 @@ int lp_workspace(long n, LpFactor* f, LpWork* w) {
   f->ldf = (n + 3) & ~3L;
   f->F = (float*)ws_get(WS_LP0, sizeof(float) * (size_t)f->ldf * np);
   const size_t pk = lp_packed_bytes(LP_TF32X3, (long)np, MB), px = lp_packed_bytes(LP_TF32X3, MB, MB);
-  char* p16 = (char*)ws_get(WS_LP1, 3 * pk + px + 1024);
+  const size_t pw = lp_packed_bytes(LP_TF32X3, (long)np, NBO);
+  char* p16 = (char*)ws_get(WS_LP1, 4 * pk + px + 2 * pw + 4096);
   char* p64 = (char*)ws_get(WS_LP3, sizeof(double) * ((size_t)MB * np + 2 * (size_t)MB * MB) + 1024);
   const long nblk = (n + MB - 1) / MB;
   char* pinv = (char*)ws_get(WS_LP4, sizeof(float) * 2 * (size_t)nblk * MB * MB + sizeof(double) * 2 * np +
                                          sizeof(int) * 2 * np + 1024);
   if (!f->F || !p16 || !p64 || !pinv) return FLA_FAILURE;
+  w->PD = (uint16_t*)(p16 + 3 * pk + px);
+  w->PW[0] = (uint16_t*)(p16 + 4 * pk + px);
+  w->PW[1] = (uint16_t*)(p16 + 4 * pk + px + pw);
+  w->planeW = (long)NBO * (long)np;
   w->PA = (uint16_t*)p16;
   w->PB = (uint16_t*)(p16 + pk);
   w->PC = (uint16_t*)(p16 + 2 * pk);
@@ -565,6 +586,15 @@ int lp_lu_factor(DMat A, LowPrec prec, bool scale, LpFactor* f) {
 }
 
 // Cholesky of diag(d) A diag(d) in low precision; F holds L (lower, FP32).
+// The structure of the FP64 driver (chol_lower_enqueue): outer panels of
+// NBO = 256 columns, each factored as two 128-column sub-panels on the
+// second stream (FP64 diagonal block and its inverse, A21 := A21 inv(L11)^T
+// as a tensor-core GEMM, the panel's later columns updated by the first
+// sub-panel), then packed once into the K-major operand buffer of the
+// updates (two buffers used in turn, so packing the next panel never
+// overwrites the operand of an update still running); the main stream
+// updates the next panel's columns first (K = 256), then the rest of the
+// trailing matrix, beside the next panel.
 int lp_chol_factor_shift(DMat A, bool upper, LowPrec prec, bool scale, double sigma, LpFactor* f) {
   Context& cx = ctx();
   cudaStream_t st = cx.stream, sd = cx.side;
@@ -590,44 +620,64 @@ int lp_chol_factor_shift(DMat A, bool upper, LowPrec prec, bool scale, double si
   int* info = cx.d_status + ST_INFO;
   auto at = [&](long i, long j) { return F + i + j * ldf; };
 
-  auto panel = [&](long k, cudaStream_t s) -> int {
-    const int b = (int)std::min<long>(MB, n - k);
-    const long kb = k / MB;
-    if (convert2d<double, float>(s, at(k, k), ldf, w.P64, MB, b, b) != FLA_SUCCESS) return FLA_FAILURE;
-    if (potrf_diag_dev(w.P64, MB, b, (int)k, s) != FLA_SUCCESS) return FLA_FAILURE;
+  // 128-column sub-panel at column j: diagonal block in FP64, its inverse,
+  // and A21 := A21 inv(L11)^T
+  auto sub = [&](long j, cudaStream_t s) -> int {
+    const int b = (int)std::min<long>(MB, n - j);
+    const long kb = j / MB;
+    if (convert2d<double, float>(s, at(j, j), ldf, w.P64, MB, b, b) != FLA_SUCCESS) return FLA_FAILURE;
+    if (potrf_diag_dev(w.P64, MB, b, (int)j, s) != FLA_SUCCESS) return FLA_FAILURE;
     if (tri_inverse(w.P64, MB, b, true, false, w.X64, MB, s) != FLA_SUCCESS) return FLA_FAILURE;
-    if (convert2d<float, double>(s, w.P64, MB, at(k, k), ldf, b, b) != FLA_SUCCESS) return FLA_FAILURE;
+    if (convert2d<float, double>(s, w.P64, MB, at(j, j), ldf, b, b) != FLA_SUCCESS) return FLA_FAILURE;
     if (convert2d<float, double>(s, w.X64, MB, f->inv1 + kb * MB * MB, MB, b, b) != FLA_SUCCESS) return FLA_FAILURE;
-    const long m2 = n - k - b;
+    const long m2 = n - j - b;
     if (m2 <= 0) return FLA_SUCCESS;
-    // A21 := A21 inv(L11)^T: B(j, kk) = inv(L11)(j, kk)
+    // B(c, kk) = inv(L11)(c, kk)
     if (pack16<double>(s, prec, w.X64, 1, MB, w.PX, MB, b, b, 1.f, w.planeX) != FLA_SUCCESS) return FLA_FAILURE;
-    if (pack16<float>(s, prec, at(k + b, k), 1, ldf, w.PC, MB, m2, b, 1.f, w.plane) != FLA_SUCCESS)
+    if (pack16<float>(s, prec, at(j + b, j), 1, ldf, w.PC, MB, m2, b, 1.f, w.plane) != FLA_SUCCESS)
       return FLA_FAILURE;
-    return lp_gemm(s, prec, m2, b, b, 1.f, w.PC, MB, w.PX, MB, 0.f, at(k + b, k), ldf, GEMM_FULL, 0, info,
-                   (int)(k + b), w.plane, w.planeX);
+    return lp_gemm(s, prec, m2, b, b, 1.f, w.PC, MB, w.PX, MB, 0.f, at(j + b, j), ldf, GEMM_FULL, 0, info,
+                   (int)(j + b), w.plane, w.planeX);
+  };
+  // Outer panel at column k: its sub-panels, the first one updating the
+  // second's columns, then the rows below the panel packed into PW.
+  auto panel = [&](long k, cudaStream_t s) -> int {
+    const long kend = std::min<long>(n, k + NBO);
+    for (long j = k; j < kend; j += MB) {
+      if (sub(j, s) != FLA_SUCCESS) return FLA_FAILURE;
+      const long j2 = j + std::min<long>(MB, n - j);
+      if (j2 >= kend) break;
+      if (pack16<float>(s, prec, at(j2, j), 1, ldf, w.PD, MB, n - j2, j2 - j, 1.f, w.plane) != FLA_SUCCESS)
+        return FLA_FAILURE;
+      if (lp_gemm(s, prec, n - j2, kend - j2, j2 - j, -1.f, w.PD, MB, w.PD, MB, 1.f, at(j2, j2), ldf, GEMM_LOWER, 0,
+                  info, (int)j2, w.plane, w.plane) != FLA_SUCCESS)
+        return FLA_FAILURE;
+    }
+    if (n > kend)
+      return pack16<float>(s, prec, at(kend, k), 1, ldf, w.PW[(k / NBO) & 1], NBO, n - kend, kend - k, 1.f,
+                           w.planeW);
+    return FLA_SUCCESS;
   };
 
   cudaEvent_t ev_look = cx.ev[2], ev_panel = cx.ev[3];
   if (panel(0, st) != FLA_SUCCESS) return FLA_FAILURE;
-  for (long k = 0; k < n; k += MB) {
-    const int b = (int)std::min<long>(MB, n - k);
+  for (long k = 0; k < n; k += NBO) {
+    const int b = (int)std::min<long>(NBO, n - k);
     const long m2 = n - k - b;
     if (m2 <= 0) break;
     const int lim = (int)(k + b);
-    const int nb2 = (int)std::min<long>(MB, m2);
-    if (pack16<float>(st, prec, at(k + b, k), 1, ldf, w.PA, MB, m2, b, 1.f, w.plane) != FLA_SUCCESS)
-      return FLA_FAILURE;
-    if (lp_gemm(st, prec, m2, nb2, b, -1.f, w.PA, MB, w.PA, MB, 1.f, at(k + b, k + b), ldf, GEMM_LOWER, 0, info,
-                lim, w.plane, w.plane) != FLA_SUCCESS)
+    const int nb2 = (int)std::min<long>(NBO, m2);
+    uint16_t* P = w.PW[(k / NBO) & 1];
+    if (lp_gemm(st, prec, m2, nb2, b, -1.f, P, NBO, P, NBO, 1.f, at(k + b, k + b), ldf, GEMM_LOWER, 0, info, lim,
+                w.planeW, w.planeW) != FLA_SUCCESS)
       return FLA_FAILURE;
     FB_CK(cudaEventRecord(ev_look, st));
     FB_CK(cudaStreamWaitEvent(sd, ev_look, 0));
     if (panel(k + b, sd) != FLA_SUCCESS) return FLA_FAILURE;
     FB_CK(cudaEventRecord(ev_panel, sd));
-    if (m2 > nb2 && lp_gemm(st, prec, m2 - nb2, m2 - nb2, b, -1.f, lp_off(w.PA, prec, (size_t)nb2 * MB), MB,
-                            lp_off(w.PA, prec, (size_t)nb2 * MB), MB, 1.f, at(k + b + nb2, k + b + nb2), ldf,
-                            GEMM_LOWER, 0, info, lim, w.plane, w.plane) != FLA_SUCCESS)
+    if (m2 > nb2 && lp_gemm(st, prec, m2 - nb2, m2 - nb2, b, -1.f, lp_off(P, prec, (size_t)nb2 * NBO), NBO,
+                            lp_off(P, prec, (size_t)nb2 * NBO), NBO, 1.f, at(k + b + nb2, k + b + nb2), ldf,
+                            GEMM_LOWER, 0, info, lim, w.planeW, w.planeW) != FLA_SUCCESS)
       return FLA_FAILURE;
     FB_CK(cudaStreamWaitEvent(st, ev_panel, 0));
   }
@@ -645,11 +695,63 @@ int lp_chol_factor_shift(DMat A, bool upper, LowPrec prec, bool scale, double si
 int lp_chol_factor(DMat A, bool upper, LowPrec prec, bool scale, LpFactor* f) {
   if (lp_chol_factor_shift(A, upper, prec, scale, 0.0, f) != FLA_SUCCESS) return FLA_FAILURE;
   const double u = prec == LP_FP16 ? std::ldexp(1.0, -11) : prec == LP_BF16 ? std::ldexp(1.0, -8) : std::ldexp(1.0, -21);
+  // (LP_TF32X3 and LP_FP16X3 are FP32-accurate: 2^-21)
   for (int t = 0; t < 4 && f->info >= 0 && scale; ++t) {
     const double sigma = u * std::ldexp(1.0, 2 * t + 1);
     if (lp_chol_factor_shift(A, upper, prec, scale, sigma, f) != FLA_SUCCESS) return FLA_FAILURE;
     f->shift = sigma;
   }
+  return FLA_SUCCESS;
+}
+
+// One triangular sweep of the correction solve in a single cooperative
+// launch (solve_sweep_kernel): forward (L y = rhs) or backward (L^T x = y,
+// U x = y).  The ready flags live in a workspace slot that is zeroed when it
+// is (re)allocated; each sweep publishes a new epoch, so no reset is needed
+// between sweeps.
+int sweep(const LpFactor& f, const float* Yin, float* Xout, long n, long nrhs, bool backward, cudaStream_t st) {
+  static void* last_flags = nullptr;
+  static int epoch = 0;
+  static int max_ctas = 0;
+  const long nblk = (n + MB - 1) / MB;
+  int* flags = (int*)ws_get(WS_SWEEP, sizeof(int) * (size_t)std::max<long>(nblk, 1024));
+  if (!flags) return FLA_FAILURE;
+  if (flags != last_flags) {
+    FB_CK(cudaMemsetAsync(flags, 0, sizeof(int) * (size_t)std::max<long>(nblk, 1024), st));
+    last_flags = flags;
+    epoch = 0;
+  }
+  ++epoch;
+  if (max_ctas == 0) {
+    FB_CK(cudaFuncSetAttribute(solve_sweep_kernel<true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               SOLVE_SMEM));
+    FB_CK(cudaFuncSetAttribute(solve_sweep_kernel<false, false, false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, SOLVE_SMEM));
+    FB_CK(cudaFuncSetAttribute(solve_sweep_kernel<true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               SOLVE_SMEM));
+    int per_sm = 0;
+    FB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, solve_sweep_kernel<true, true, true>, 256,
+                                                        SOLVE_SMEM));
+    max_ctas = std::max(1, per_sm) * ctx().num_sms;
+  }
+  const int G = (int)std::min<long>(nblk, max_ctas);
+  const float* F = f.F;
+  long ldf = f.ldf;
+  const float* inv = backward ? (f.chol ? f.inv1 : f.inv2) : f.inv1;
+  float* X = Xout;
+  const float* Y = Yin;
+  long ldy = n;
+  int ni = (int)n, nr = (int)nrhs, nb = (int)nblk, ep = epoch;
+  int* err = ctx().d_status + ST_ERROR;
+  void* args[] = {(void*)&F, (void*)&ldf, (void*)&inv, (void*)&X, (void*)&Y, (void*)&ldy,
+                  (void*)&ni, (void*)&nr, (void*)&nb, (void*)&flags, (void*)&ep, (void*)&err};
+  void* fn;
+  if (backward) fn = (void*)solve_sweep_kernel<true, true, true>;
+  else fn = f.chol ? (void*)solve_sweep_kernel<false, false, false> : (void*)solve_sweep_kernel<true, true, false>;
+  const int ps = prof_begin(st);
+  FB_CK(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(256), args, SOLVE_SMEM, st));
+  prof_end(ps, st, PROF_TRSM, (double)n * (double)n * (double)nrhs);
+  count_launch();
   return FLA_SUCCESS;
 }
 
@@ -673,52 +775,10 @@ int lp_solve(const LpFactor& f, const double* R, long ldr, double* D, long ldd, 
   }
   count_launch();
   // Forward sweep L y = T (T -> Tb), backward sweep U x = y or L^T x = y
-  // (Tb -> T), one fused launch per 128-row block while nrhs <= 32.
+  // (Tb -> T): one cooperative launch each while nrhs <= 32.
   if (nrhs <= 32) {
-    static bool attr = false;
-    if (!attr) {
-      FB_CK(cudaFuncSetAttribute(solve_step_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 SOLVE_SMEM));
-      FB_CK(cudaFuncSetAttribute(solve_step_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 SOLVE_SMEM));
-      attr = true;
-    }
-    auto blk = [&](long kb) { return std::make_pair(kb * MB, (int)std::min<long>(MB, n - kb * MB)); };
-    // LU: inv(L11) = inv(L11^T)^T, L(r, c) = F[c + r * ldf]; Cholesky: inv(L11), L(r, c) = F[r + c * ldf]
-    auto fwd = [&](long kb, int w, long r_lo, long r_hi, long own) {
-      const unsigned g = (unsigned)std::max<long>(1, (r_hi - r_lo + 127) / 128);
-      const auto nx = blk(own / MB);
-      const float* inv = f.inv1 + (own / MB) * MB * MB;
-      if (!f.chol)
-        solve_step_kernel<true, true><<<g, 256, SOLVE_SMEM, st>>>(F, ldf, inv, Tb, T, n, (int)nrhs, (int)(kb * MB), w,
-                                                         (int)r_lo, (int)r_hi, (int)own, nx.second);
-      else
-        solve_step_kernel<false, false><<<g, 256, SOLVE_SMEM, st>>>(F, ldf, inv, Tb, T, n, (int)nrhs, (int)(kb * MB), w,
-                                                           (int)r_lo, (int)r_hi, (int)own, nx.second);
-    };
-    // Forward sweep L y = T: y into Tb block by block
-    fwd(0, 0, 0, blk(0).second, 0);
-    for (long kb = 0; kb + 1 < nblk; ++kb) {
-      const auto c = blk(kb);
-      fwd(kb, c.second, c.first + c.second, n, c.first + c.second);
-    }
-    // Backward sweep U x = y or L^T x = y: Tb is updated, x into T.
-    // LU: inv(U11) = inv(U11^T)^T, U(r, c) = F[c + r * ldf]; Cholesky: inv(L11)^T, L^T(r, c) = F[c + r * ldf]
-    auto bwd = [&](long kb, int w, long r_lo, long r_hi, long own) {
-      const unsigned g = (unsigned)std::max<long>(1, (r_hi - r_lo + 127) / 128);
-      const auto nx = blk(own / MB);
-      const float* inv = (f.chol ? f.inv1 : f.inv2) + (own / MB) * MB * MB;
-      solve_step_kernel<true, true><<<g, 256, SOLVE_SMEM, st>>>(F, ldf, inv, T, Tb, n, (int)nrhs, (int)(kb * MB), w,
-                                                       (int)r_lo, (int)r_hi, (int)own, nx.second);
-    };
-    const auto last = blk(nblk - 1);
-    bwd(nblk - 1, 0, last.first, n, last.first);
-    for (long kb = nblk - 1; kb >= 1; --kb) {
-      const auto c = blk(kb);
-      bwd(kb, c.second, 0, c.first, c.first - MB);
-    }
-    count_launch((unsigned)(2 * nblk));
-    FB_CK(cudaGetLastError());
+    if (sweep(f, T, Tb, n, nrhs, false, st) != FLA_SUCCESS) return FLA_FAILURE;
+    if (sweep(f, Tb, T, n, nrhs, true, st) != FLA_SUCCESS) return FLA_FAILURE;
   } else {
     // wide right-hand sides: sgemm per block
     for (long kb = 0; kb < nblk; ++kb) {
@@ -960,6 +1020,11 @@ int ir_refine(const DMat& A, const DMat& B, double* X, long ldx, const LpFactor&
     return w;
   };
   auto tlast = std::chrono::steady_clock::now();
+  // timing events of the trace (the context's events are created without
+  // timing)
+  static cudaEvent_t tev[3] = {nullptr, nullptr, nullptr};
+  if (trace && !tev[0])
+    for (auto& e : tev) FB_CK(cudaEventCreate(&e));
   if (converged(X, ldx, b.R, ldn, n, nrhs, cte, b, st, &ok) != FLA_SUCCESS) return FLA_FAILURE;
   double last = ratio();
   if (trace) std::fprintf(stderr, "libflame_b200 ir: step 0  r/(|A||x|) %.3e\n", last);
@@ -975,17 +1040,26 @@ int ir_refine(const DMat& A, const DMat& B, double* X, long ldx, const LpFactor&
       if (gmres(A, f, b.R, b.D, nrhs, m, cfg.gmres_tol, b, st, &inner) != FLA_SUCCESS) return FLA_FAILURE;
       res->inner += inner;
     } else {
+      if (trace) cudaEventRecord(tev[0], st);
       if (lp_solve(f, b.R, ldn, b.D, ldn, nrhs, b.T, b.Tb, st) != FLA_SUCCESS) return FLA_FAILURE;
+      if (trace) cudaEventRecord(tev[1], st);
     }
     add_kernel<<<grid_for(n * nrhs), 256, 0, st>>>(X, ldx, b.D, ldn, (int)n, (int)nrhs, 1.0);
     count_launch();
     if (residual(A, B, X, ldx, b.R, ldn, nrhs, st) != FLA_SUCCESS) return FLA_FAILURE;
+    if (trace) cudaEventRecord(tev[2], st);
     if (converged(X, ldx, b.R, ldn, n, nrhs, cte, b, st, &ok) != FLA_SUCCESS) return FLA_FAILURE;
     const double now = ratio();
     if (trace) {
       const auto tnow = std::chrono::steady_clock::now();
-      std::fprintf(stderr, "libflame_b200 ir: step %d  r/(|A||x|) %.3e  gmres %d  %.3f ms\n", it, now, res->inner,
-                   std::chrono::duration<double, std::milli>(tnow - tlast).count());
+      float ms_solve = 0.f, ms_res = 0.f;
+      if (cfg.solver != IR_GMRES) {
+        cudaEventElapsedTime(&ms_solve, tev[0], tev[1]);
+        cudaEventElapsedTime(&ms_res, tev[1], tev[2]);
+      }
+      std::fprintf(stderr, "libflame_b200 ir: step %d  r/(|A||x|) %.3e  gmres %d  %.3f ms (solve %.3f, update + "
+                   "residual %.3f)\n", it, now, res->inner,
+                   std::chrono::duration<double, std::milli>(tnow - tlast).count(), ms_solve, ms_res);
       tlast = tnow;
     }
     if (met && !(now < 0.5 * last)) {
@@ -1037,6 +1111,7 @@ IrConfig ir_default_config() {
     if (s == "bf16") c.prec = LP_BF16;
     if (s == "fp16") c.prec = LP_FP16;
     if (s == "tf32x3") c.prec = LP_TF32X3;
+    if (s == "fp16x3") c.prec = LP_FP16X3;
   }
   if (const char* e = std::getenv("FLA_B200_IR_SOLVER")) {
     const std::string s(e);

@@ -646,6 +646,7 @@ IrConfig config_from(int prec, int solver) {
   if (prec == 0) c.prec = LP_BF16;
   if (prec == 1) c.prec = LP_FP16;
   if (prec == 2) c.prec = LP_TF32X3;
+  if (prec == 3) c.prec = LP_FP16X3;
   if (solver == 0) c.solver = IR_CLASSIC;
   if (solver == 1) c.solver = IR_GMRES;
   if (solver == 2) c.solver = IR_AUTO;

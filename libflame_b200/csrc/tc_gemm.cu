@@ -18,6 +18,14 @@
 // Two CTAs fit on an SM (3 stages x 32 KB of shared memory, 2 x 128 TMEM
 // columns), so one CTA's epilogue overlaps the other's main loop.
 //
+// Split form (FP32-accurate products from FP16 operands): each operand
+// comes as two FP16 planes, hi = fp16(x) and lo = fp16((x - hi) * 2^11), so
+// x = hi + 2^-11 lo to about 2^-22 relative.  Per k-step the kernel issues
+// three MMAs, D1 += A_hi B_hi^T and D2 += A_hi B_lo^T + A_lo B_hi^T, into two
+// TMEM accumulators, and the epilogue forms D1 + 2^-11 D2 (the dropped
+// lo x lo term is below 2^-22 of the product).  Stages hold four tiles (64 KB
+// each), one CTA per SM.
+//
 // The shared-memory operand descriptors describe K-major tiles with the
 // 128-byte swizzle (rows of 128 bytes, 8-row atoms 1024 bytes apart); the
 // K = 16 sub-steps of a 64-wide k-block advance the start address by 32
@@ -45,16 +53,19 @@ constexpr int TC_BM = 128;
 constexpr int TC_BK = 64;  // 64 16-bit values = 128 bytes = one swizzle row
 constexpr int TC_THREADS = 128;
 
-template <int TN, int STAGES>
+template <int TN, int STAGES, bool SPLIT>
 struct TcCfg {
-  static constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2;
+  static constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2;  // one plane
   static constexpr uint32_t B_BYTES = TN * TC_BK * 2;
-  static constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;
+  static constexpr uint32_t NPLANE = SPLIT ? 2 : 1;
+  static constexpr uint32_t STAGE_BYTES = NPLANE * (A_BYTES + B_BYTES);
   static constexpr uint32_t BAR_OFF = STAGES * STAGE_BYTES;
   // stages, then 2*STAGES+1 mbarriers and the TMEM address slot, plus slack
   // to align the ring to 1024 bytes (the swizzle atom)
   static constexpr uint32_t SMEM_BYTES = BAR_OFF + 8 * (2 * STAGES + 1) + 16 + 1024;
-  static constexpr uint32_t TMEM_COLS = TN;  // FP32 accumulator columns (power of 2 >= 32)
+  // FP32 accumulator columns (a power of 2 >= 32): one TN-wide accumulator,
+  // two for the split form
+  static constexpr uint32_t TMEM_COLS = NPLANE * TN;
 };
 
 // K-major, 128-byte swizzle, 8-row atoms 1024 bytes apart (SBO), version 1.
@@ -101,12 +112,13 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-template <int TN, int STAGES>
-__global__ void __launch_bounds__(TC_THREADS, 2)
-    tc_gemm16_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB, float* C,
+template <int TN, int STAGES, bool SPLIT>
+__global__ void __launch_bounds__(TC_THREADS, SPLIT ? 1 : 2)
+    tc_gemm16_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB,
+                     const __grid_constant__ CUtensorMap mAl, const __grid_constant__ CUtensorMap mBl, float* C,
                      long ldc, int M, int N, int K, float alpha, float beta, uint32_t idesc, int lower,
                      long diag_off, const int* guard, int guard_limit, int* err) {
-  using Cfg = TcCfg<TN, STAGES>;
+  using Cfg = TcCfg<TN, STAGES, SPLIT>;
   extern __shared__ uint8_t smem_raw[];
   const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TN;
   // tile entirely outside the written triangle: nothing to do (CTA-uniform)
@@ -132,6 +144,10 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
     s_abort = 0;
     prefetch_tmap(&mA);
     prefetch_tmap(&mB);
+    if (SPLIT) {
+      prefetch_tmap(&mAl);
+      prefetch_tmap(&mBl);
+    }
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -159,6 +175,11 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
       mbar_arrive_expect_tx(bar0 + 8 * s, Cfg::STAGE_BYTES);
       tma_load_2d(sa, &mA, kb * TC_BK, m0, bar0 + 8 * s);
       tma_load_2d(sb, &mB, kb * TC_BK, n0, bar0 + 8 * s);
+      if (SPLIT) {
+        const uint32_t sal = sb + Cfg::B_BYTES, sbl = sal + Cfg::A_BYTES;
+        tma_load_2d(sal, &mAl, kb * TC_BK, m0, bar0 + 8 * s);
+        tma_load_2d(sbl, &mBl, kb * TC_BK, n0, bar0 + 8 * s);
+      }
       issued = kb + 1;
     }
     // drain: the last load issued into each stage has landed (bounded)
@@ -175,9 +196,15 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
       tc_fence_after();
       const uint32_t sa = base + s * Cfg::STAGE_BYTES, sb = sa + Cfg::A_BYTES;
 #pragma unroll
-      for (int k = 0; k < TC_BK / 16; ++k)
-        tc_mma_f16(tmem, umma_desc_k_sw128(sa + 32 * k), umma_desc_k_sw128(sb + 32 * k), idesc,
-                   (kb > 0 || k > 0) ? 1u : 0u);
+      for (int k = 0; k < TC_BK / 16; ++k) {
+        const uint32_t acc = (kb > 0 || k > 0) ? 1u : 0u;
+        tc_mma_f16(tmem, umma_desc_k_sw128(sa + 32 * k), umma_desc_k_sw128(sb + 32 * k), idesc, acc);
+        if (SPLIT) {
+          const uint32_t sal = sb + Cfg::B_BYTES, sbl = sal + Cfg::A_BYTES;
+          tc_mma_f16(tmem + TN, umma_desc_k_sw128(sa + 32 * k), umma_desc_k_sw128(sbl + 32 * k), idesc, acc);
+          tc_mma_f16(tmem + TN, umma_desc_k_sw128(sal + 32 * k), umma_desc_k_sw128(sb + 32 * k), idesc, 1u);
+        }
+      }
       tc_commit(bar0 + 8 * (STAGES + s));  // stage s free once these MMAs are done
     }
     tc_commit(done_bar);  // every MMA issued above has completed
@@ -194,15 +221,26 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
     if (n0 + c0 >= N) break;
     float v[32];
     tc_ld32(tl + c0, v);
+    if (SPLIT) {
+      float v2[32];
+      tc_ld32(tl + TN + c0, v2);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = fmaf(v2[j], 1.0f / 2048.0f, v[j]);
+    }
     if (row < M) {
+      // all 32 loads of C first (a store between them would serialize each
+      // load on its memory latency), then the stores
+      bool ok[32];
+      float cv[32];
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
         const int col = n0 + c0 + j;
-        if (col < N && (!lower || (long)row - (long)col >= diag_off)) {
-          float* cp = C + row + (long)col * ldc;
-          *cp = (beta == 0.f) ? alpha * v[j] : fmaf(alpha, v[j], beta * *cp);
-        }
+        ok[j] = col < N && (!lower || (long)row - (long)col >= diag_off);
+        cv[j] = (ok[j] && beta != 0.f) ? __ldcs(C + row + (long)col * ldc) : 0.f;
       }
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (ok[j]) __stcs(C + row + (long)(n0 + c0 + j) * ldc, fmaf(alpha, v[j], beta * cv[j]));
     }
   }
   tc_fence_before();
@@ -244,31 +282,44 @@ bool make_map16(CUtensorMap* map, const uint16_t* p, long rows, long kdim, long 
 constexpr int TC_TN = 128;
 constexpr int TC_STAGES = 3;
 
+template <bool SPLIT>
+void tc_set_attr() {
+  static bool done = false;
+  if (!done) {
+    cudaFuncSetAttribute(tc_gemm16_kernel<TC_TN, TC_STAGES, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)TcCfg<TC_TN, TC_STAGES, SPLIT>::SMEM_BYTES);
+    done = true;
+  }
+}
+
 }  // namespace
 
 // C := alpha A B^T + beta C on the tcgen05 tensor cores (see the top of
 // this file); A, B packed 16-bit, k contiguous, lda / ldb multiples of 8 and
-// 16-byte aligned bases (the TMA rules).  GEMM_LOWER writes i - j >= diag_off
-// only and skips tiles with nothing to write.
-int tc_gemm16(cudaStream_t st, bool bf16, long m, long n, long k, float alpha, const uint16_t* A, long lda,
-              const uint16_t* B, long ldb, float beta, float* C, long ldc, GemmMode mode, long diag_off,
-              const int* guard, int guard_limit) {
-  using Cfg = TcCfg<TC_TN, TC_STAGES>;
+// 16-byte aligned bases (the TMA rules).  split: FP16 hi planes at A / B and
+// lo planes (scaled by 2^11) aplane / bplane elements further.  GEMM_LOWER
+// writes i - j >= diag_off only and skips tiles with nothing to write.
+int tc_gemm16(cudaStream_t st, bool bf16, bool split, long m, long n, long k, float alpha, const uint16_t* A,
+              long lda, const uint16_t* B, long ldb, float beta, float* C, long ldc, GemmMode mode, long diag_off,
+              const int* guard, int guard_limit, long aplane, long bplane) {
   if (m <= 0 || n <= 0) return FLA_SUCCESS;
   if (k <= 0) {
     set_last_error("tc_gemm16: k must be positive");
     return FLA_FAILURE;
   }
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(tc_gemm16_kernel<TC_TN, TC_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)Cfg::SMEM_BYTES);
-    attr = true;
-  }
-  CUtensorMap mA, mB;
+  CUtensorMap mA, mB, mAl, mBl;
   if (!make_map16(&mA, A, m, k, lda, TC_BM) || !make_map16(&mB, B, n, k, ldb, TC_TN)) {
     set_last_error("tc_gemm16: cuTensorMapEncodeTiled failed");
     return FLA_FAILURE;
+  }
+  if (split) {
+    if (!make_map16(&mAl, A + aplane, m, k, lda, TC_BM) || !make_map16(&mBl, B + bplane, n, k, ldb, TC_TN)) {
+      set_last_error("tc_gemm16: cuTensorMapEncodeTiled failed");
+      return FLA_FAILURE;
+    }
+  } else {
+    mAl = mA;
+    mBl = mB;
   }
   // instruction descriptor: FP32 accumulator, A/B FP16 (0) or BF16 (1),
   // both K-major, N = TN, M = 128
@@ -277,11 +328,21 @@ int tc_gemm16(cudaStream_t st, bool bf16, long m, long n, long k, float alpha, c
                          ((uint32_t)(TC_BM >> 4) << 24);
   dim3 grid((unsigned)((m + TC_BM - 1) / TC_BM), (unsigned)((n + TC_TN - 1) / TC_TN));
   const int ps = prof_begin(st);
-  tc_gemm16_kernel<TC_TN, TC_STAGES><<<grid, TC_THREADS, Cfg::SMEM_BYTES, st>>>(
-      mA, mB, C, ldc, (int)m, (int)n, (int)k, alpha, beta, idesc, mode == GEMM_LOWER ? 1 : 0, diag_off, guard,
-      guard_limit, ctx().d_status + ST_ERROR);
-  prof_end(ps, st, PROF_GEMM,
-           mode == GEMM_LOWER && m == n ? (double)m * (double)(m + 1) * (double)k : 2.0 * m * (double)n * k);
+  const int lower = mode == GEMM_LOWER ? 1 : 0;
+  int* err = ctx().d_status + ST_ERROR;
+  if (split) {
+    tc_set_attr<true>();
+    tc_gemm16_kernel<TC_TN, TC_STAGES, true><<<grid, TC_THREADS, TcCfg<TC_TN, TC_STAGES, true>::SMEM_BYTES, st>>>(
+        mA, mB, mAl, mBl, C, ldc, (int)m, (int)n, (int)k, alpha, beta, idesc, lower, diag_off, guard, guard_limit,
+        err);
+  } else {
+    tc_set_attr<false>();
+    tc_gemm16_kernel<TC_TN, TC_STAGES, false><<<grid, TC_THREADS, TcCfg<TC_TN, TC_STAGES, false>::SMEM_BYTES, st>>>(
+        mA, mB, mAl, mBl, C, ldc, (int)m, (int)n, (int)k, alpha, beta, idesc, lower, diag_off, guard, guard_limit,
+        err);
+  }
+  const double fl = mode == GEMM_LOWER && m == n ? (double)m * (double)(m + 1) * (double)k : 2.0 * m * (double)n * k;
+  prof_end(ps, st, PROF_GEMM, fl);
   count_launch();
   FB_CK(cudaGetLastError());
   return FLA_SUCCESS;

@@ -14,7 +14,9 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
 @pytest.mark.parametrize("m,n,k", [(1, 1, 1), (128, 64, 16), (130, 70, 33), (300, 257, 128), (513, 190, 200),
                                    # few output tiles, long K: split-K slices and their ordered reduction
-                                   (32, 64, 16384), (64, 130, 5000), (33, 7, 3001)])
+                                   (32, 64, 16384), (64, 130, 5000), (33, 7, 3001),
+                                   # at most 32 columns, long K: 128 x 32 tiles, split K (refinement residuals)
+                                   (4099, 32, 8192), (1000, 17, 2048)])
 def test_dgemm_matches_torch(cuda, flame, ta, tb, m, n, k):
     torch = cuda
     g = torch.Generator(device="cuda").manual_seed(m * 1000 + n * 10 + k + 7 * ta + 3 * tb)

@@ -36,7 +36,7 @@ def backward_error(A, X, B):
                for c in range(B.shape[1]))
 
 
-@pytest.mark.parametrize("prec,name", [(0, "bfloat16"), (1, "float16"), (2, None)])
+@pytest.mark.parametrize("prec,name", [(0, "bfloat16"), (1, "float16"), (2, None), (3, None)])
 @pytest.mark.parametrize("m,n,k", [(300, 200, 128), (1000, 700, 256), (64, 64, 40), (2049, 513, 1000),
                                    (128, 128, 64), (257, 129, 8)])
 def test_lp_gemm_matches_rounded_product(cuda, flame, prec, name, m, n, k):
@@ -49,7 +49,7 @@ def test_lp_gemm_matches_rounded_product(cuda, flame, prec, name, m, n, k):
     rc = flame.lib().FLA_B200_lp_gemm(prec, m, n, k, -1.0, C.c_void_p(A.data_ptr()), m, C.c_void_p(B.data_ptr()), n,
                                       1.0, C.c_void_p(Cm.data_ptr()), m)
     assert rc == flame.FLA_SUCCESS, flame.last_error()
-    if name is None:  # 3xTF32: FP32-accurate products of the FP32 operands
+    if name is None:  # 3xTF32 / split FP16: FP32-accurate products of the FP32 operands
         ref = C0.double() - A.double() @ B.double().t()
     else:
         dt = getattr(torch, name)
@@ -65,7 +65,7 @@ def _oracle_lu_solution(oracle, A, B):
 
 
 @pytest.mark.parametrize("n,kappa", [(300, 1e2), (1000, 1e5)])
-@pytest.mark.parametrize("prec", [0, 1, 2])
+@pytest.mark.parametrize("prec", [0, 1, 2, 3])
 @pytest.mark.parametrize("solver", [0, 1])
 def test_lu_solve_mixed_matches_oracle(cuda, flame, oracle, n, kappa, prec, solver):
     rng = seeded(n + int(np.log10(kappa)) + 10 * prec + 100 * solver)
@@ -133,6 +133,31 @@ def test_chol_solve_mixed_matches_oracle(cuda, flame, oracle, n, kappa, uplo):
     assert be <= max(4 * be_o, 1e-15), (be, be_o, it, inner)
     assert rel_fro(X, Xo) <= kappa * 1e-14, (rel_fro(X, Xo), it)
     assert it >= 0, (it, inner)
+
+
+@pytest.mark.parametrize("n,kappa,max_iter", [(1000, 1e2, 5), (1000, 1e5, 12)])
+@pytest.mark.parametrize("spd", [True, False])
+def test_split_fp16_factors_converge_with_classic_refinement(cuda, flame, oracle, n, kappa, max_iter, spd):
+    """prec 3: FP16 hi/lo split operands, three tensor-core products per
+    update (FP32-accurate factors): classic refinement alone converges at
+    kappa up to 1e5, to the FP64 oracle's backward error."""
+    rng = seeded(n + int(np.log10(kappa)) + (0 if spd else 99))
+    A = conditioned(rng, n, kappa, spd=spd)
+    B = rng.standard_normal((n, 4))
+    Ad, Bd = to_dev(cuda, A), to_dev(cuda, B)
+    Xd = to_dev(cuda, np.zeros_like(B))
+    if spd:
+        r, it, inner = flame.chol_solve_mixed(Ad, Bd, Xd, flame.FLA_LOWER_TRIANGULAR, 3, 0)
+        Lo, _ = oracle.chol(A)
+        Xo = oracle.chol_solve(Lo, B)
+    else:
+        r, it, inner = flame.lu_piv_solve_mixed(Ad, Bd, Xd, 3, 0)
+        Xo = _oracle_lu_solution(oracle, A, B)
+    assert r == flame.FLA_SUCCESS, flame.last_error()
+    X = to_host(Xd)
+    assert 0 <= it <= max_iter, it
+    assert backward_error(A, X, B) <= max(4 * backward_error(A, Xo, B), 1e-15)
+    assert rel_fro(X, Xo) <= kappa * 1e-14
 
 
 def test_chol_solve_mixed_falls_back(cuda, flame, oracle):
