@@ -93,6 +93,7 @@ enum WsSlot : int {
   WS_LP2,
   WS_LP3,           //   FP64 panel / inverses
   WS_LP4,           //   inverse blocks kept for the correction solves
+  WS_LP5,           //   coupling blocks of the correction sweeps
   WS_IR0,           //   refinement vectors (FP64 / FP32)
   WS_IR1,
   WS_IR2,

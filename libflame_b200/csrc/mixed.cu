@@ -337,20 +337,26 @@ __device__ __forceinline__ void st_release_flag(int* p, int v) {
 // right-hand sides, 128-row blocks):
 //   X_i := op(Inv_i) (Y_i - sum_j op(F)(block i, block j) X_j)
 // over the blocks j solved before i (j < i forward, j > i backward).  CTA g
-// owns the blocks solved g-th, (g + G)-th, ... (G = gridDim.x); for each it
-// accumulates the contributions of the earlier blocks as they are published
-// (the next op(F) block is loaded before waiting on the previous X block),
-// then applies the inverse and publishes its own block: X stores, a fence,
-// and flags[i] := epoch.  Every block depends only on blocks solved earlier
-// and every CTA takes its blocks in solve order, so with all CTAs resident
-// (cooperative launch) the sweep cannot deadlock; each wait is bounded.
-// X blocks of other CTAs are read through L2 (ld.global.cg): they were
-// written during this launch.
+// owns the blocks solved g-th, (g + G)-th, ... (G = gridDim.x).  For block i,
+// whose predecessor in solve order is p (i - 1 forward, i + 1 backward):
+//   Z_i := op(Inv_i) (Y_i - sum_{j before p} op(F)(i, j) X_j)
+// is formed while p is still being solved (the contributions are taken as
+// the blocks are published), and once p is published only
+//   X_i := Z_i - W_i X_p,   W_i = op(Inv_i) op(F)(i, p)
+// (W precomputed per factorization, sweep_couplings) remains on the critical
+// path: one block product per block of the chain.  A block is published by
+// its X stores, a fence, and flags[i] := epoch.  Every block depends only on
+// blocks solved earlier and every CTA takes its blocks in solve order, so
+// with all CTAs resident (cooperative launch) the sweep cannot deadlock; each
+// wait is bounded.  X blocks of other CTAs are read through L2
+// (ld.global.cg): they were written during this launch.
 // op(Inv)(i, k) = Inv[k + i * 128] when TI (else Inv[i + k * 128]);
-// op(F)(r, c) = F[c + r * ldf] when TF (else F[r + c * ldf]).
+// op(F)(r, c) = F[c + r * ldf] when TF (else F[r + c * ldf]); W_i(r, c) at
+// W[i * 128 * 128 + r + c * 128].
 template <bool TI, bool TF, bool BWD>
 __global__ void __launch_bounds__(256) solve_sweep_kernel(const float* __restrict__ F, long ldf,
-                                                          const float* __restrict__ Inv, float* X,
+                                                          const float* __restrict__ Inv,
+                                                          const float* __restrict__ W, float* X,
                                                           const float* __restrict__ Y, long ldy, int n, int nr,
                                                           int nblk, int* flags, int epoch, int* err) {
   extern __shared__ __align__(16) float sm_solve[];
@@ -359,6 +365,33 @@ __global__ void __launch_bounds__(256) solve_sweep_kernel(const float* __restric
   __shared__ int s_ok;
   const int tid = threadIdx.x;
   const int rg = tid & 31, cg = tid >> 5;
+  // wait (thread 0, bounded) until block bj is published; CTA-uniform result
+  auto wait_block = [&](int bj) -> bool {
+    if (tid == 0) {
+      int ok = 1;
+      if (ld_acquire_flag(flags + bj) < epoch) {
+        const unsigned long long t0 = globaltimer_ns();
+        while (ld_acquire_flag(flags + bj) < epoch) {
+          if (*((volatile int*)err) != 0 || globaltimer_ns() - t0 > kWaitLimitNs) {
+            atomicExch(err, 51);
+            ok = 0;
+            break;
+          }
+        }
+      }
+      s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+  };
+  auto load_x = [&](int c0, int w) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int e = tid + j * 256;
+      const int k = e & 127, c = e >> 7;
+      sX[k][c] = (k < w && c < nr) ? __ldcg(X + (long)(c0 + k) + (long)c * ldy) : 0.f;
+    }
+  };
   for (int q = blockIdx.x; q < nblk; q += gridDim.x) {
     const int bi = BWD ? nblk - 1 - q : q;
     const int r0 = bi * 128, wn = min(128, n - r0);
@@ -367,40 +400,19 @@ __global__ void __launch_bounds__(256) solve_sweep_kernel(const float* __restric
     for (int a = 0; a < 4; ++a)
 #pragma unroll
       for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
-    for (int t = 0; t < q; ++t) {
+    float4 v[16];
+    for (int t = 0; t + 1 < q; ++t) {
       const int bj = BWD ? nblk - 1 - t : t;
       const int c0 = bj * 128, w = min(128, n - c0);
-      float4 v[16];
       block_load<TF>(TF ? F + c0 + (long)r0 * ldf : F + r0 + (long)c0 * ldf, ldf, wn, w, v);
-      if (tid == 0) {
-        int ok = 1;
-        if (ld_acquire_flag(flags + bj) < epoch) {
-          const unsigned long long t0 = globaltimer_ns();
-          while (ld_acquire_flag(flags + bj) < epoch) {
-            if (*((volatile int*)err) != 0 || globaltimer_ns() - t0 > kWaitLimitNs) {
-              atomicExch(err, 51);
-              ok = 0;
-              break;
-            }
-          }
-        }
-        s_ok = ok;
-      }
-      __syncthreads();
-      if (!s_ok) return;
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int e = tid + j * 256;
-        const int k = e & 127, c = e >> 7;
-        sX[k][c] = (k < w && c < nr) ? __ldcg(X + (long)(c0 + k) + (long)c * ldy) : 0.f;
-      }
+      if (!wait_block(bj)) return;
+      load_x(c0, w);
       block_store<TF>(sF, v);
       __syncthreads();
       block_fma(sF, sX, w, rg, cg, acc);
       __syncthreads();
     }
-    // X_i := op(Inv_i) (Y_i - acc)
-    float4 v[16];
+    // Z_i := op(Inv_i) (Y_i - acc)
     block_load<TI>(Inv + (long)bi * 128 * 128, 128, wn, wn, v);
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
@@ -415,6 +427,26 @@ __global__ void __launch_bounds__(256) solve_sweep_kernel(const float* __restric
     block_store<TI>(sF, v);
     __syncthreads();
     block_fma(sF, sX, wn, rg, cg, acc);
+    if (q > 0) {
+      // X_i := Z_i - W_i X_p once the predecessor p is published
+      const int bp = BWD ? bi + 1 : bi - 1;
+      const int c0 = bp * 128, w = min(128, n - c0);
+      block_load<false>(W + (long)bi * 128 * 128, 128, wn, w, v);
+      __syncthreads();
+      if (!wait_block(bp)) return;
+      load_x(c0, w);
+      block_store<false>(sF, v);
+      __syncthreads();
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = -acc[a][b];
+      block_fma(sF, sX, w, rg, cg, acc);  // acc = W X_p - Z
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = -acc[a][b];
+    }
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
       const int i = rg + 32 * a;
@@ -426,6 +458,53 @@ __global__ void __launch_bounds__(256) solve_sweep_kernel(const float* __restric
     __threadfence();
     __syncthreads();
     if (tid == 0) st_release_flag(flags + bi, epoch);
+  }
+}
+
+// Coupling blocks of the sweeps: W_i = op(Inv_i) op(F)(block i, block p),
+// p the block solved just before i (i - 1 forward, i + 1 backward), one CTA
+// per block, four 32-column passes of the 128 x 128 x 128 product; W_i(r, c)
+// at W[i * 128 * 128 + r + c * 128].
+template <bool TI, bool TF, bool BWD>
+__global__ void __launch_bounds__(256) sweep_coupling_kernel(const float* __restrict__ F, long ldf,
+                                                             const float* __restrict__ Inv, float* __restrict__ W,
+                                                             int n, int nblk) {
+  extern __shared__ __align__(16) float sm_solve[];
+  float (*sX)[36] = reinterpret_cast<float (*)[36]>(sm_solve);
+  float* sF = sm_solve + 128 * 36;
+  const int bi = blockIdx.x;
+  const int bp = BWD ? bi + 1 : bi - 1;
+  if (bp < 0 || bp >= nblk) return;
+  const int tid = threadIdx.x, rg = tid & 31, cg = tid >> 5;
+  const int r0 = bi * 128, wn = min(128, n - r0), c0 = bp * 128, w = min(128, n - c0);
+  float4 v[16];
+  block_load<TI>(Inv + (long)bi * 128 * 128, 128, wn, wn, v);
+  block_store<TI>(sF, v);
+  for (int pc = 0; pc < 4; ++pc) {
+    // sX(k, c) = op(F)(r0 + k, c0 + 32 pc + c)
+    for (int e = tid; e < 128 * 32; e += 256) {
+      const int k = e & 127, c = e >> 7;
+      const int col = 32 * pc + c;
+      sX[k][c] = (k < wn && col < w) ? (TF ? F[(c0 + col) + (long)(r0 + k) * ldf] : F[(r0 + k) + (long)(c0 + col) * ldf])
+                                     : 0.f;
+    }
+    __syncthreads();
+    float acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
+    block_fma(sF, sX, wn, rg, cg, acc);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int i = rg + 32 * a;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int c = 32 * pc + 4 * cg + b;
+        W[(long)bi * 128 * 128 + i + c * 128] = (i < wn && c < w) ? acc[a][b] : 0.f;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -486,6 +565,39 @@ int lp_workspace(long n, LpFactor* f, LpWork* w) {
 }
 
 }  // namespace
+
+// Coupling blocks of both correction sweeps for the current factors (see
+// solve_sweep_kernel), one launch per direction.
+int lp_couplings(LpFactor* f, cudaStream_t st) {
+  const long n = f->n;
+  const long nblk = (n + MB - 1) / MB;
+  float* w = (float*)ws_get(WS_LP5, sizeof(float) * 2 * (size_t)std::max<long>(nblk, 1) * MB * MB);
+  if (!w) return FLA_FAILURE;
+  f->wf = w;
+  f->wb = w + (size_t)nblk * MB * MB;
+  static bool attr = false;
+  if (!attr) {
+    FB_CK(cudaFuncSetAttribute(sweep_coupling_kernel<false, false, false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, SOLVE_SMEM));
+    FB_CK(cudaFuncSetAttribute(sweep_coupling_kernel<true, true, false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, SOLVE_SMEM));
+    FB_CK(cudaFuncSetAttribute(sweep_coupling_kernel<true, true, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, SOLVE_SMEM));
+    attr = true;
+  }
+  if (f->chol)
+    sweep_coupling_kernel<false, false, false><<<(unsigned)nblk, 256, SOLVE_SMEM, st>>>(f->F, f->ldf, f->inv1,
+                                                                                        f->wf, (int)n, (int)nblk);
+  else
+    sweep_coupling_kernel<true, true, false><<<(unsigned)nblk, 256, SOLVE_SMEM, st>>>(f->F, f->ldf, f->inv1, f->wf,
+                                                                                      (int)n, (int)nblk);
+  sweep_coupling_kernel<true, true, true><<<(unsigned)nblk, 256, SOLVE_SMEM, st>>>(
+      f->F, f->ldf, f->chol ? f->inv1 : f->inv2, f->wb, (int)n, (int)nblk);
+  count_launch(2);
+  FB_CK(cudaGetLastError());
+  f->coupled = true;
+  return FLA_SUCCESS;
+}
 
 // LU with partial pivoting of (diag(sr) A diag(sc)) in low precision, on the
 // transposed FP32 copy F = (scaled A)^T (n x n, ld ldf): the layout and the
@@ -579,6 +691,7 @@ int lp_lu_factor(DMat A, LowPrec prec, bool scale, LpFactor* f) {
     count_launch();
     FB_CK(cudaGetLastError());
   }
+  if (lp_couplings(f, st) != FLA_SUCCESS) return FLA_FAILURE;
   int info = -1;
   if (status_read(&info) != FLA_SUCCESS) return FLA_FAILURE;
   f->info = info;
@@ -681,6 +794,7 @@ int lp_chol_factor_shift(DMat A, bool upper, LowPrec prec, bool scale, double si
       return FLA_FAILURE;
     FB_CK(cudaStreamWaitEvent(st, ev_panel, 0));
   }
+  if (lp_couplings(f, st) != FLA_SUCCESS) return FLA_FAILURE;
   int inf = -1;
   if (status_read(&inf) != FLA_SUCCESS) return FLA_FAILURE;
   f->info = inf;
@@ -738,12 +852,13 @@ int sweep(const LpFactor& f, const float* Yin, float* Xout, long n, long nrhs, b
   const float* F = f.F;
   long ldf = f.ldf;
   const float* inv = backward ? (f.chol ? f.inv1 : f.inv2) : f.inv1;
+  const float* Wc = backward ? f.wb : f.wf;
   float* X = Xout;
   const float* Y = Yin;
   long ldy = n;
   int ni = (int)n, nr = (int)nrhs, nb = (int)nblk, ep = epoch;
   int* err = ctx().d_status + ST_ERROR;
-  void* args[] = {(void*)&F, (void*)&ldf, (void*)&inv, (void*)&X, (void*)&Y, (void*)&ldy,
+  void* args[] = {(void*)&F, (void*)&ldf, (void*)&inv, (void*)&Wc, (void*)&X, (void*)&Y, (void*)&ldy,
                   (void*)&ni, (void*)&nr, (void*)&nb, (void*)&flags, (void*)&ep, (void*)&err};
   void* fn;
   if (backward) fn = (void*)solve_sweep_kernel<true, true, true>;

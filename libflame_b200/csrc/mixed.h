@@ -41,6 +41,9 @@ struct LpFactor {
   int* perm = nullptr;  // LU: row order of P b (perm[i] = source row of row i)
   float* inv1 = nullptr;  // per 128-block: LU inv(L11^T); Cholesky inv(L11)
   float* inv2 = nullptr;  // per 128-block: LU inv(U11^T)
+  float* wf = nullptr;    // per 128-block: coupling blocks of the forward sweep
+  float* wb = nullptr;    //   and of the backward sweep (solve_sweep_kernel)
+  bool coupled = false;   // wf / wb formed for the current factors
   double* sr = nullptr;   // row scaling (or the symmetric scaling)
   double* sc = nullptr;   // column scaling
   int info = -1;          // first failing column of the low-precision factorization

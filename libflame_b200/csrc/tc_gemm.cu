@@ -4,40 +4,36 @@
 //   C (FP32, column-major) := alpha * A * B^T + beta * C
 //   A: m x k, B: n x k, FP16 or BF16, k contiguous (row r at A + r * lda)
 //
-// One CTA of 128 threads per 128 x TN output tile:
-//   * thread 0 (warp 0) streams the k-blocks of A (128 x 64) and B (TN x 64)
+// Persistent kernel, at most one CTA per SM, looping over 128 x TN output
+// tiles (TN = 128), six warps with fixed roles:
+//   * warp 0 (one thread) streams the k-blocks of A (128 x 64) and B (TN x 64)
 //     with 2D TMA loads (128-byte swizzle) into an S-stage ring of shared
 //     memory buffers, each stage completing an mbarrier transaction count;
-//   * thread 32 (warp 1) issues tcgen05.mma (M = 128, N = TN, K = 16, FP32
-//     accumulate) into a TN-column TMEM accumulator and releases each stage
-//     with tcgen05.commit on the stage's "empty" mbarrier, then commits a
-//     final "done" mbarrier;
-//   * the four warps read the accumulator (warp w owns TMEM lanes 32w..32w+31,
-//     i.e. tile rows) with tcgen05.ld and write C column by column (32
-//     consecutive rows per store: coalesced).
-// Two CTAs fit on an SM (3 stages x 32 KB of shared memory, 2 x 128 TMEM
-// columns), so one CTA's epilogue overlaps the other's main loop.
-//
-// Split form (FP32-accurate products from FP16 operands): each operand
-// comes as two FP16 planes, hi = fp16(x) and lo = fp16((x - hi) * 2^11), so
-// x = hi + 2^-11 lo to about 2^-22 relative.  Per k-step the kernel issues
-// three MMAs, D1 += A_hi B_hi^T and D2 += A_hi B_lo^T + A_lo B_hi^T, into two
-// TMEM accumulators, and the epilogue forms D1 + 2^-11 D2 (the dropped
-// lo x lo term is below 2^-22 of the product).  Stages hold four tiles (64 KB
-// each), one CTA per SM.
-//
+//   * warp 1 (one thread) issues tcgen05.mma (M = 128, N = TN, K = 16, FP32
+//     accumulate) into one of two TMEM accumulators, releases each stage with
+//     tcgen05.commit on the stage's "empty" mbarrier, and after a tile's last
+//     k-block commits the accumulator's "full" mbarrier;
+//   * warps 2-9 drain the accumulator (warp w reads TMEM lanes 32 (w mod 4) +
+//     0..31, i.e. tile rows, and half of the tile's columns) with
+//     tcgen05.ld, update C column by column (32 consecutive rows per store:
+//     coalesced) and arrive on the accumulator's "empty" mbarrier; eight
+//     warps keep enough loads of C in flight to run at the memory's pace.
+// With two accumulators the epilogue of one tile (the FP32 C read and write)
+// runs while the MMAs of the next tile proceed.
 // The shared-memory operand descriptors describe K-major tiles with the
 // 128-byte swizzle (rows of 128 bytes, 8-row atoms 1024 bytes apart); the
 // K = 16 sub-steps of a 64-wide k-block advance the start address by 32
 // bytes inside the swizzle atom.
 //
 // Every mbarrier wait is bounded (kWaitLimitNs); on expiry the kernel
-// records the error in the status block, lets the MMA thread commit what it
-// issued, waits (bounded) for its own TMA loads still in flight, frees its
-// TMEM and returns without storing.
+// records the error in the status block and raises a CTA-wide abort flag
+// that every role checks: the producer waits (bounded) for its own TMA loads
+// still in flight, nothing more is stored, the TMEM is freed and the CTA
+// returns.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 
@@ -51,7 +47,8 @@ namespace {
 
 constexpr int TC_BM = 128;
 constexpr int TC_BK = 64;  // 64 16-bit values = 128 bytes = one swizzle row
-constexpr int TC_THREADS = 128;
+constexpr int TC_THREADS = 320;  // producer, MMA, eight epilogue warps
+constexpr int TC_EPI_WARPS = 8;
 
 template <int TN, int STAGES, bool SPLIT>
 struct TcCfg {
@@ -60,12 +57,14 @@ struct TcCfg {
   static constexpr uint32_t NPLANE = SPLIT ? 2 : 1;
   static constexpr uint32_t STAGE_BYTES = NPLANE * (A_BYTES + B_BYTES);
   static constexpr uint32_t BAR_OFF = STAGES * STAGE_BYTES;
-  // stages, then 2*STAGES+1 mbarriers and the TMEM address slot, plus slack
-  // to align the ring to 1024 bytes (the swizzle atom)
-  static constexpr uint32_t SMEM_BYTES = BAR_OFF + 8 * (2 * STAGES + 1) + 16 + 1024;
-  // FP32 accumulator columns (a power of 2 >= 32): one TN-wide accumulator,
-  // two for the split form
-  static constexpr uint32_t TMEM_COLS = NPLANE * TN;
+  // stages, then 2*STAGES + 5 mbarriers (stage full / empty, accumulator
+  // full / empty, final) and the TMEM address slot, plus slack to align the ring
+  // to 1024 bytes (the swizzle atom)
+  static constexpr uint32_t SMEM_BYTES = BAR_OFF + 8 * (2 * STAGES + 5) + 16 + 1024;
+  // FP32 columns of one accumulator (TN wide; a pair for the split form) and
+  // of the two accumulators the CTA allocates (a power of 2 <= 512)
+  static constexpr uint32_t ACC_COLS = NPLANE * TN;
+  static constexpr uint32_t TMEM_COLS = 2 * ACC_COLS;
 };
 
 // K-major, 128-byte swizzle, 8-row atoms 1024 bytes apart (SBO), version 1.
@@ -112,34 +111,71 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Bounded mbarrier wait that also gives up as soon as another role of the
+// CTA has raised the abort flag; false on timeout or abort (a timeout sets
+// the flag and records `code` in *err).
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err,
+                                        int code) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer_ns();
+  for (;;) {
+    for (int i = 0; i < 32; ++i)
+      if (mbar_try_wait(bar, parity)) return true;
+    if (*abort_flag) return false;
+    if (globaltimer_ns() - t0 > kWaitLimitNs) {
+      atomicExch(err, code);
+      *abort_flag = 1;
+      return false;
+    }
+  }
+}
+
 template <int TN, int STAGES, bool SPLIT>
-__global__ void __launch_bounds__(TC_THREADS, SPLIT ? 1 : 2)
+__global__ void __launch_bounds__(TC_THREADS, 1)
     tc_gemm16_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB,
                      const __grid_constant__ CUtensorMap mAl, const __grid_constant__ CUtensorMap mBl, float* C,
                      long ldc, int M, int N, int K, float alpha, float beta, uint32_t idesc, int lower,
                      long diag_off, const int* guard, int guard_limit, int* err) {
   using Cfg = TcCfg<TN, STAGES, SPLIT>;
   extern __shared__ uint8_t smem_raw[];
-  const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TN;
-  // tile entirely outside the written triangle: nothing to do (CTA-uniform)
-  if (lower && (long)(m0 + TC_BM - 1) - (long)n0 < diag_off) return;
   if (guard && *((volatile const int*)guard) < guard_limit) return;
+  const int tiles_m = (M + TC_BM - 1) / TC_BM, tiles_n = (N + TN - 1) / TN;
+  const int ntiles = tiles_m * tiles_n;
+  const int nk = (K + TC_BK - 1) / TC_BK;
+  // tile t: rows tm * 128.., columns tn * TN..; tiles entirely outside the
+  // written triangle are skipped by every role alike
+  auto tile_of = [&](int t, int& m0, int& n0) -> bool {
+    m0 = (t % tiles_m) * TC_BM;
+    n0 = (t / tiles_m) * TN;
+    return !lower || (long)(m0 + TC_BM - 1) - (long)n0 >= diag_off;
+  };
 
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   uint8_t* gbase = smem_raw + (base - raw);
-  const uint32_t bar0 = base + Cfg::BAR_OFF;  // full[s] = bar0 + 8s, empty[s] = bar0 + 8(S+s), done
-  const uint32_t done_bar = bar0 + 8 * (2 * STAGES);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + Cfg::BAR_OFF + 8 * (2 * STAGES + 1));
+  // full[s] = bar0 + 8s, empty[s] = bar0 + 8(S+s), accf[b] = bar0 + 8(2S+b),
+  // acce[b] = bar0 + 8(2S+2+b)
+  const uint32_t bar0 = base + Cfg::BAR_OFF;
+  auto full = [&](int s_) { return bar0 + 8u * s_; };
+  auto empty = [&](int s_) { return bar0 + 8u * (STAGES + s_); };
+  auto accf = [&](int b_) { return bar0 + 8u * (2 * STAGES + b_); };
+  auto acce = [&](int b_) { return bar0 + 8u * (2 * STAGES + 2 + b_); };
+  const uint32_t fin = bar0 + 8u * (2 * STAGES + 4);  // every MMA of the CTA done
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + Cfg::BAR_OFF + 8 * (2 * STAGES + 5));
   __shared__ int s_abort;
+  volatile int* abort_flag = &s_abort;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
-      mbar_init(bar0 + 8 * s, 1);
-      mbar_init(bar0 + 8 * (STAGES + s), 1);
+    for (int s_ = 0; s_ < STAGES; ++s_) {
+      mbar_init(full(s_), 1);
+      mbar_init(empty(s_), 1);
     }
-    mbar_init(done_bar, 1);
+    for (int b_ = 0; b_ < 2; ++b_) {
+      mbar_init(accf(b_), 1);
+      mbar_init(acce(b_), TC_EPI_WARPS);  // one arrive per epilogue warp
+    }
+    mbar_init(fin, 1);
     fence_barrier_init();
     s_abort = 0;
     prefetch_tmap(&mA);
@@ -149,7 +185,7 @@ __global__ void __launch_bounds__(TC_THREADS, SPLIT ? 1 : 2)
       prefetch_tmap(&mBl);
     }
   }
-  if (warp == 0) {
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(Cfg::TMEM_COLS)
                  : "memory");
@@ -159,93 +195,124 @@ __global__ void __launch_bounds__(TC_THREADS, SPLIT ? 1 : 2)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const int nk = (K + TC_BK - 1) / TC_BK;
 
-  if (threadIdx.x == 0) {
-    // ---- TMA producer
-    int issued = 0;
-    for (int kb = 0; kb < nk; ++kb) {
-      const int s = kb % STAGES, r = kb / STAGES;
-      if (r > 0 && !mbar_wait(bar0 + 8 * (STAGES + s), (uint32_t)((r - 1) & 1), err, 41)) {
-        s_abort = 1;
-        break;
-      }
-      if (*((volatile int*)&s_abort)) break;
-      const uint32_t sa = base + s * Cfg::STAGE_BYTES, sb = sa + Cfg::A_BYTES;
-      mbar_arrive_expect_tx(bar0 + 8 * s, Cfg::STAGE_BYTES);
-      tma_load_2d(sa, &mA, kb * TC_BK, m0, bar0 + 8 * s);
-      tma_load_2d(sb, &mB, kb * TC_BK, n0, bar0 + 8 * s);
-      if (SPLIT) {
-        const uint32_t sal = sb + Cfg::B_BYTES, sbl = sal + Cfg::A_BYTES;
-        tma_load_2d(sal, &mAl, kb * TC_BK, m0, bar0 + 8 * s);
-        tma_load_2d(sbl, &mBl, kb * TC_BK, n0, bar0 + 8 * s);
-      }
-      issued = kb + 1;
-    }
-    // drain: the last load issued into each stage has landed (bounded)
-    for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; ++kb)
-      mbar_wait(bar0 + 8 * (kb % STAGES), (uint32_t)((kb / STAGES) & 1), err, 42);
-  } else if (threadIdx.x == 32) {
-    // ---- MMA issuer
-    for (int kb = 0; kb < nk; ++kb) {
-      const int s = kb % STAGES, r = kb / STAGES;
-      if (!mbar_wait(bar0 + 8 * s, (uint32_t)(r & 1), err, 43)) {
-        s_abort = 1;
-        break;
-      }
-      tc_fence_after();
-      const uint32_t sa = base + s * Cfg::STAGE_BYTES, sb = sa + Cfg::A_BYTES;
-#pragma unroll
-      for (int k = 0; k < TC_BK / 16; ++k) {
-        const uint32_t acc = (kb > 0 || k > 0) ? 1u : 0u;
-        tc_mma_f16(tmem, umma_desc_k_sw128(sa + 32 * k), umma_desc_k_sw128(sb + 32 * k), idesc, acc);
-        if (SPLIT) {
-          const uint32_t sal = sb + Cfg::B_BYTES, sbl = sal + Cfg::A_BYTES;
-          tc_mma_f16(tmem + TN, umma_desc_k_sw128(sa + 32 * k), umma_desc_k_sw128(sbl + 32 * k), idesc, acc);
-          tc_mma_f16(tmem + TN, umma_desc_k_sw128(sal + 32 * k), umma_desc_k_sw128(sb + 32 * k), idesc, 1u);
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---- TMA producer
+      int kstep = 0;
+      for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
+        int m0, n0;
+        if (!tile_of(t, m0, n0)) continue;
+        for (int kb = 0; kb < nk; ++kb, ++kstep) {
+          const int s_ = kstep % STAGES, u = kstep / STAGES;
+          if (u > 0 && !tc_wait(empty(s_), (uint32_t)((u - 1) & 1), abort_flag, err, 41)) break;
+          if (*abort_flag) break;
+          const uint32_t sa = base + s_ * Cfg::STAGE_BYTES, sb = sa + Cfg::A_BYTES;
+          mbar_arrive_expect_tx(full(s_), Cfg::STAGE_BYTES);
+          tma_load_2d(sa, &mA, kb * TC_BK, m0, full(s_));
+          tma_load_2d(sb, &mB, kb * TC_BK, n0, full(s_));
+          if (SPLIT) {
+            const uint32_t sal = sb + Cfg::B_BYTES, sbl = sal + Cfg::A_BYTES;
+            tma_load_2d(sal, &mAl, kb * TC_BK, m0, full(s_));
+            tma_load_2d(sbl, &mBl, kb * TC_BK, n0, full(s_));
+          }
         }
       }
-      tc_commit(bar0 + 8 * (STAGES + s));  // stage s free once these MMAs are done
+      // drain: the last load issued into each stage has landed (bounded)
+      for (int q = (kstep > STAGES ? kstep - STAGES : 0); q < kstep; ++q)
+        mbar_wait(full(q % STAGES), (uint32_t)((q / STAGES) & 1), err, 42);
     }
-    tc_commit(done_bar);  // every MMA issued above has completed
-  }
-  // ---- epilogue: all four warps
-  const bool got = mbar_wait(done_bar, 0, err, 44);
-  tc_fence_after();
-  const bool store = got && nk > 0 && !*((volatile int*)&s_abort);
-  const int row = m0 + warp * 32 + lane;
-  const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll 1
-  for (int c0 = 0; c0 < TN; c0 += 32) {
-    if (!__all_sync(0xffffffffu, store ? 1 : 0)) break;
-    if (n0 + c0 >= N) break;
-    float v[32];
-    tc_ld32(tl + c0, v);
-    if (SPLIT) {
-      float v2[32];
-      tc_ld32(tl + TN + c0, v2);
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---- MMA issuer
+      int kstep = 0, lt = 0;
+      for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
+        int m0, n0;
+        if (!tile_of(t, m0, n0)) continue;
+        const int b_ = lt & 1, ua = lt >> 1;
+        // the epilogue has drained this accumulator's previous tile
+        if (ua > 0 && !tc_wait(acce(b_), (uint32_t)((ua - 1) & 1), abort_flag, err, 45)) break;
+        if (*abort_flag) break;
+        tc_fence_after();
+        const uint32_t dacc = tmem + (uint32_t)b_ * Cfg::ACC_COLS;
+        for (int kb = 0; kb < nk; ++kb, ++kstep) {
+          const int s_ = kstep % STAGES, u = kstep / STAGES;
+          if (!tc_wait(full(s_), (uint32_t)(u & 1), abort_flag, err, 43)) break;
+          tc_fence_after();
+          const uint32_t sa = base + s_ * Cfg::STAGE_BYTES, sb = sa + Cfg::A_BYTES;
 #pragma unroll
-      for (int j = 0; j < 32; ++j) v[j] = fmaf(v2[j], 1.0f / 2048.0f, v[j]);
-    }
-    if (row < M) {
-      // all 32 loads of C first (a store between them would serialize each
-      // load on its memory latency), then the stores
-      bool ok[32];
-      float cv[32];
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const int col = n0 + c0 + j;
-        ok[j] = col < N && (!lower || (long)row - (long)col >= diag_off);
-        cv[j] = (ok[j] && beta != 0.f) ? __ldcs(C + row + (long)col * ldc) : 0.f;
+          for (int k = 0; k < TC_BK / 16; ++k) {
+            const uint32_t acc = (kb > 0 || k > 0) ? 1u : 0u;
+            tc_mma_f16(dacc, umma_desc_k_sw128(sa + 32 * k), umma_desc_k_sw128(sb + 32 * k), idesc, acc);
+            if (SPLIT) {
+              const uint32_t sal = sb + Cfg::B_BYTES, sbl = sal + Cfg::A_BYTES;
+              tc_mma_f16(dacc + TN, umma_desc_k_sw128(sa + 32 * k), umma_desc_k_sw128(sbl + 32 * k), idesc, acc);
+              tc_mma_f16(dacc + TN, umma_desc_k_sw128(sal + 32 * k), umma_desc_k_sw128(sb + 32 * k), idesc, 1u);
+            }
+          }
+          tc_commit(empty(s_));  // stage free once these MMAs are done
+        }
+        if (*abort_flag) break;
+        tc_commit(accf(b_));  // the tile's accumulator is complete
+        ++lt;
       }
+      // nothing of this CTA's may still run on the tensor cores when its
+      // TMEM is freed
+      if (kstep > 0) {
+        tc_commit(fin);
+        mbar_wait(fin, 0, err, 46);
+      }
+    }
+  } else {
+    // ---- epilogue: warps 2-9, warp w owns TMEM lanes 32 (w mod 4) + 0..31
+    // and columns [h TN/2, (h+1) TN/2) of the tile, h = (w - 2) / 4
+    const int q = warp & 3, h = (warp - 2) >> 2;
+    int lt = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      int m0, n0;
+      if (!tile_of(t, m0, n0)) continue;
+      const int b_ = lt & 1, ua = lt >> 1;
+      const bool got = tc_wait(accf(b_), (uint32_t)(ua & 1), abort_flag, err, 44);
+      tc_fence_after();
+      if (!__all_sync(0xffffffffu, (got && !*abort_flag) ? 1 : 0)) break;
+      const int row = m0 + q * 32 + lane;
+      const uint32_t tl = tmem + (uint32_t)b_ * Cfg::ACC_COLS + ((uint32_t)(q * 32) << 16);
+#pragma unroll 1
+      for (int c0 = h * (TN / 2); c0 < (h + 1) * (TN / 2) && n0 + c0 < N; c0 += 32) {
+        float v[32];
+        tc_ld32(tl + c0, v);
+        if (SPLIT) {
+          float v2[32];
+          tc_ld32(tl + TN + c0, v2);
 #pragma unroll
-      for (int j = 0; j < 32; ++j)
-        if (ok[j]) __stcs(C + row + (long)(n0 + c0 + j) * ldc, fmaf(alpha, v[j], beta * cv[j]));
+          for (int j = 0; j < 32; ++j) v[j] = fmaf(v2[j], 1.0f / 2048.0f, v[j]);
+        }
+        if (row < M) {
+          // all 32 loads of C first (a store between them would serialize
+          // each load on its memory latency), then the stores
+          bool ok[32];
+          float cv[32];
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int col = n0 + c0 + j;
+            ok[j] = col < N && (!lower || (long)row - (long)col >= diag_off);
+            cv[j] = (ok[j] && beta != 0.f) ? __ldcs(C + row + (long)col * ldc) : 0.f;
+          }
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (ok[j]) __stcs(C + row + (long)(n0 + c0 + j) * ldc, fmaf(alpha, v[j], beta * cv[j]));
+        }
+      }
+      // accumulator drained: the MMA warp may reuse it
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acce(b_));
+      ++lt;
     }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) {
+  if (warp == 1) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::TMEM_COLS)
                  : "memory");
@@ -326,7 +393,8 @@ int tc_gemm16(cudaStream_t st, bool bf16, bool split, long m, long n, long k, fl
   const uint32_t fmt = bf16 ? 1u : 0u;
   const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(TC_TN >> 3) << 17) |
                          ((uint32_t)(TC_BM >> 4) << 24);
-  dim3 grid((unsigned)((m + TC_BM - 1) / TC_BM), (unsigned)((n + TC_TN - 1) / TC_TN));
+  const long ntiles = ((m + TC_BM - 1) / TC_BM) * ((n + TC_TN - 1) / TC_TN);
+  dim3 grid((unsigned)std::min<long>(ntiles, ctx().num_sms));
   const int ps = prof_begin(st);
   const int lower = mode == GEMM_LOWER ? 1 : 0;
   int* err = ctx().d_status + ST_ERROR;
