@@ -179,6 +179,22 @@ __device__ __forceinline__ void st_async_b32(uint32_t raddr, uint32_t v, uint32_
                : "memory");
 }
 
+// Orders this thread's generic-proxy writes to shared memory before later
+// async-proxy reads of them (a bulk copy issued after a CTA barrier).
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned)
+// from this CTA's shared memory to a cluster peer's (rdst, from mapa),
+// completing the bytes on the peer's mbarrier rbar.  No multicast.
+__device__ __forceinline__ void bulk_copy_to_peer(uint32_t rdst, uint32_t src, uint32_t bytes, uint32_t rbar) {
+  asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   rdst),
+               "r"(src), "r"(bytes), "r"(rbar)
+               : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait_cluster(uint32_t bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(

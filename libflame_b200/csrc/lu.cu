@@ -585,7 +585,9 @@ int lu_piv_dev(DMat A, int* d_piv, int* info) {
   const int NBL = (int)std::min<long>(lu_blocksize(), mn);
   const long ldT = even(n);
   double* AT = (double*)ws_get(WS_REPACK, sizeof(double) * (size_t)ldT * (size_t)m);
-  double* X = (double*)ws_get(WS_MISC, sizeof(double) * (size_t)(NBL + 1) * (NBL + 1));
+  // inverted U12_BS x U12_BS diagonal blocks of L11, each at stride U12_BS^2
+  const size_t xblocks = (size_t)(NBL + U12_BS - 1) / U12_BS;
+  double* X = (double*)ws_get(WS_MISC, sizeof(double) * xblocks * U12_BS * U12_BS);
   double* W = (double*)ws_get(WS_MISC2, sizeof(double) * (size_t)(NBL + 1) * (size_t)even(n));
   if (!AT || !X || !W) return FLA_FAILURE;
   if (status_reset() != FLA_SUCCESS) return FLA_FAILURE;

@@ -295,18 +295,67 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
 // Register-resident leaf for a panel stored transposed (element (i, col) at
 // P[i * ld + col]), w == W columns: thread t of each CTA owns the slab rows
 // i = t + k * 512 (k < RPT) and keeps their W entries in registers, so the
-// rank-1 updates never touch memory.  Per column: warp shuffles and warp 0
-// find the CTA's candidate (two CTA barriers); the warp holding the
-// candidate row gathers it by shuffles and pushes it, with the magnitude
-// and row index, into every CTA's shared memory, and the warp holding row j
-// does the same with row j; one cluster barrier; warp 0 picks the winner
-// (one CTA barrier); then each thread exchanges, scales and updates its own
-// rows and forms its candidate for the next column.  Same pivot order, tie
-// rule, null-column and NaN handling as lu_leaf_cluster_kernel.
+// rank-1 updates never touch memory.  Per column:
+//  1. each warp finds its candidate (largest magnitude, smallest row among
+//     equals) with three redux.sync reductions over a 64-bit ordering key,
+//     and the lane holding it writes the whole row, with the key and row
+//     index, into the warp's slot in shared memory; the owner of row j
+//     writes row j beside them;
+//  2. one CTA barrier; every warp reduces the 16 slot headers the same way
+//     and so knows the CTA's candidate and where its row lies;
+//  3. (clusters only) warp 0 bulk-copies the CTA's candidate slot, and row j
+//     if this CTA owns it, into every other CTA's shared memory, each copy
+//     completing bytes on the receiver's mbarrier; warp 0 waits for the
+//     column's bytes, a second CTA barrier releases the other warps, and
+//     every warp reduces the C candidate headers to the winner;
+//  4. each thread exchanges, scales and updates its own rows and forms its
+//     candidate for the next column.
+// Same pivot order, tie rule, null-column and NaN handling as
+// lu_leaf_cluster_kernel.  Exchange slots alternate between two halves by
+// column parity: a CTA cannot receive column j + 2's copies before every
+// CTA has finished reading column j's (it must first have passed column
+// j + 1's exchange, which needs this CTA's column j + 1 copies, issued
+// after its column j work).
 constexpr int RLEAF_THREADS = 512;
+constexpr int RLEAF_NW = RLEAF_THREADS / 32;
 
+// One exchange slot: 16-byte header and the W entries of the row.
+template <int W>
+struct RSlot {
+  unsigned long long key;  // ordering key: 0 no candidate, else bits(|x|) + 1
+  int row;                 // global row of the candidate (INT_MAX: none)
+  int pad;
+  double v[W];
+};
+
+// Layout: wslot [2][16] (the warps' candidates), cslot [2][C] (the CTAs'
+// candidates), rowj [2][W], two mbarriers, then one 32 x (W + 1) staging
+// tile per warp for the coalesced load and store of the slab.
+__host__ __device__ inline size_t rleaf_tile_offset(int w, int C) {
+  const size_t slot = 16 + 8 * (size_t)w;
+  return 2 * (RLEAF_NW + (size_t)C) * slot + 16 * (size_t)w + 16;
+}
 __host__ __device__ inline size_t rleaf_smem_bytes(int w, int C) {
-  return sizeof(double) * (2 * (size_t)C * w + 2 * C + 2 * w) + sizeof(int) * 2 * C + 64;
+  return rleaf_tile_offset(w, C) + sizeof(double) * RLEAF_NW * 32 * ((size_t)w + 1) + 128;
+}
+
+// Non-negative magnitudes order like their bit patterns, so the key orders
+// candidates by magnitude; no candidate orders below every magnitude (and
+// NaN never becomes a candidate: `t > best` is false for it).
+__device__ __forceinline__ unsigned long long rleaf_key(double bv, int bi) {
+  return bi == INT_MAX ? 0ull : (unsigned long long)__double_as_longlong(bv) + 1ull;
+}
+
+// Warp argmax of (key, row): the largest key, the smallest row among equal
+// keys; every lane receives the result.  Rows are distinct, INT_MAX marks
+// no candidate (key 0).
+__device__ __forceinline__ void rleaf_argmax_warp(unsigned long long& key, int& row) {
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  const bool top = hi == mhi && lo == mlo;
+  row = (int)__reduce_min_sync(0xffffffffu, top ? (unsigned)row : 0xffffffffu);
+  key = ((unsigned long long)mhi << 32) | mlo;
 }
 
 template <int W, int RPT>
@@ -318,24 +367,50 @@ __device__ __forceinline__ double rleaf_pick(const double (&rv)[RPT][W], int k, 
   return v;
 }
 
-// Lane `src` of the calling warp holds the row (slot k; have = false pushes
-// zeros); every lane gets it by shuffles and lane d < C stores it into CTA
-// d's buffer at local offset `dst` with st.async, completing bytes on CTA
-// d's mbarrier `bar` (both shared::cta addresses of this CTA, mapped).
+// Row slot k of the calling thread into shared memory (16-byte aligned).
 template <int W, int RPT>
-__device__ __forceinline__ void rleaf_push_row(const double (&rv)[RPT][W], int k, int src, bool have, uint32_t dst,
-                                               uint32_t bar, int C) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t rank = (uint32_t)(lane < C ? lane : 0);
-  const uint32_t rdst = mapa_shared(dst, rank), rbar = mapa_shared(bar, rank);
+__device__ __forceinline__ void rleaf_store_row(const double (&rv)[RPT][W], int k, double* dst) {
 #pragma unroll
-  for (int q0 = 0; q0 < W; q0 += 4) {
-    double row[4];
+  for (int q = 0; q < W; q += 2)
+    *reinterpret_cast<double2*>(dst + q) = make_double2(rleaf_pick<W, RPT>(rv, k, q), rleaf_pick<W, RPT>(rv, k, q + 1));
+}
+
+// The warp's 32 rows of slot k (slab rows base .. base + 31) pass through
+// its 32 x (W + 1) shared tile, so every global access of the warp reads or
+// writes whole rows (W contiguous doubles) instead of one entry of 32 rows.
+template <int W, int RPT>
+__device__ __forceinline__ void rleaf_load(double (&rv)[RPT][W], const LeafArgs& a, int r0, int rows,
+                                           double* tile, int warp, int lane) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) row[q] = __shfl_sync(0xffffffffu, rleaf_pick<W, RPT>(rv, k, q0 + q), src);
-    if (lane < C)
+  for (int k = 0; k < RPT; ++k) {
+    const int base = warp * 32 + k * RLEAF_THREADS;
+#pragma unroll 8
+    for (int e = lane; e < 32 * W; e += 32) {
+      const int rr = e / W, q = e % W;
+      tile[rr * (W + 1) + q] = (base + rr < rows) ? a.P[(long)(r0 + base + rr) * a.ld + q] : 0.0;
+    }
+    __syncwarp();
 #pragma unroll
-      for (int q = 0; q < 4; ++q) st_async_f64(rdst + 8 * (q0 + q), have ? row[q] : 0.0, rbar);
+    for (int q = 0; q < W; ++q) rv[k][q] = tile[lane * (W + 1) + q];
+    __syncwarp();
+  }
+}
+
+template <int W, int RPT>
+__device__ __forceinline__ void rleaf_store(const double (&rv)[RPT][W], const LeafArgs& a, int r0, int rows,
+                                            double* tile, int warp, int lane) {
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) {
+    const int base = warp * 32 + k * RLEAF_THREADS;
+#pragma unroll
+    for (int q = 0; q < W; ++q) tile[lane * (W + 1) + q] = rv[k][q];
+    __syncwarp();
+#pragma unroll 8
+    for (int e = lane; e < 32 * W; e += 32) {
+      const int rr = e / W, q = e % W;
+      if (base + rr < rows) a.P[(long)(r0 + base + rr) * a.ld + q] = tile[rr * (W + 1) + q];
+    }
+    __syncwarp();
   }
 }
 
@@ -357,7 +432,7 @@ __device__ __forceinline__ double rleaf_pick_col(const double (&row)[W], int j) 
 template <int W, int RPT, int J>
 __device__ __forceinline__ void rleaf_column(double (&rv)[RPT][W], int tid, int r0, int rows, int r,
                                              const double* u, const double* oldj, double rinv, double& bv,
-                                             int& bi) {
+                                             int& bi, int& bk) {
 #pragma unroll
   for (int k = 0; k < RPT; ++k) {
     const int i = tid + k * RLEAF_THREADS, gi = r0 + i;
@@ -377,161 +452,152 @@ __device__ __forceinline__ void rleaf_column(double (&rv)[RPT][W], int tid, int 
     for (int q = J + 1; q < W; ++q) rv[k][q] = fma(-l, u[q], rv[k][q]);
     if constexpr (J + 1 < W) {
       const double t = fabs(rv[k][J + 1]);
-      if (t > bv) { bv = t; bi = gi; }
+      if (t > bv) { bv = t; bi = gi; bk = k; }
     }
   }
 }
 
-template <int W, int RPT, int J = 0>
+// Run-time column j to its compile-time body through one jump table.
+template <int W, int RPT>
 __device__ __forceinline__ void rleaf_column_at(int j, double (&rv)[RPT][W], int tid, int r0, int rows, int r,
                                                 const double* u, const double* oldj, double rinv, double& bv,
-                                                int& bi) {
-  if constexpr (J < W) {
-    if (j == J) {
-      rleaf_column<W, RPT, J>(rv, tid, r0, rows, r, u, oldj, rinv, bv, bi);
-      return;
-    }
-    rleaf_column_at<W, RPT, J + 1>(j, rv, tid, r0, rows, r, u, oldj, rinv, bv, bi);
+                                                int& bi, int& bk) {
+  static_assert(W <= 32, "leaf width");
+  switch (j) {
+#define FB_RLEAF_CASE(J)                                                              \
+  case J:                                                                             \
+    if constexpr (J < W) rleaf_column<W, RPT, J>(rv, tid, r0, rows, r, u, oldj, rinv, bv, bi, bk); \
+    break;
+    FB_RLEAF_CASE(0) FB_RLEAF_CASE(1) FB_RLEAF_CASE(2) FB_RLEAF_CASE(3) FB_RLEAF_CASE(4) FB_RLEAF_CASE(5)
+    FB_RLEAF_CASE(6) FB_RLEAF_CASE(7) FB_RLEAF_CASE(8) FB_RLEAF_CASE(9) FB_RLEAF_CASE(10) FB_RLEAF_CASE(11)
+    FB_RLEAF_CASE(12) FB_RLEAF_CASE(13) FB_RLEAF_CASE(14) FB_RLEAF_CASE(15) FB_RLEAF_CASE(16)
+    FB_RLEAF_CASE(17) FB_RLEAF_CASE(18) FB_RLEAF_CASE(19) FB_RLEAF_CASE(20) FB_RLEAF_CASE(21)
+    FB_RLEAF_CASE(22) FB_RLEAF_CASE(23) FB_RLEAF_CASE(24) FB_RLEAF_CASE(25) FB_RLEAF_CASE(26)
+    FB_RLEAF_CASE(27) FB_RLEAF_CASE(28) FB_RLEAF_CASE(29) FB_RLEAF_CASE(30) FB_RLEAF_CASE(31)
+#undef FB_RLEAF_CASE
+    default:
+      break;
   }
 }
 
 template <int W, int RPT>
 __global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs a) {
-  extern __shared__ double S[];
-  constexpr int NW = RLEAF_THREADS / 32;
-  __shared__ double s_rv[2][NW];
-  __shared__ int s_ri[2][NW];
+  using Slot = RSlot<W>;
+  extern __shared__ __align__(128) unsigned char rleaf_smem[];
   cg::cluster_group cluster = cg::this_cluster();
   const int C = (int)cluster.num_blocks();
   const int c = (int)cluster.block_rank();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double* xrow = S;                                  // [2][C][W] candidate rows
-  double* xval = xrow + 2 * (size_t)C * W;           // [2][C] candidate magnitudes
-  double* rowj = xval + 2 * C;                       // [2][W] row j
-  int* xidx = reinterpret_cast<int*>(rowj + 2 * W);  // [2][C] candidate rows (INT_MAX: none)
+  Slot* wslot = reinterpret_cast<Slot*>(rleaf_smem);                               // [2][16]
+  Slot* cslot = wslot + 2 * RLEAF_NW;                                              // [2][C]
+  double* rowj = reinterpret_cast<double*>(cslot + 2 * C);                         // [2][W]
+  const uint32_t full0 = smem_u32(rowj + 2 * W);                                   // 2 mbarriers
   const int r0 = c * a.R;
   const int rows = max(0, min(a.R, a.M - r0));
-  // full[p]: the exchange buffers of parity p are complete (armed by thread
-  // 0 with the bytes expected per column, completed by the st.async pushes)
-  __shared__ __align__(8) unsigned long long s_full[2];
-  const uint32_t full0 = smem_u32(&s_full[0]);
-  const uint32_t xrow_s = smem_u32(xrow), xval_s = smem_u32(xval), rowj_s = smem_u32(rowj), xidx_s = smem_u32(xidx);
-  const uint32_t col_bytes = (uint32_t)(C * (8 * W + 8 + 4) + 8 * W);
-  if (tid == 0) {
-    mbar_init(full0, 1);
-    mbar_init(full0 + 8, 1);
-    fence_barrier_init();
+  if (C > 1) {
+    if (tid == 0) {
+      mbar_init(full0, 1);
+      mbar_init(full0 + 8, 1);
+      fence_barrier_init();
+    }
+    cluster.sync();  // every CTA's barriers exist before the first copy
   }
-  cluster.sync();  // every CTA's barriers exist before the first push
 
+  double* tile = reinterpret_cast<double*>(rleaf_smem + rleaf_tile_offset(W, C)) + warp * 32 * (W + 1);
   double rv[RPT][W];
-#pragma unroll
-  for (int k = 0; k < RPT; ++k) {
-    const int i = tid + k * RLEAF_THREADS;
-#pragma unroll
-    for (int q = 0; q < W; ++q) rv[k][q] = (i < rows) ? a.P[(long)(r0 + i) * a.ld + q] : 0.0;
-  }
+  rleaf_load<W, RPT>(rv, a, r0, rows, tile, warp, lane);
   int first_null = -1;
   double bv = -1.0;
-  int bi = INT_MAX;
+  int bi = INT_MAX, bk = 0;
 #pragma unroll
   for (int k = 0; k < RPT; ++k) {
     const int i = tid + k * RLEAF_THREADS;
     if (i < rows) {
       const double v = fabs(rv[k][0]);
-      if (v > bv) { bv = v; bi = r0 + i; }  // rows ascend with k
+      if (v > bv) { bv = v; bi = r0 + i; bk = k; }  // rows ascend with k
     }
   }
   // The column loop is not unrolled (the unrolled body would overflow the
   // instruction cache); the per-column update is dispatched to a
-  // compile-time column.  Per column one CTA barrier (the warps' candidates)
-  // and one cluster barrier (the pushed rows); every warp reduces the
-  // warps' candidates and the CTAs' candidates itself.
+  // compile-time column.
 #pragma unroll 1
   for (int j = 0; j < W; ++j) {
     const int par = j & 1;
-    // ---- 1. CTA candidate
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    const bool own_j = j >= r0 && j < r0 + rows;  // uniform in the CTA
+    // ---- 1. the warp's candidate into its slot; row j by its owner
+    {
+      unsigned long long wk = rleaf_key(bv, bi);
+      int wi = bi;
+      rleaf_argmax_warp(wk, wi);
+      Slot* ws = wslot + par * RLEAF_NW + warp;
+      if (wi == INT_MAX ? lane == 0 : wi == bi) {
+        ws->key = wk;
+        ws->row = wi;
+        if (wi != INT_MAX) rleaf_store_row<W, RPT>(rv, bk, ws->v);
+        if (C > 1) fence_proxy_async_smem();
+      }
+      if (own_j && tid == ((j - r0) & (RLEAF_THREADS - 1))) {
+        rleaf_store_row<W, RPT>(rv, (j - r0) / RLEAF_THREADS, rowj + par * W);
+        if (C > 1) fence_proxy_async_smem();
+      }
     }
-    if (lane == 0) { s_rv[par][warp] = bv; s_ri[par][warp] = bi; }
     __syncthreads();
+    // ---- 2. the CTA's candidate (every warp, same data, same result)
+    const Slot* best;
+    int r;
     {
-      double v = lane < NW ? s_rv[par][lane] : -1.0;
-      int i0 = lane < NW ? s_ri[par][lane] : INT_MAX;
-      // all 32 lanes take part (lanes >= NW hold the neutral element), so
-      // every lane of every warp ends with the same candidate
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, v, off);
-        const int oi = __shfl_xor_sync(0xffffffffu, i0, off);
-        if (ov > v || (ov == v && oi < i0)) { v = ov; i0 = oi; }
+      const Slot* hs = wslot + par * RLEAF_NW + (lane < RLEAF_NW ? lane : 0);
+      unsigned long long ck = lane < RLEAF_NW ? hs->key : 0ull;
+      const int mine = lane < RLEAF_NW ? hs->row : INT_MAX;
+      int ci = mine;
+      rleaf_argmax_warp(ck, ci);
+      const unsigned m = __ballot_sync(0xffffffffu, lane < RLEAF_NW && mine == ci);
+      best = wslot + par * RLEAF_NW + (m ? __ffs(m) - 1 : 0);
+      r = ci;
+    }
+    // ---- 3. exchange with the other CTAs of the cluster
+    if (C > 1) {
+      const uint32_t fullp = full0 + 8 * par;
+      const uint32_t ph = (uint32_t)((j >> 1) & 1);
+      bool ok = true;
+      if (warp == 0) {
+        if (lane < C && lane != c) {
+          const uint32_t rbar = mapa_shared(fullp, (uint32_t)lane);
+          bulk_copy_to_peer(mapa_shared(smem_u32(cslot + par * C + c), (uint32_t)lane), smem_u32(best),
+                            (uint32_t)sizeof(Slot), rbar);
+          if (own_j)
+            bulk_copy_to_peer(mapa_shared(smem_u32(rowj + par * W), (uint32_t)lane), smem_u32(rowj + par * W),
+                              (uint32_t)(8 * W), rbar);
+        }
+        if (lane == 0) mbar_arrive_expect_tx(fullp, (uint32_t)((C - 1) * sizeof(Slot) + (own_j ? 0 : 8 * W)));
+        ok = mbar_wait_cluster(fullp, ph, a.err, 21);
       }
-      bv = v;
-      bi = i0;
+      // the CTA leaves the loop together if the (bounded) wait ran out
+      if (__syncthreads_or(ok ? 0 : 1)) break;
+      if (warp != 0) (void)mbar_try_wait_cluster(fullp, ph);  // acquire of the completed phase
+      const Slot* hs = lane < C ? (lane == c ? best : cslot + par * C + lane) : best;
+      unsigned long long gk = lane < C ? hs->key : 0ull;
+      const int mine = lane < C ? hs->row : INT_MAX;
+      int gi = mine;
+      rleaf_argmax_warp(gk, gi);
+      const unsigned m = __ballot_sync(0xffffffffu, lane < C && mine == gi);
+      const int q = m ? __ffs(m) - 1 : c;
+      best = q == c ? best : cslot + par * C + q;
+      r = gi;
     }
-    // ---- 2. push the candidate row (zeros when this CTA has none), its
-    // magnitude and row, and row j (by its owner) into every CTA with
-    // st.async; each CTA waits for the column's bytes on its own mbarrier
-    const uint32_t fullp = full0 + 8 * par;
-    {
-      const bool have = bi != INT_MAX && bi - r0 >= 0 && bi - r0 < rows;
-      const int li = have ? bi - r0 : 0, ot = li & (RLEAF_THREADS - 1);
-      if (warp == (ot >> 5))
-        rleaf_push_row<W, RPT>(rv, li / RLEAF_THREADS, ot & 31, have,
-                               xrow_s + 8u * (uint32_t)((par * C + c) * W), fullp, C);
-    }
-    if (warp == NW - 1 && lane < C) {
-      const uint32_t rbar = mapa_shared(fullp, (uint32_t)lane);
-      st_async_f64(mapa_shared(xval_s + 8u * (uint32_t)(par * C + c), (uint32_t)lane), bv, rbar);
-      st_async_b32(mapa_shared(xidx_s + 4u * (uint32_t)(par * C + c), (uint32_t)lane), (uint32_t)bi, rbar);
-    }
-    if (j >= r0 && j < r0 + rows) {
-      const int lj = j - r0, jt = lj & (RLEAF_THREADS - 1);
-      if (warp == (jt >> 5))
-        rleaf_push_row<W, RPT>(rv, lj / RLEAF_THREADS, jt & 31, true, rowj_s + 8u * (uint32_t)(par * W), fullp, C);
-    }
-    if (tid == 0) mbar_arrive_expect_tx(fullp, col_bytes);
-    // every thread waits with cluster-scope acquire; the CTA leaves the loop
-    // together if the (bounded) wait ran out
-    const bool got = mbar_wait_cluster(fullp, (uint32_t)((j >> 1) & 1), a.err, 21);
-    if (!__syncthreads_and(got ? 1 : 0)) break;
-    // ---- 3. winner (identical in every warp of every CTA: same data, same
-    // order)
-    int r, w0;
-    {
-      double v = -2.0;
-      int i0 = INT_MAX, q0 = 0;
-      for (int q = lane; q < C; q += 32) {
-        const double cv = xval[par * C + q];
-        const int ci = xidx[par * C + q];
-        if (ci != INT_MAX && (cv > v || (cv == v && ci < i0))) { v = cv; i0 = ci; q0 = q; }
-      }
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, v, off);
-        const int oi = __shfl_xor_sync(0xffffffffu, i0, off);
-        const int oq = __shfl_xor_sync(0xffffffffu, q0, off);
-        if (ov > v || (ov == v && oi < i0)) { v = ov; i0 = oi; q0 = oq; }
-      }
-      r = i0;
-      w0 = q0;
-    }
-    const double* u = xrow + ((size_t)par * C + w0) * W;  // the pivot row
+    const double* u = best->v;  // the pivot row
+    const double* oldj = rowj + par * W;
     if (r == INT_MAX) {
       // no orderable candidate (every magnitude NaN): keep row j, as idamax
       // does when no later entry compares greater than the first
       r = j;
-      u = rowj + par * W;
+      u = oldj;
     }
-    const double* oldj = rowj + par * W;
     const double piv = u[j];
     if (c == 0 && tid == 0) a.piv[j] = r - j;
     bv = -1.0;
     bi = INT_MAX;
+    bk = 0;
     if (piv == 0.0) {
       // null column: no exchange, no scaling, no update
       if (first_null < 0) first_null = j;
@@ -541,24 +607,18 @@ __global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs 
           const int i = tid + k * RLEAF_THREADS, gi = r0 + i;
           if (i < rows && gi > j) {
             const double t = fabs(rleaf_pick_col<W>(rv[k], j + 1));
-            if (t > bv) { bv = t; bi = gi; }
+            if (t > bv) { bv = t; bi = gi; bk = k; }
           }
         }
       continue;
     }
     // ---- 4. exchange, scale, update, next candidate
-    rleaf_column_at<W, RPT>(j, rv, tid, r0, rows, r, u, oldj, 1.0 / piv, bv, bi);
+    rleaf_column_at<W, RPT>(j, rv, tid, r0, rows, r, u, oldj, 1.0 / piv, bv, bi, bk);
   }
-  // no CTA leaves while another may still push into its shared memory
-  cluster.sync();
-#pragma unroll
-  for (int k = 0; k < RPT; ++k) {
-    const int i = tid + k * RLEAF_THREADS;
-    if (i < rows)
-#pragma unroll
-      for (int q = 0; q < W; ++q) a.P[(long)(r0 + i) * a.ld + q] = rv[k][q];
-  }
+  rleaf_store<W, RPT>(rv, a, r0, rows, tile, warp, lane);
   if (c == 0 && tid == 0 && first_null >= 0) atomicMin(a.info, a.gcol + first_null);
+  // no CTA leaves while another may still copy into its shared memory
+  if (C > 1) cluster.sync();
 }
 
 struct LeafConfig {
@@ -601,8 +661,11 @@ int leaf_setup() {
     cudaGetLastError();
   }
   // the register-resident leaf: 512 threads, a few KB of SMEM
-  for (auto kern : {lu_leaf_reg_kernel<8, 4>, lu_leaf_reg_kernel<16, 2>, lu_leaf_reg_kernel<32, 1>})
+  for (auto kern : {lu_leaf_reg_kernel<8, 4>, lu_leaf_reg_kernel<16, 2>, lu_leaf_reg_kernel<32, 1>}) {
     FB_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    FB_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)rleaf_smem_bytes(32, LEAF_MAXC)));
+  }
   g_leaf.max_cluster_reg = 1;
   for (int cs = LEAF_MAXC; cs >= 2; cs >>= 1) {
     cudaLaunchConfig_t cfg = {};
