@@ -103,7 +103,11 @@ enum WsSlot : int {
   WS_PERM_T,        // gathered rows
   WS_TRINV,         // inverted diagonal blocks of the solves
   WS_SOLVE_W,       // block of solved unknowns
-  WS_SPLITK,        // partial products of split-K GEMMs
+  WS_SPLITK,        // partial products of split-K GEMMs (main stream)
+  WS_SPLITK_SIDE,   //   (side stream: the two streams' GEMMs may overlap)
+  WS_QR_T,          // FLA_QR_UT: the T factors of two panels (ping-pong)
+  WS_QR_U,          //   unit lower trapezoids of the panel recursion
+  WS_QR_W,          //   its W products
   WS_PANEL_T,       // transposed copies of Cholesky panels (two, ping-pong)
   WS_SWEEP,         // ready flags of the one-launch triangular sweeps
   WS_NSLOTS
@@ -182,7 +186,10 @@ enum GemmMode : int { GEMM_FULL = 0, GEMM_LOWER = 1 };
 int gemm_f64(cudaStream_t st, bool ta, bool tb, long m, long n, long k, double alpha,
              const double* A, long lda, const double* B, long ldb, double beta, double* C,
              long ldc, GemmMode mode = GEMM_FULL, long diag_off = 0,
-             const int* guard = nullptr, int guard_limit = 0x7fffffff);
+             const int* guard = nullptr, int guard_limit = 0x7fffffff, long kmax = 0);
+// kmax > 0 (full mode only): split k so that no CTA runs more than about
+// kmax of it, for GEMMs whose long-running tiles would keep SMs from a
+// cluster kernel waiting on the other stream.
 // The guard pointer is the status block's info word (INT_MAX, or the first
 // failing column): the kernel returns at once when it holds a column below
 // guard_limit, i.e. when a factorization step this update follows has failed.

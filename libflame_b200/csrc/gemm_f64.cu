@@ -407,6 +407,75 @@ __global__ void splitk_reduce_kernel(const double* __restrict__ P, long ldp, lon
   }
 }
 
+// Partial products of C = A^T B for small outputs (m, n <= 64) with a long
+// k (the W = U1^T B and T12 = U1^T U2 products of the QR panel recursion):
+// CTA z multiplies rows [z kc, (z+1) kc) of A (k x m) and B (k x n) with
+// FP64 FMAs, 32 rows at a time through shared memory, each of the 256
+// threads owning a TB x TB block of the output (16 TB >= m, n), and writes
+// its m x n partial to P + z m n; splitk_reduce_warp_kernel adds the
+// partials.  A 128 x 64 DMMA tile would spend most of its work on padding
+// for these shapes.
+constexpr int SK_ROWS = 32;
+template <int TB>
+__global__ void __launch_bounds__(256) gemm_tn_small_kernel(const double* __restrict__ A, long lda,
+                                                            const double* __restrict__ B, long ldb, int m, int n,
+                                                            long k, long kc, double* __restrict__ P) {
+  constexpr int D = 16 * TB;  // output block covered by the CTA
+  __shared__ double As[SK_ROWS][D + 1], Bs[SK_ROWS][D + 1];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const long k0 = blockIdx.x * kc, k1 = min(k, k0 + kc);
+  double acc[TB][TB] = {};
+  for (long kb = k0; kb < k1; kb += SK_ROWS) {
+    const int rows = (int)(k1 - kb < SK_ROWS ? k1 - kb : SK_ROWS);
+    for (int e = tid; e < SK_ROWS * D; e += 256) {
+      const int r = e % SK_ROWS, c = e / SK_ROWS;
+      As[r][c] = (r < rows && c < m) ? A[(kb + r) + (long)c * lda] : 0.0;
+      Bs[r][c] = (r < rows && c < n) ? B[(kb + r) + (long)c * ldb] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int r = 0; r < SK_ROWS; ++r) {
+      double av[TB], bv[TB];
+#pragma unroll
+      for (int t = 0; t < TB; ++t) {
+        av[t] = As[r][tx + 16 * t];
+        bv[t] = Bs[r][ty + 16 * t];
+      }
+#pragma unroll
+      for (int t = 0; t < TB; ++t)
+#pragma unroll
+        for (int u = 0; u < TB; ++u) acc[t][u] = fma(av[t], bv[u], acc[t][u]);
+    }
+    __syncthreads();
+  }
+  double* Pz = P + (long)blockIdx.x * m * n;
+#pragma unroll
+  for (int t = 0; t < TB; ++t)
+#pragma unroll
+    for (int u = 0; u < TB; ++u) {
+      const int i = tx + 16 * t, j = ty + 16 * u;
+      if (i < m && j < n) Pz[i + (long)j * m] = acc[t][u];
+    }
+}
+
+// C := alpha sum_z P_z + beta C for S partials of m x n (contiguous, m x n
+// apart): one warp per element, lane l adding partials l, l + 32, ..., then
+// a fixed shuffle tree (the same order on every run).
+__global__ void splitk_reduce_warp_kernel(const double* __restrict__ P, int S, int m, int n, double alpha,
+                                          double beta, double* __restrict__ C, long ldc) {
+  const long e = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (e >= (long)m * n) return;
+  double s = 0.0;
+  for (int z = lane; z < S; z += 32) s += P[(long)z * m * n + e];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  if (lane == 0) {
+    double* c = C + (e % m) + (e / m) * ldc;
+    *c = beta != 0.0 ? fma(beta, *c, alpha * s) : alpha * s;
+  }
+}
+
 // Tile height: 64 (four CTAs per SM hide one another's prologue and
 // epilogue best on the rank-128 updates of the factorizations: 26.6 against
 // 25.0 TFLOP/s at 16256 x 16256 x 128); FLA_B200_GEMM_BM=128 selects the
@@ -425,12 +494,33 @@ int tile_bm() {
 
 int gemm_f64(cudaStream_t st, bool ta, bool tb, long m, long n, long k, double alpha,
              const double* A, long lda, const double* B, long ldb, double beta, double* C,
-             long ldc, GemmMode mode, long diag_off, const int* guard, int guard_limit) {
+             long ldc, GemmMode mode, long diag_off, const int* guard, int guard_limit, long kmax) {
   if (m <= 0 || n <= 0) return FLA_SUCCESS;
   if (k <= 0 || alpha == 0.0) {
     // C := beta*C only; k == 0 never occurs on the factorization path with
     // beta != 1, so only the trivial case is supported here.
     if (beta == 1.0) return FLA_SUCCESS;
+  }
+  if (ta && !tb && mode == GEMM_FULL && !guard && m <= 64 && n <= 64 && k >= 1024) {
+    // slices of 128 rows, at most two per SM
+    const int sms = ctx().num_sms;
+    long S = std::max<long>(1, std::min<long>(2L * sms, k / 128));
+    const long kc = ((k + S - 1) / S + SK_ROWS - 1) / SK_ROWS * SK_ROWS;
+    S = (k + kc - 1) / kc;
+    double* Pz = (double*)ws_get(st == ctx().side ? WS_SPLITK_SIDE : WS_SPLITK, sizeof(double) * (size_t)(S * m * n));
+    if (!Pz) return FLA_FAILURE;
+    const int ps = prof_begin(st);
+    if (m <= 32 && n <= 32)
+      gemm_tn_small_kernel<2><<<(unsigned)S, 256, 0, st>>>(A, lda, B, ldb, (int)m, (int)n, k, kc, Pz);
+    else
+      gemm_tn_small_kernel<4><<<(unsigned)S, 256, 0, st>>>(A, lda, B, ldb, (int)m, (int)n, k, kc, Pz);
+    count_launch();
+    splitk_reduce_warp_kernel<<<(unsigned)((m * n * 32 + 255) / 256), 256, 0, st>>>(Pz, (int)S, (int)m, (int)n,
+                                                                                   alpha, beta, C, ldc);
+    count_launch();
+    prof_end(ps, st, PROF_GEMM, 2.0 * (double)m * (double)n * (double)k);
+    FB_CK(cudaGetLastError());
+    return FLA_SUCCESS;
   }
   if (!tma_ok(A, lda) || !tma_ok(B, ldb)) {
     dim3 g((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));
@@ -468,14 +558,16 @@ int gemm_f64(cudaStream_t st, bool ta, bool tb, long m, long n, long k, double a
   const int sms = ctx().num_sms;
   long S = 1, kc = 0, ldp = 0, zs = 0;
   double* Pz = nullptr;
-  if (mode == GEMM_FULL && !guard && (tiles * 2 <= sms || narrow) && k >= 2048) {
+  const bool capped = mode == GEMM_FULL && !guard && kmax > 0 && k > kmax;
+  if (mode == GEMM_FULL && !guard && (((tiles * 2 <= sms || narrow) && k >= 2048) || capped)) {
     S = std::min<long>(std::min<long>(((narrow ? 4L : 2L) * sms + tiles - 1) / tiles, k / 512), 64);
+    if (capped) S = std::min<long>(std::max<long>(S, (k + kmax - 1) / kmax), 64);
     if (S > 1) {
       kc = ((k + S - 1) / S + BK - 1) / BK * BK;
       S = (k + kc - 1) / kc;
       ldp = (m + 1) & ~1L;
       zs = ldp * n;
-      Pz = (double*)ws_get(WS_SPLITK, sizeof(double) * (size_t)(S * zs));
+      Pz = (double*)ws_get(st == ctx().side ? WS_SPLITK_SIDE : WS_SPLITK, sizeof(double) * (size_t)(S * zs));
       if (!Pz) return FLA_FAILURE;
       grid.z = (unsigned)S;
     }

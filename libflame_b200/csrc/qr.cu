@@ -31,7 +31,8 @@ namespace fb {
 namespace {
 
 constexpr int QR_THREADS = 256;
-constexpr int QR_NBMAX = 64;
+constexpr int QR_NBMAX = 64;  // widest panel of the cooperative kernel
+constexpr int QR_NB = 128;     // panel width of the blocked factorization (T blocks per panel: 128 / b_alg)
 constexpr size_t QR_SMEM_CAP = 200 * 1024;
 
 struct QrPanelArgs {
@@ -39,7 +40,8 @@ struct QrPanelArgs {
   long ld;
   int M, nb;       // panel rows, columns
   int R, lds, G;   // rows per CTA, SMEM stride, CTAs
-  double* Tbig;    // out: nb x nb (ld nb), upper triangle with diagonal
+  double* Tbig;    // out: nb x nb (ld ldt), upper triangle with diagonal
+  long ldt;
   double* part_ss; // [2][G]      partial ||x2||^2 per CTA
   double* part;    // [2][G][nb]  partial dot products per CTA
   double* rowj;    // [2][nb + 1] row j (and chi1 at [nb])
@@ -152,9 +154,9 @@ __global__ void __launch_bounds__(QR_THREADS) qr_panel_kernel(QrPanelArgs a) {
         if (col > j) {
           sw[col] = (rj + d) * s_rtau;  // w = (a1t + A2^T u2) / tau
         } else if (col < j) {
-          if (c == 0) a.Tbig[col + (long)j * nb] = rj + d;  // t01 = a10t^T + A20^T u21
+          if (c == 0) a.Tbig[col + (long)j * a.ldt] = rj + d;  // t01 = a10t^T + A20^T u21
         } else if (c == 0) {
-          a.Tbig[j + (long)j * nb] = s_tau;
+          a.Tbig[j + (long)j * a.ldt] = s_tau;
         }
       }
     }
@@ -187,16 +189,18 @@ __global__ void form_unit_lower_kernel(const double* __restrict__ P, long ldp, d
   U[row + (long)col * ldu] = v;
 }
 
-// Copy the b_alg x b_alg diagonal blocks of Tbig (nb x nb) into T's columns
-// [k, k+nb) (T is b_alg x n, ld ldt); only the upper triangles.
-__global__ void extract_t_blocks_kernel(const double* __restrict__ Tbig, int nb, int cols, double* T,
+// Copy the b_alg x b_alg diagonal blocks of Tbig (cols x cols, ld ldb)
+// into T's columns [k, k+cols) (T is b_alg x n, ld ldt); only the upper
+// triangles.
+__global__ void extract_t_blocks_kernel(const double* __restrict__ Tbig, long ldb, int cols, double* T,
                                         long ldt, int b_alg) {
   const int j = blockIdx.x;           // panel column
-  const int i = threadIdx.x;          // row within its T block
-  if (j >= cols || i >= b_alg) return;
+  if (j >= cols) return;
   const int blk0 = (j / b_alg) * b_alg;
-  const int r = blk0 + i;             // row of Tbig
-  if (r <= j) T[i + (long)j * ldt] = Tbig[r + (long)j * nb];
+  for (int i = threadIdx.x; i < b_alg; i += blockDim.x) {
+    const int r = blk0 + i;           // row of Tbig
+    if (r <= j) T[i + (long)j * ldt] = Tbig[r + (long)j * ldb];
+  }
 }
 
 // t[j] := T(j mod b_alg, j) (FLA_QR_UT_recover_tau), optionally 1/t[j]
@@ -235,110 +239,193 @@ long even_up(long x) { return (x + 1) & ~1L; }
 
 }  // namespace
 
-// A := QR in place (A m x n); T (b_alg x n, ld ldt) receives the T blocks.
-int qr_ut_dev(DMat A, DMat T, int b_alg) {
+// One M x nb panel (nb <= 64) by the cooperative kernel: two grid barriers
+// per column; for pieces taller than any cluster leaf holds.  Tb (ld ldtb)
+// receives the panel's nb x nb T.
+int qr_coop_panel(double* P, long ld, long M, int nb, double* Tb, long ldtb, cudaStream_t st) {
   set_qr_attrs();
   Context& cx = ctx();
-  cudaStream_t st = cx.stream;
-  const long m = A.m, n = A.n, mn = std::min(m, n);
-  if (mn == 0) return FLA_SUCCESS;
-  const int NBQ = std::max(1, QR_NBMAX / b_alg) * b_alg;
-  QrGeom g0 = qr_geom(m, NBQ);
-  if ((size_t)g0.lds * NBQ * 8 + NBQ * 8 > QR_SMEM_CAP || g0.G > cx.num_sms) {
+  QrGeom g = qr_geom(M, nb);
+  if (nb > QR_NBMAX || (size_t)g.lds * nb * 8 + nb * 8 > QR_SMEM_CAP || g.G > cx.num_sms) {
     set_last_error("FLA_QR_UT: panel too tall for the cooperative panel kernel");
     return FLA_FAILURE;
   }
-  // workspace: panel exchange, Tbig, Uw (m x NBQ), W (NBQ x n)
   const int GMAX = cx.num_sms;
-  size_t b_part = sizeof(double) * (size_t)2 * GMAX * (NBQ + 1);
-  size_t b_rowj = sizeof(double) * 2 * (NBQ + 1);
-  size_t b_tbig = sizeof(double) * NBQ * NBQ;
-  char* ws = (char*)ws_get(WS_PANEL, b_part + b_rowj + b_tbig + 1024);
-  const long ldu = even_up(m);
-  const long ldw = even_up(NBQ);
-  double* Uw = (double*)ws_get(WS_MISC, sizeof(double) * (size_t)ldu * NBQ);
-  double* W = (double*)ws_get(WS_MISC2, sizeof(double) * (size_t)ldw * std::max<long>(n, 1));
-  if (!ws || !Uw || !W) return FLA_FAILURE;
-  double* part = (double*)ws;
-  double* part_ss = part + (size_t)2 * GMAX * NBQ;
-  double* rowj = (double*)(ws + b_part);
-  double* Tbig = (double*)(ws + b_part + b_rowj + 256 - ((b_part + b_rowj) % 256));
-  unsigned* bar = (unsigned*)(cx.d_status + ST_BAR);
-  if (status_reset() != FLA_SUCCESS) return FLA_FAILURE;
+  const size_t b_part = sizeof(double) * (size_t)2 * GMAX * (QR_NBMAX + 1);
+  const size_t b_rowj = sizeof(double) * 2 * (QR_NBMAX + 1);
+  char* ws = (char*)ws_get(WS_PANEL, b_part + b_rowj + 256);
+  if (!ws) return FLA_FAILURE;
+  QrPanelArgs pa;
+  pa.P = P;
+  pa.ld = ld;
+  pa.M = (int)M;
+  pa.nb = nb;
+  pa.R = g.R;
+  pa.lds = g.lds;
+  pa.G = g.G;
+  pa.Tbig = Tb;
+  pa.ldt = ldtb;
+  pa.part = (double*)ws;
+  pa.part_ss = pa.part + (size_t)2 * GMAX * nb;
+  pa.rowj = (double*)(ws + b_part);
+  pa.bar = (unsigned*)(cx.d_status + ST_BAR);
+  pa.err = cx.d_status + ST_ERROR;
+  FB_CK(cudaMemsetAsync(pa.bar, 0, sizeof(unsigned), st));
+  const size_t smem = (size_t)g.lds * nb * 8 + (size_t)nb * 8;
+  void* args[] = {&pa};
+  const int ps = prof_begin(st);
+  FB_CK(cudaLaunchCooperativeKernel((void*)qr_panel_kernel, dim3(g.G), dim3(QR_THREADS), args, smem, st));
+  prof_end(ps, st, PROF_PANEL, 0.0);
+  count_launch();
+  return FLA_SUCCESS;
+}
 
+// qr_panel.cu
+int qr_panel_factor(double* P, long ld, long M, int w, double* Tb, long ldtb, double* U, long ldu, double* Wk,
+                    long ldw, cudaStream_t st);
+int unit_lower_copy(const double* P, long ldp, double* U, long ldu, long M, int b, cudaStream_t st);
+
+namespace {
+
+// B := (I - U T^-T U^T) B, U the M x b unit lower trapezoid (explicit,
+// ld ldu), B M x nc, with Ti = T^-1 (ld ldti) precomputed: W := U^T B,
+// W2 := Ti^T W, B -= U W2 (W and W2 b x nc, ld ldw, scratch).  The
+// explicit inverse turns the b-step triangular solve into a GEMM.  The
+// k = M product is split into slices of at most 1024 rows so that its
+// tiles leave SMs often enough for the cluster leaves of the next panel.
+int apply_block_qt(const double* U, long ldu, const double* Ti, long ldti, long M, int b, double* B, long ldb,
+                   long nc, double* W, double* W2, long ldw, cudaStream_t st) {
+  if (nc <= 0) return FLA_SUCCESS;
+  if (gemm_f64(st, true, false, b, nc, M, 1.0, U, ldu, B, ldb, 0.0, W, ldw, GEMM_FULL, 0, nullptr, 0x7fffffff,
+               1024) != FLA_SUCCESS)
+    return FLA_FAILURE;
+  if (gemm_f64(st, true, false, b, nc, b, 1.0, Ti, ldti, W, ldw, 0.0, W2, ldw) != FLA_SUCCESS) return FLA_FAILURE;
+  return gemm_f64(st, false, false, M, nc, b, -1.0, U, ldu, W2, ldw, 1.0, B, ldb);
+}
+
+}  // namespace
+
+// A := QR in place (A m x n); T (b_alg x n, ld ldt) receives the T blocks.
+// Panels of NBQ = (128 / b_alg) b_alg columns (recursive cluster panels,
+// qr_panel.cu) on the side stream, one panel ahead: after panel k, the
+// main stream first updates panel k+1's columns, then the side stream
+// factors panel k+1 while the main stream updates the remaining columns
+// with the UT transform of panel k (two GEMMs and a triangular solve with
+// its T).
+int qr_ut_dev(DMat A, DMat T, int b_alg) {
+  set_qr_attrs();
+  Context& cx = ctx();
+  cudaStream_t st = cx.stream, sd = cx.side;
+  const long m = A.m, n = A.n, mn = std::min(m, n);
+  if (mn == 0) return FLA_SUCCESS;
+  const int NBQ = std::max(1, QR_NB / b_alg) * b_alg;
+  const long ldu = even_up(m), ldtb = even_up(NBQ), ldw = even_up(NBQ);
+  double* Tb2 = (double*)ws_get(WS_QR_T, sizeof(double) * 4 * (size_t)ldtb * NBQ);  // T, T^-1 of two panels
+  double* Wt = (double*)ws_get(WS_MISC2, sizeof(double) * 2 * (size_t)ldw * std::max<long>(n, 1));
+  double* Up2 = (double*)ws_get(WS_QR_U, sizeof(double) * 2 * (size_t)ldu * NBQ);  // U of two panels
+  double* Wp = (double*)ws_get(WS_QR_W, sizeof(double) * 3 * (size_t)ldw * NBQ);
+  if (!Tb2 || !Wt || !Up2 || !Wp) return FLA_FAILURE;
+  double* Wt2 = Wt + (size_t)ldw * std::max<long>(n, 1);
+  if (status_reset() != FLA_SUCCESS) return FLA_FAILURE;
+  cudaEvent_t ev_look = cx.ev[0], ev_panel = cx.ev[1];
+  auto a_at = [&](long i, long j) { return A.p + i + j * A.ld; };
+  auto tb = [&](long k) { return Tb2 + (size_t)((k / NBQ) & 1) * ldtb * NBQ; };
+  auto ti = [&](long k) { return Tb2 + (size_t)(2 + ((k / NBQ) & 1)) * ldtb * NBQ; };
+  auto up = [&](long k) { return Up2 + (size_t)((k / NBQ) & 1) * ldu * NBQ; };
+  auto panel = [&](long k, int b, cudaStream_t s) -> int {
+    if (qr_panel_factor(a_at(k, k), A.ld, m - k, b, tb(k), ldtb, up(k), ldu, Wp, ldw, s) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    extract_t_blocks_kernel<<<b, std::min(std::max(32, b_alg), 1024), 0, s>>>(tb(k), ldtb, b, T.p + k * T.ld,
+                                                                            T.ld, b_alg);
+    count_launch();
+    if (k + b >= n) return FLA_SUCCESS;  // no trailing columns: T^-1 unused
+    return tri_inverse(tb(k), ldtb, b, false, false, ti(k), ldtb, s);
+  };
+  if (panel(0, (int)std::min<long>(NBQ, mn), st) != FLA_SUCCESS) return FLA_FAILURE;
   for (long k = 0; k < mn; k += NBQ) {
     const int b = (int)std::min<long>(NBQ, mn - k);
-    const long M = m - k;
-    QrGeom g = qr_geom(M, NBQ);
-    QrPanelArgs pa;
-    pa.P = A.p + k + k * A.ld;
-    pa.ld = A.ld;
-    pa.M = (int)M;
-    pa.nb = b;
-    pa.R = g.R;
-    pa.lds = g.lds;
-    pa.G = g.G;
-    pa.Tbig = Tbig;
-    pa.part = part;
-    pa.part_ss = part_ss;
-    pa.rowj = rowj;
-    pa.bar = bar;
-    pa.err = cx.d_status + ST_ERROR;
-    FB_CK(cudaMemsetAsync(bar, 0, sizeof(unsigned), st));
-    const size_t smem = (size_t)g.lds * b * 8 + (size_t)b * 8;
-    void* args[] = {&pa};
-    const int ps = prof_begin(st);
-    FB_CK(cudaLaunchCooperativeKernel((void*)qr_panel_kernel, dim3(g.G), dim3(QR_THREADS), args, smem, st));
-    prof_end(ps, st, PROF_PANEL, 0.0);
-    count_launch();
-    extract_t_blocks_kernel<<<b, std::max(32, b_alg), 0, st>>>(Tbig, b, b, T.p + k * T.ld, T.ld, b_alg);
-    count_launch();
-    const long n2 = n - k - b;
-    if (n2 <= 0) continue;
-    // B := (I - U Tbig^-T U^T) B for B = A(k:m, k+b:n)
-    const unsigned nthr = 256;
-    form_unit_lower_kernel<<<(unsigned)((M * b + nthr - 1) / nthr), nthr, 0, st>>>(pa.P, A.ld, Uw, ldu,
-                                                                                   (int)M, b);
-    count_launch();
-    double* B = A.p + k + (k + b) * A.ld;
-    if (gemm_f64(st, true, false, b, n2, M, 1.0, Uw, ldu, B, A.ld, 0.0, W, ldw) != FLA_SUCCESS)
+    const long M = m - k, n2 = n - k - b;
+    if (n2 <= 0) break;
+    double* Uk = up(k);
+    const int nb2 = (int)std::min<long>(NBQ, mn - k - b);  // next panel's width (0: none)
+    if (nb2 > 0) {
+      if (apply_block_qt(Uk, ldu, ti(k), ldtb, M, b, a_at(k, k + b), A.ld, nb2, Wt, Wt2, ldw, st) != FLA_SUCCESS)
+        return FLA_FAILURE;
+      FB_CK(cudaEventRecord(ev_look, st));
+      FB_CK(cudaStreamWaitEvent(sd, ev_look, 0));
+      if (panel(k + b, nb2, sd) != FLA_SUCCESS) return FLA_FAILURE;
+      FB_CK(cudaEventRecord(ev_panel, sd));
+    }
+    if (apply_block_qt(Uk, ldu, ti(k), ldtb, M, b, a_at(k, k + b + nb2), A.ld, n2 - nb2, Wt, Wt2, ldw, st) !=
+        FLA_SUCCESS)
       return FLA_FAILURE;
-    if (trsm_block(Tbig, b, W, ldw, b, n2, false, true, false, st) != FLA_SUCCESS) return FLA_FAILURE;
-    if (gemm_f64(st, false, false, M, n2, b, -1.0, Uw, ldu, W, ldw, 1.0, B, A.ld) != FLA_SUCCESS)
-      return FLA_FAILURE;
+    if (nb2 > 0) FB_CK(cudaStreamWaitEvent(st, ev_panel, 0));
   }
   int info;
   return status_read(&info);
 }
 
+namespace {
+
+// The s x s triangular factor of a super-block of s / b_alg consecutive
+// UT blocks: the stored b_alg x b_alg T blocks on the diagonal, the Gram
+// blocks U_i^T U_j of G (ld ldg) above them; below the diagonal is unused.
+__global__ void assemble_t_kernel(const double* __restrict__ T, long ldt, int b_alg, const double* __restrict__ G,
+                                  long ldg, int s, double* __restrict__ Ts, long ldts) {
+  const int j = blockIdx.x;
+  for (int i = threadIdx.x; i <= j && i < s; i += blockDim.x) {
+    const bool diag_blk = (i / b_alg) == (j / b_alg);
+    Ts[i + (long)j * ldts] = diag_blk ? T[(i % b_alg) + (long)j * ldt] : G[i + (long)j * ldg];
+  }
+}
+
+}  // namespace
+
 // B := Q^T B (transpose_q) or Q B for Q = H(0) H(1) ... from the UT
-// representation in U (m x k, below the diagonal) and T (b_alg x k).
+// representation in U (m x k, below the diagonal) and T (b_alg x k), the
+// blocks of FLA_Apply_Q_UT_lhfc/lhfc var1
+// (src/lapack/util/app/qut/lhfc/flamec/FLA_Apply_Q_UT_lhfc_blk_var1.c:
+// 148-182), grouped into super-blocks of S = (128 / b_alg) b_alg columns:
+// one GEMM U^T [U | B] gives both the Gram blocks that complete the
+// super-block's triangular factor (its diagonal blocks are the stored T
+// blocks) and W = U^T B; then W2 := Ts^-T W (Q^T) or Ts^-1 W (Q), through
+// the explicit inverse of Ts, and B -= U W2.  The product of the super-block's UT transforms is the single
+// UT transform with that factor, so the result is the block-by-block one up
+// to rounding.
 int apply_q_dev(DMat U, DMat T, int b_alg, DMat B, bool transpose_q) {
   Context& cx = ctx();
   cudaStream_t st = cx.stream;
   const long m = U.m, k = std::min(U.m, U.n), nr = B.n;
   if (k == 0 || nr == 0) return FLA_SUCCESS;
-  const long ldu = even_up(m), ldw = even_up(b_alg);
-  double* Uw = (double*)ws_get(WS_MISC, sizeof(double) * (size_t)ldu * b_alg);
-  double* W = (double*)ws_get(WS_MISC2, sizeof(double) * (size_t)ldw * nr);
-  if (!Uw || !W) return FLA_FAILURE;
+  const int S = std::max(1, QR_NB / b_alg) * b_alg;
+  const long ldy = even_up(m), ldg = even_up(S);
+  double* Y = (double*)ws_get(WS_QR_U, sizeof(double) * (size_t)ldy * (size_t)(S + nr));  // [U | B]
+  // [Gram | W], Ts, Ts^-1, W2
+  double* G = (double*)ws_get(WS_QR_W, sizeof(double) * (size_t)ldg * (size_t)(3 * S + 2 * nr));
+  if (!Y || !G) return FLA_FAILURE;
+  double* Ts = G + (size_t)ldg * (S + nr);
+  double* Tsi = Ts + (size_t)ldg * S;
+  double* W2 = Tsi + (size_t)ldg * S;
   op_begin(st);
-  const long nblk = (k + b_alg - 1) / b_alg;
-  for (long bi = 0; bi < nblk; ++bi) {
-    const long jb = transpose_q ? bi * b_alg : (nblk - 1 - bi) * b_alg;
-    const int b = (int)std::min<long>(b_alg, k - jb);
+  const long nsb = (k + S - 1) / S;
+  for (long bi = 0; bi < nsb; ++bi) {
+    const long jb = transpose_q ? bi * S : (nsb - 1 - bi) * S;
+    const int s = (int)std::min<long>(S, k - jb);
     const long M = m - jb;
-    const unsigned nthr = 256;
-    form_unit_lower_kernel<<<(unsigned)((M * b + nthr - 1) / nthr), nthr, 0, st>>>(
-        U.p + jb + jb * U.ld, U.ld, Uw, ldu, (int)M, b);
-    count_launch();
     double* Bj = B.p + jb;
-    if (gemm_f64(st, true, false, b, nr, M, 1.0, Uw, ldu, Bj, B.ld, 0.0, W, ldw) != FLA_SUCCESS)
+    if (unit_lower_copy(U.p + jb + jb * U.ld, U.ld, Y, ldy, M, s, st) != FLA_SUCCESS) return FLA_FAILURE;
+    FB_CK(cudaMemcpy2DAsync(Y + (size_t)ldy * s, sizeof(double) * ldy, Bj, sizeof(double) * B.ld,
+                            sizeof(double) * M, nr, cudaMemcpyDeviceToDevice, st));
+    if (gemm_f64(st, true, false, s, s + nr, M, 1.0, Y, ldy, Y, ldy, 0.0, G, ldg) != FLA_SUCCESS)
       return FLA_FAILURE;
-    // W := T^-T W (Q^T) or T^-1 W (Q); T block upper triangular
-    if (trsm_block(T.p + jb * T.ld, T.ld, W, ldw, b, nr, false, transpose_q, false, st) != FLA_SUCCESS)
+    assemble_t_kernel<<<s, 128, 0, st>>>(T.p + jb * T.ld, T.ld, b_alg, G, ldg, s, Ts, ldg);
+    count_launch();
+    // W2 := Ts^-T W (Q^T) or Ts^-1 W (Q), through the explicit inverse
+    double* W = G + (size_t)ldg * s;
+    if (tri_inverse(Ts, ldg, s, false, false, Tsi, ldg, st) != FLA_SUCCESS) return FLA_FAILURE;
+    if (gemm_f64(st, transpose_q, false, s, nr, s, 1.0, Tsi, ldg, W, ldg, 0.0, W2, ldg) != FLA_SUCCESS)
       return FLA_FAILURE;
-    if (gemm_f64(st, false, false, M, nr, b, -1.0, Uw, ldu, W, ldw, 1.0, Bj, B.ld) != FLA_SUCCESS)
+    if (gemm_f64(st, false, false, M, nr, s, -1.0, Y, ldy, W2, ldg, 1.0, Bj, B.ld) != FLA_SUCCESS)
       return FLA_FAILURE;
   }
   op_end(st);

@@ -49,6 +49,37 @@ def test_qr_ut_matches_oracle(cuda, flame, oracle, m, n):
     assert be <= be_o + 1.0, (be, be_o)
 
 
+# Tall panels and other T block sizes: 16-CTA cluster leaves of width 32
+# (8000 rows), 16 (9000, 20000 rows) and 8, pieces beyond any cluster
+# (40000 rows: the cooperative panel kernel), the recursive panel's T
+# assembly, panels of 96 (b = 48) and 200 (b = 200) columns.
+@pytest.mark.parametrize("m,n,b", [(8000, 96, 32), (9000, 64, 32), (20000, 40, 32), (40000, 24, 8),
+                                   (3000, 200, 48), (600, 300, 200), (700, 520, 16)])
+def test_qr_ut_tall_and_block_sizes(cuda, flame, oracle, m, n, b):
+    rng = seeded(m * 17 + n + b)
+    A = rng.standard_normal((m, n))
+    Ad = to_dev(cuda, A)
+    Td = to_dev(cuda, np.zeros((b, n)))
+    assert flame.qr_ut(Ad, Td) == flame.FLA_SUCCESS, flame.last_error()
+    QR, T = to_host(Ad), to_host(Td)
+    QRo, To = oracle.qr_ut(A, b)
+    assert rel_fro(QR, QRo) < TOL
+    mask = t_mask(To, min(m, n))
+    assert rel_fro(T[mask], To[mask]) < TOL
+    be, be_o = _be_tall(oracle, A, QR, T), _be_tall(oracle, A, QRo, To)
+    assert be <= be_o + 1.0, (be, be_o)
+
+
+def _be_tall(oracle, A, QR, T):
+    """||Q^T A - [R; 0]||_F / (max(m,n) eps ||A||_F), equal to ||A - QR|| for
+    an orthogonal Q, without forming the m x m Q."""
+    m, n = A.shape
+    k = min(m, n)
+    R = np.zeros((m, n))
+    R[:k] = np.triu(QR[:k, :])
+    return np.linalg.norm(oracle.apply_qt(QR, T, A) - R) / (max(m, n) * np.finfo(float).eps * np.linalg.norm(A))
+
+
 def test_qr_golden(cuda, flame, golden):
     for key in ["40x40", "130x64", "160x80"]:
         A = golden["qr_%s_A" % key]
