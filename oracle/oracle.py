@@ -102,6 +102,57 @@ def lu_piv_solve(LU, p, B):
     return b
 
 
+def _trsm_lut(U, B):
+    """B := inv(U^T) B, U upper non-unit: netlib dtrsm Left/Upper/Transpose,
+    rows in ascending order (each row's dot product vectorized)."""
+    b = np.array(B, dtype=np.float64, order="F", copy=True)
+    for i in range(b.shape[0]):
+        b[i] = (b[i] - U[:i, i] @ b[:i]) / U[i, i]
+    return b
+
+
+def _trsm_lltu(L, B):
+    """B := inv(L^T) B, L unit lower: netlib dtrsm Left/Lower/Transpose/Unit,
+    rows in descending order."""
+    b = np.array(B, dtype=np.float64, order="F", copy=True)
+    for i in range(b.shape[0] - 1, -1, -1):
+        b[i] = b[i] - L[i + 1:, i] @ b[i + 1:]
+    return b
+
+
+def _trsm_lun(U, B):
+    """B := inv(U) B, U upper non-unit: dtrsm Left/Upper/No transpose, rows
+    descending."""
+    b = np.array(B, dtype=np.float64, order="F", copy=True)
+    for i in range(b.shape[0] - 1, -1, -1):
+        b[i] = (b[i] - U[i, i + 1:] @ b[i + 1:]) / U[i, i]
+    return b
+
+
+def lu_piv_solve_t(LU, p, B):
+    """A^T X = B from FLA_LU_piv's factor (relative pivots p): the TRANS = 'T'
+    branch of dgetrs (src/map/common/lapacksrc/f2c/dgetrs.c:201-205): X :=
+    inv(U^T) B, X := inv(L^T) X (unit), then the interchanges in reverse
+    order (dlaswp with incx = -1).  NumPy restatement for small cases."""
+    b = np.array(B, dtype=np.float64, order="F", copy=True)
+    if b.ndim == 1:
+        b = b.reshape(-1, 1, order="F")
+    lu = np.asarray(LU, dtype=np.float64)
+    b = _trsm_lltu(lu, _trsm_lut(lu, b))
+    return apply_pivots(p, b, transpose=True)
+
+
+def chol_solve_u(Ufac, B):
+    """X := inv(A) B with A = U^T U (upper factor), FLA_Chol_solve's upper
+    branch (src/lapack/dec/chol/front/flamec/FLA_Chol_solve.c:29-34): X :=
+    inv(U^T) B, then X := inv(U) X.  NumPy restatement for small cases."""
+    b = np.array(B, dtype=np.float64, order="F", copy=True)
+    if b.ndim == 1:
+        b = b.reshape(-1, 1, order="F")
+    u = np.asarray(Ufac, dtype=np.float64)
+    return _trsm_lun(u, _trsm_lut(u, b))
+
+
 def apply_pivots(p, A, transpose=False):
     a = _f(A)
     if a.ndim == 1:

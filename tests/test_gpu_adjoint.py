@@ -117,3 +117,71 @@ def test_gp_gradient_matches_oracle_and_fd(cuda, flame, oracle):
         fd = (loss_of(K + h * E) - loss_of(K - h * E)) / (2 * h)
         an = np.sum(G * E)
         assert abs(fd - an) <= 1e-5 * max(1.0, abs(an)), (i, j, fd, an)
+
+
+def _colmajor(t):
+    """A column-major copy of a 2-D tensor (stride(1) = rows, also for one column)."""
+    import torch
+    out = torch.empty_strided(tuple(t.shape), (1, t.shape[0]), dtype=t.dtype, device=t.device)
+    out.copy_(t)
+    return out
+
+
+def test_gp_gradient_n8192_sampled_oracle_and_fd(cuda, flame, oracle):
+    """The GP gradient at n = 8192 (one GP of the batched-GP workload): the
+    adjoint chain's dloss/dK against 0.5 (K^-1 - alpha alpha^T) on 200
+    sampled entries, with the needed columns of K^-1 and alpha from the
+    oracle's triangular solves on the factor (CPU), and against central
+    differences of the loss on the same 200 entries, each loss evaluated by
+    FLA_Chol on the GPU."""
+    torch = cuda
+    # nugget 0.1: the central differences of the loss (h = 1e-5) stay clear
+    # of its rounding noise at this size (with 1e-2 and h = 1e-6 the noise
+    # reaches 1e-5 relative)
+    n, h = 8192, 1e-5
+    g = torch.Generator(device="cuda").manual_seed(8192)
+    x = torch.rand((n, 3), dtype=torch.float64, device="cuda", generator=g)
+    K = torch.exp(-torch.cdist(x, x) ** 2 / (2 * 0.3 ** 2)) + 0.1 * torch.eye(n, dtype=torch.float64, device="cuda")
+    K = _colmajor(0.5 * (K + K.t()))
+    y = torch.randn((n, 1), dtype=torch.float64, device="cuda", generator=g)
+    Ld = _colmajor(K)
+    assert flame.chol(Ld) == flame.FLA_SUCCESS, flame.last_error()
+    Lt = _colmajor(torch.tril(Ld))
+    v = torch.linalg.solve_triangular(Lt, y, upper=False)
+    Lbar = _colmajor(torch.zeros((n, n), dtype=torch.float64, device="cuda"))
+    Vd, Vb = _colmajor(v), _colmajor(v)
+    assert flame.trsm_llnn_adjoint(Lt, Vd, Vb, Lbar) == flame.FLA_SUCCESS, flame.last_error()
+    r, logdet = flame.chol_logdet_adjoint(Lt, Lbar, 1.0)
+    assert r == flame.FLA_SUCCESS
+    assert flame.chol_adjoint(Lt, Lbar) == flame.FLA_SUCCESS, flame.last_error()
+    Ab = torch.tril(Lbar)
+    Gh = (0.5 * (Ab + Ab.t())).cpu().numpy()
+    del Ab, Lbar, Vd, Vb, Ld
+    rng = seeded(8192)
+    idx = rng.integers(0, n, size=(200, 2))
+    # oracle: the needed columns of K^-1 and alpha = K^-1 y from the factor
+    L = np.asfortranarray(Lt.cpu().numpy())
+    cols = np.unique(idx[:, 1])
+    E = np.zeros((n, cols.size + 1), order="F")
+    E[cols, np.arange(cols.size)] = 1.0
+    E[:, -1] = y.cpu().numpy()[:, 0]
+    Z = oracle.chol_solve(L, E)
+    Kinv_cols, alpha = Z[:, :-1], Z[:, -1]
+    where = {c: k for k, c in enumerate(cols)}
+    for i, j in idx:
+        ref = 0.5 * (Kinv_cols[i, where[j]] - alpha[i] * alpha[j])
+        assert abs(Gh[i, j] - ref) <= 1e-9 * max(1.0, abs(ref)), (i, j, Gh[i, j], ref)
+
+    def loss_of(i, j, d):
+        M = K.clone()
+        M[i, j] += d
+        if i != j:
+            M[j, i] += d
+        assert flame.chol(M) == flame.FLA_SUCCESS
+        Lm = torch.tril(M)
+        vv = torch.linalg.solve_triangular(Lm, y, upper=False)
+        return 0.5 * float((vv * vv).sum()) + float(torch.log(torch.diagonal(Lm)).sum())
+    for i, j in idx:
+        fd = (loss_of(i, j, h) - loss_of(i, j, -h)) / (2 * h)
+        an = float(Gh[i, j]) * (1 if i == j else 2)
+        assert abs(fd - an) <= 1e-5 * max(1.0, abs(an)), (i, j, fd, an)

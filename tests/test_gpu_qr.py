@@ -127,3 +127,32 @@ def test_recover_tau_and_dgeqrf(cuda, flame, golden, oracle):
     assert info.value == 0
     assert rel_fro(a, golden["dgeqrf_QR"]) < TOL
     assert rel_fro(tau, golden["dgeqrf_tau"]) < TOL
+
+
+def test_create_t_and_workspace_objects(cuda, flame, oracle):
+    """FLA_QR_UT_create_T and FLA_Apply_Q_UT_create_workspace through the
+    C-ABI: the objects they allocate (in HBM) have the reference's shapes
+    (T: min(32, min_dim) x width(A); W: length(T) x max_dim(B), as
+    FLA_Apply_Q_UT_create_workspace.c:19-22) and drive
+    FLA_QR_UT and FLA_Apply_Q_UT to the oracle's results; FLA_Obj_free
+    releases them."""
+    L = flame.lib()
+    rng = seeded(53)
+    m, n, nrhs = 300, 180, 5
+    A = rng.standard_normal((m, n))
+    B = rng.standard_normal((m, nrhs))
+    Ad, Bd = to_dev(cuda, A), to_dev(cuda, B)
+    va, vb = flame.View(Ad), flame.View(Bd)
+    T, W = flame.FLA_Obj(), flame.FLA_Obj()
+    assert L.FLA_QR_UT_create_T(va.obj, C.byref(T)) == flame.FLA_SUCCESS
+    assert (L.FLA_Obj_length(T), L.FLA_Obj_width(T)) == (32, n)
+    assert L.FLA_QR_UT(va.obj, T) == flame.FLA_SUCCESS, flame.last_error()
+    assert L.FLA_Apply_Q_UT_create_workspace(T, vb.obj, C.byref(W)) == flame.FLA_SUCCESS
+    assert (L.FLA_Obj_length(W), L.FLA_Obj_width(W)) == (32, max(m, nrhs))
+    assert L.FLA_Apply_Q_UT(flame.FLA_LEFT, flame.FLA_CONJ_TRANSPOSE, flame.FLA_FORWARD, flame.FLA_COLUMNWISE,
+                            va.obj, T, W, vb.obj) == flame.FLA_SUCCESS, flame.last_error()
+    QRo, To = oracle.qr_ut(A)
+    assert rel_fro(to_host(Ad), QRo) < TOL
+    assert rel_fro(to_host(Bd), oracle.apply_qt(QRo, To, B)) < TOL
+    assert L.FLA_Obj_free(C.byref(T)) == flame.FLA_SUCCESS
+    assert L.FLA_Obj_free(C.byref(W)) == flame.FLA_SUCCESS

@@ -98,3 +98,52 @@ def test_dgetrs_transpose_and_device_pointers(cuda, flame, oracle):
     L.dgetrs_(C.c_char_p(b"N"), _ip(n), _ip(nrhs), C.c_void_p(Ad.data_ptr()), _ip(n),
               C.c_void_p(ipiv.data_ptr()), C.c_void_p(Bd.data_ptr()), _ip(n), C.byref(info))
     assert rel_fro(A @ to_host(Bd), B) < 1e-11
+
+
+def test_dgetrs_transpose_matches_oracle(cuda, flame, oracle):
+    """dgetrs_ 'T' against the oracle's restatement of dgetrs' transposed
+    branch on the oracle's own factor (identical pivots)."""
+    torch = cuda
+    L = flame.lib()
+    rng = seeded(37)
+    n, nrhs = 260, 6
+    A = rng.uniform(-1, 1, (n, n))
+    B = rng.standard_normal((n, nrhs))
+    Ad = to_dev(cuda, A)
+    ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    info = C.c_int(9)
+    L.dgetrf_(_ip(n), _ip(n), C.c_void_p(Ad.data_ptr()), _ip(n), C.c_void_p(ipiv.data_ptr()), C.byref(info))
+    assert info.value == 0
+    LUo, po, ro = oracle.lu_piv(A)
+    assert np.array_equal(ipiv.cpu().numpy() - 1 - np.arange(n), po)
+    Bd = to_dev(cuda, B)
+    L.dgetrs_(C.c_char_p(b"T"), _ip(n), _ip(nrhs), C.c_void_p(Ad.data_ptr()), _ip(n),
+              C.c_void_p(ipiv.data_ptr()), C.c_void_p(Bd.data_ptr()), _ip(n), C.byref(info))
+    assert info.value == 0
+    Xo = oracle.lu_piv_solve_t(LUo, po, B)
+    assert rel_fro(to_host(Bd), Xo) < TOL
+    assert rel_fro(A.T @ Xo, B) < 1e-11  # the restatement itself solves A^T X = B
+
+
+def test_dposv_upper_matches_oracle(cuda, flame, oracle):
+    """dposv_ 'U' on host buffers: the upper factor against the transpose of
+    the oracle's lower factor (U = L^T for the same A), and X against the
+    oracle's upper Cholesky solve."""
+    L = flame.lib()
+    rng = seeded(41)
+    n, nrhs = 230, 4
+    A = spd(rng, n)
+    B = rng.standard_normal((n, nrhs))
+    a = np.asfortranarray(A.copy())
+    b = np.asfortranarray(B.copy())
+    info = C.c_int(9)
+    L.dposv_(C.c_char_p(b"U"), _ip(n), _ip(nrhs), a.ctypes.data_as(C.c_void_p), _ip(n),
+             b.ctypes.data_as(C.c_void_p), _ip(n), C.byref(info))
+    assert info.value == 0
+    Lo, ro = oracle.chol(A)
+    Uo = np.triu(Lo.T)
+    assert rel_fro(np.triu(a), Uo) < TOL
+    assert np.array_equal(np.tril(a, -1), np.tril(A, -1))  # the strictly lower part is not referenced
+    Xo = oracle.chol_solve_u(Uo, B)
+    assert rel_fro(b, Xo) < TOL
+    assert rel_fro(A @ Xo, B) < 1e-11

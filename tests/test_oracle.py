@@ -104,3 +104,19 @@ def test_oracle_against_live_reference(oracle, seed):
     q1, t1 = oracle.qr_ut(A)
     q2, t2, _ = R.qr_ut(A)
     assert np.array_equal(q1, q2)
+
+
+def test_transposed_and_upper_solves_solve_their_systems(oracle):
+    """The oracle's dgetrs 'T' and upper FLA_Chol_solve restatements (used as
+    the GPU checkers) solve A^T X = B and A X = B on small systems."""
+    rng = np.random.default_rng(7)
+    n = 40
+    A = rng.uniform(-1, 1, (n, n))
+    B = rng.standard_normal((n, 3))
+    LU, p, r = oracle.lu_piv(A)
+    X = oracle.lu_piv_solve_t(LU, p, B)
+    assert np.linalg.norm(A.T @ X - B) / np.linalg.norm(B) < 1e-12
+    S = A @ A.T + n * np.eye(n)
+    Lf, r = oracle.chol(S)
+    X = oracle.chol_solve_u(np.triu(Lf.T), B)
+    assert np.linalg.norm(S @ X - B) / np.linalg.norm(B) < 1e-12
