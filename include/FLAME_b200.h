@@ -105,7 +105,8 @@ int           FLA_B200_lp_gemm( int prec, long m, long n, long k, float alpha, c
 
 /* ---- Batched factorizations (no counterpart in the reference) ----
  * `count` independent matrices A[i] (device pointers, column-major, order
- * n[i] <= 512, leading dimension lda[i]; the arrays n, A, lda, piv, B, ldb
+ * n[i] <= 512 -- <= 1024 for the FP64 Cholesky, whose updates run on the
+ * FP64 tensor cores --, leading dimension lda[i]; the arrays n, A, lda, piv, B, ldb
  * and info are host arrays) in one persistent launch, largest first.  Each
  * matrix gets the single-matrix semantics: info[i] = FLA_SUCCESS, or the
  * zero-based failing column (Cholesky) / first zero-pivot column (LU).
@@ -121,6 +122,12 @@ FLA_Error     FLA_B200_Chol_batched_f32( int count, const int* n, float** A, con
                                          float** B, const int* ldb, int* info );
 FLA_Error     FLA_B200_LU_piv_batched_f32( int count, const int* n, float** A, const int* lda, int** piv,
                                            int nrhs, float** B, const int* ldb, int* info );
+/* FLA_Chol_batched (lower, FP64; orders up to 1024) that also returns
+ * logdet[i] = sum_j log L_i(j, j) (host array of count doubles, NaN where
+ * the factorization failed): the forward pass of a batch of Gaussian-process
+ * likelihoods (with nrhs = 1, B[i] := K_i^-1 y_i). */
+FLA_Error     FLA_B200_Chol_batched_logdet( int count, const int* n, double** A, const int* lda, int nrhs,
+                                            double** B, const int* ldb, double* logdet, int* info );
 /* Autotuner of the batched kernels: per size bin (orders 1-32, 33-64,
  * 65-128, 129-256, 257-512) times the panel widths 8, 16, 24, 32 on
  * `samples` scratch matrices and keeps the fastest for later calls on this
@@ -137,6 +144,12 @@ int           FLA_B200_batched_nb( int lu, int f64, int n );
  * the adjoint of the lower entries of A (the gradient with respect to a
  * symmetric A is (Abar + Abar^T)/2).  Only FLA_LOWER_TRIANGULAR. */
 FLA_Error     FLA_Chol_adjoint( FLA_Uplo uplo, FLA_Obj L, FLA_Obj Lbar );
+/* FLA_Chol_adjoint over a batch (device pointers, host arrays n, ld, L,
+ * Lbar; L[i] and Lbar[i] share the leading dimension ld[i]): Lbar[i](j,j)
+ * += logdet_scale / L[i](j,j) first (0 skips it), then Lbar[i] := Abar[i]
+ * in its lower triangle.  The backward pass of a batch of GP likelihoods. */
+FLA_Error     FLA_Chol_adjoint_batched( int count, const int* n, double** L, const int* ld, double** Lbar,
+                                        double logdet_scale );
 /* Lbar += scale * diag(1/L(i,i)): the adjoint of scale * sum_i log L(i,i)
  * (log det A = 2 sum_i log L(i,i)); logdet (optional) receives the sum. */
 FLA_Error     FLA_B200_Chol_logdet_adjoint( FLA_Obj L, FLA_Obj Lbar, double scale, double* logdet );

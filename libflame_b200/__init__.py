@@ -97,6 +97,9 @@ _SIGS = {
                                             C.c_void_p, C.c_void_p]),
     "FLA_B200_LU_piv_batched_f32": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                               C.c_void_p, C.c_void_p, C.c_void_p]),
+    "FLA_B200_Chol_batched_logdet": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                               C.c_void_p, C.c_void_p, C.c_void_p]),
+    "FLA_Chol_adjoint_batched": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]),
     "FLA_B200_batched_tune": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "FLA_B200_batched_nb": (C.c_int, [C.c_int, C.c_int, C.c_int]),
     "FLA_Chol_adjoint": (C.c_int, [C.c_int, FLA_Obj, FLA_Obj]),
@@ -320,6 +323,35 @@ def batched(kind, mats, pivs=None, rhs=None, f32=False):
         else:
             r = L.FLA_LU_piv_batched(cnt, P(n), A, P(lda), pv, nrhs, B, P(ldb), P(info))
     return r, info.tolist()
+
+
+def chol_batched_logdet(mats, rhs=None):
+    """FLA_B200_Chol_batched_logdet on column-major CUDA tensors: lower
+    Cholesky of every matrix in place (+ solves of rhs), per-matrix
+    log-determinants.  Returns (error code, info list, logdet list)."""
+    import numpy as _np
+    cnt = len(mats)
+    n = _np.array([m.shape[0] for m in mats], dtype=_np.int32)
+    lda = _np.array([max(1, m.stride(1)) for m in mats], dtype=_np.int32)
+    nrhs = 0 if rhs is None else rhs[0].shape[1]
+    B = _ptr_array(rhs) if rhs is not None else None
+    ldb = _np.array([max(1, b.stride(1)) for b in rhs], dtype=_np.int32) if rhs is not None else None
+    info = _np.zeros(cnt, dtype=_np.int32)
+    logdet = _np.zeros(cnt, dtype=_np.float64)
+    P = (lambda a: a.ctypes.data_as(C.c_void_p) if a is not None else None)
+    r = lib().FLA_B200_Chol_batched_logdet(cnt, P(n), _ptr_array(mats), P(lda), nrhs, B, P(ldb), P(logdet), P(info))
+    return r, info.tolist(), logdet.tolist()
+
+
+def chol_adjoint_batched(Ls, Lbars, logdet_scale=0.0):
+    """FLA_Chol_adjoint_batched over lists of column-major CUDA tensors (each
+    L[i] and Lbar[i] with the same leading dimension)."""
+    import numpy as _np
+    n = _np.array([m.shape[0] for m in Ls], dtype=_np.int32)
+    ld = _np.array([max(1, m.stride(1)) for m in Ls], dtype=_np.int32)
+    assert all(max(1, b.stride(1)) == l for b, l in zip(Lbars, ld))
+    P = (lambda a: a.ctypes.data_as(C.c_void_p))
+    return lib().FLA_Chol_adjoint_batched(len(Ls), P(n), _ptr_array(Ls), P(ld), _ptr_array(Lbars), logdet_scale)
 
 
 def chol_adjoint(L, Lbar):

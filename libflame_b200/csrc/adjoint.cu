@@ -28,6 +28,8 @@
 #include <climits>
 #include <cmath>
 
+#include <string>
+
 #include "common.h"
 
 namespace fb {
@@ -298,6 +300,35 @@ FLA_Error FLA_B200_Trsm_llnn_adjoint(FLA_Obj L, FLA_Obj X, FLA_Obj Xbar, FLA_Obj
   op_end(st);
   if (unstage(sxb) != FLA_SUCCESS || unstage(slb) != FLA_SUCCESS || sync_all() != FLA_SUCCESS) return FLA_FAILURE;
   return FLA_SUCCESS;
+}
+
+// No counterpart in the reference.  FLA_Chol_adjoint over a batch: for each
+// i, L[i] (device, order n[i], leading dimension ld[i]) holds a lower
+// Cholesky factor and Lbar[i] (device, same order and leading dimension)
+// the adjoint of L[i]; first Lbar[i](j, j) += logdet_scale / L[i](j, j) (the
+// adjoint of logdet_scale * sum_j log L(j, j); 0 skips it), then Lbar[i]'s
+// lower triangle is replaced by Abar[i] as FLA_Chol_adjoint does.  The
+// matrices are processed one after another with the blocked adjoint.
+FLA_Error FLA_Chol_adjoint_batched(int count, const int* n, double** L, const int* ld, double** Lbar,
+                                   double logdet_scale) {
+  if (!ctx().initialized) FLA_Init();
+  for (int i = 0; i < count; ++i) {
+    FB_REQUIRE(n[i] >= 0 && ld[i] >= std::max(1, n[i]), "FLA_Chol_adjoint_batched", "bad order or leading dimension");
+    if (n[i] > 0 && (!is_device_ptr(L[i]) || !is_device_ptr(Lbar[i]))) {
+      set_last_error("FLA_Chol_adjoint_batched: matrix " + std::to_string(i) + ": buffers must be device memory");
+      return FLA_FAILURE;
+    }
+  }
+  cudaStream_t st = ctx().stream;
+  op_begin(st);
+  for (int i = 0; i < count; ++i) {
+    if (n[i] == 0) continue;
+    if (logdet_scale != 0.0 && logdet_adjoint_dev(L[i], Lbar[i], ld[i], n[i], logdet_scale, st) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    if (chol_adjoint_dev(L[i], Lbar[i], ld[i], n[i], st) != FLA_SUCCESS) return FLA_FAILURE;
+  }
+  op_end(st);
+  return sync_all();
 }
 
 }  // extern "C"

@@ -30,6 +30,7 @@
 
 #include "common.h"
 #include "batched.h"
+#include "dev_util.cuh"
 
 namespace fb {
 
@@ -117,8 +118,9 @@ __device__ void left_update(T* P, int ldp, int R, int w, const T* G, long ld, in
 // or the transposed (upper) backward sweep with the lower factor (Cholesky:
 // L^T; LU: the upper factor U is read as stored, upper = true).
 template <typename T>
-__device__ void block_solve(const T* F, long ld, int n, T* X, int nrhs, bool lower, bool trans, bool unit) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+__device__ void block_solve(const T* F, long ld, int n, T* X, int nrhs, bool lower, bool trans, bool unit,
+                            int ldx = BMAXN) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
   // op(F) is lower triangular when (lower && !trans) or (!lower && trans)
   const bool fwd = (lower != trans);
   const int nblk = (n + 31) / 32;
@@ -126,8 +128,8 @@ __device__ void block_solve(const T* F, long ld, int n, T* X, int nrhs, bool low
     const int b = fwd ? bi : nblk - 1 - bi;
     const int b0 = b * 32, w = min(32, n - b0);
     // op(F)(r, c) = trans ? F[c + r * ld] : F[r + c * ld]
-    for (int q = warp; q < nrhs; q += BT / 32) {
-      T y = lane < w ? X[b0 + lane + q * BMAXN] : T(0);
+    for (int q = warp; q < nrhs; q += nt / 32) {
+      T y = lane < w ? X[b0 + lane + q * ldx] : T(0);
       for (int s = 0; s < w; ++s) {
         const int k = fwd ? s : w - 1 - s;
         if (lane == k && !unit) {
@@ -142,21 +144,21 @@ __device__ void block_solve(const T* F, long ld, int n, T* X, int nrhs, bool low
           y -= o * yk;
         }
       }
-      if (lane < w) X[b0 + lane + q * BMAXN] = y;
+      if (lane < w) X[b0 + lane + q * ldx] = y;
     }
     __syncthreads();
     // remaining rows: fwd rows [b0 + w, n), bwd rows [0, b0)
     const int r_lo = fwd ? b0 + w : 0, r_hi = fwd ? n : b0;
     const int nr = r_hi - r_lo;
-    for (int e = tid; e < nr * nrhs; e += BT) {
+    for (int e = tid; e < nr * nrhs; e += nt) {
       const int r = r_lo + e % nr, q = e / nr;
       T s = T(0);
       for (int k = 0; k < w; ++k) {
         const int c = b0 + k;
         const T o = trans ? F[(long)c + (long)r * ld] : F[(long)r + (long)c * ld];
-        s = fma(o, X[c + q * BMAXN], s);
+        s = fma(o, X[c + q * ldx], s);
       }
-      X[r + q * BMAXN] -= s;
+      X[r + q * ldx] -= s;
     }
     __syncthreads();
   }
@@ -241,6 +243,227 @@ __global__ void __launch_bounds__(BT, 1) chol_batched_kernel(BatchArgs<T> a) {
       block_solve<T>(G, ld, n, sX, nrhs, true, false, false);
       block_solve<T>(G, ld, n, sX, nrhs, true, true, false);
       for (int e = tid; e < n * nrhs; e += BT) Bm[(long)(e % n) + (long)(e / n) * ldb] = sX[e % n + (e / n) * BMAXN];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 Cholesky, orders up to 1024, updates on the FP64 tensor cores
+// ---------------------------------------------------------------------------
+// One CTA of 16 warps per matrix (persistent over the schedule), left-looking
+// in panels of 32 columns:
+//   1. P := A(j:n, j:j+32) - L(j:n, 0:j) L(j:j+32, 0:j)^T with DMMA m8n8k4
+//      tiles: the previous columns stream through shared memory 8 at a time
+//      (cp.async, double-buffered) and each warp accumulates 4 x 4 8x8 tiles
+//      in registers; panels taller than 512 rows take several passes of 512
+//      rows, each staging the panel's own 32 rows (the B operand) beside its
+//      rows, so no warp holds more than 16 tiles;
+//   2. warp 0 factors the 32 x 32 diagonal block in registers (lane r holds
+//      row r; shuffles broadcast the pivot column): sqrt, reciprocal scaling
+//      and the rank-1 update as FLA_Chol's unblocked variant, stopping at the
+//      first pivot that is not > 0 (NaN included);
+//   3. every thread solves rows below with the block: x := x L11^-T by
+//      columns (reciprocal multiply, then axpy), as dtrsm Right/Lower/Trans.
+// The per-column work of a panel stays inside one warp: no CTA barrier per
+// column.  Optionally the log-determinant sum_i log L(i, i) per matrix and
+// the solve of up to 8 right-hand sides in the same launch.
+constexpr int DT = 512;                 // threads per CTA
+constexpr int DMAXN = 1024;             // largest order
+constexpr int DNB = 32;                 // panel width
+constexpr int DKC = 8;                  // previous columns per staged chunk
+constexpr int DPASS = 512;              // rows per update pass
+constexpr int DRP = DNB + DPASS + 8;    // chunk row stride (doubles): panel rows, pass rows, bank spread
+constexpr size_t DCHUNK = (size_t)DRP * DKC;
+constexpr size_t DSMEM_BYTES = (2 * DCHUNK + (size_t)DNB * (DNB + 1) + DNB) * sizeof(double) + 256;
+static_assert((size_t)DMAXN * BMAXRHS <= 2 * DCHUNK, "right-hand sides reuse the chunk buffers");
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Stage columns k0 .. k0 + 7 of rows j .. j + 31 (panel rows, buffer rows
+// 0 .. 31) and rows j + p0 .. j + p0 + np - 1 (buffer rows 32 ..) of G;
+// rows past the matrix, and the pad of the last 8-row tile, are zero.
+__device__ __forceinline__ void dchunk_issue(double* buf, const double* G, long ld, int j, int R, int p0, int np,
+                                             int k0) {
+  const int rows = DNB + ((np + 7) & ~7);
+  for (int e = threadIdx.x; e < rows * DKC; e += DT) {
+    const int r = e % rows, q = e / rows;
+    const int pr = r < DNB ? r : p0 + (r - DNB);  // row of the panel (0 .. R - 1)
+    const bool in = (r < DNB) ? (r < R) : (r - DNB < np);
+    double* d = buf + r + q * DRP;
+    if (in) cp_async8(d, G + (long)(j + pr) + (long)(k0 + q) * ld);
+    else *d = 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(DT, 1) chol_batched_dmma_kernel(BatchArgs<double> a) {
+  extern __shared__ __align__(16) unsigned char bsm_raw[];
+  double* sC = reinterpret_cast<double*>(bsm_raw);  // [2][DKC][DRP]
+  double* sL = sC + 2 * DCHUNK;                     // L11, row-major [DNB][DNB + 1]
+  double* sR = sL + DNB * (DNB + 1);                // 1 / L11(k, k)
+  __shared__ int s_next, s_fail;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned full = 0xffffffffu;
+  for (;;) {
+    if (tid == 0) s_next = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int slot = s_next;
+    __syncthreads();
+    if (slot >= a.count) break;
+    const int mi = a.order[slot];
+    const int n = a.n[mi];
+    const long ld = a.ld[mi];
+    double* G = a.A[mi];
+    if (tid == 0) s_fail = -1;
+    __syncthreads();
+    for (int j = 0; j < n; j += DNB) {
+      const int w = min(DNB, n - j), R = n - j;
+      // ---- 1. the panel update, in passes of up to 512 rows
+      if (j > 0) {
+        const int nch = j / DKC;  // j is a multiple of 32
+        for (int p0 = 0; p0 < R; p0 += DPASS) {
+          const int np = min(DPASS, R - p0);
+          double acc[4][4][2];
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int ct = 0; ct < 4; ++ct) acc[i][ct][0] = acc[i][ct][1] = 0.0;
+          dchunk_issue(sC, G, ld, j, R, p0, np, 0);
+          cp_async_commit();
+          for (int ch = 0; ch < nch; ++ch) {
+            if (ch + 1 < nch) {
+              dchunk_issue(sC + ((ch + 1) & 1) * DCHUNK, G, ld, j, R, p0, np, (ch + 1) * DKC);
+              cp_async_commit();
+              cp_async_wait<1>();
+            } else {
+              cp_async_wait<0>();
+            }
+            __syncthreads();
+            const double* C = sC + (ch & 1) * DCHUNK;
+#pragma unroll
+            for (int kk = 0; kk < DKC; kk += 4) {
+              const double* Ck = C + (kk + (lane & 3)) * DRP + (lane >> 2);
+              double b[4];
+#pragma unroll
+              for (int ct = 0; ct < 4; ++ct) b[ct] = Ck[ct * 8];
+#pragma unroll
+              for (int i = 0; i < 4; ++i) {
+                const int rt = warp + 16 * i;  // 8-row tile of the pass
+                if (rt * 8 < np) {
+                  const double av = Ck[DNB + rt * 8];
+#pragma unroll
+                  for (int ct = 0; ct < 4; ++ct) dmma_884(acc[i][ct][0], acc[i][ct][1], av, b[ct]);
+                }
+              }
+            }
+            __syncthreads();  // the buffer is refilled two chunks later
+          }
+          // P -= acc (lower part of the diagonal block only)
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int r = p0 + (warp + 16 * i) * 8 + (lane >> 2);
+            if (r >= p0 + np) continue;
+#pragma unroll
+            for (int ct = 0; ct < 4; ++ct)
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                const int c = ct * 8 + 2 * (lane & 3) + e;
+                if (c < w && r >= c) G[(long)(j + r) + (long)(j + c) * ld] -= acc[i][ct][e];
+              }
+          }
+        }
+        __syncthreads();
+      }
+      // ---- 2. the diagonal block in warp 0
+      if (warp == 0) {
+        double d[DNB];
+#pragma unroll
+        for (int c = 0; c < DNB; ++c) d[c] = (lane < w && c < w && c <= lane) ? G[(long)(j + lane) + (long)(j + c) * ld] : 0.0;
+        int fail = -1;
+#pragma unroll
+        for (int c = 0; c < DNB; ++c) {
+          // columns past the block or after a failure change nothing (the
+          // loop is unrolled, so d stays in registers)
+          const double piv = __shfl_sync(full, d[c], c);
+          const bool live = c < w && fail < 0;
+          if (live && !(piv > 0.0)) fail = c;
+          if (live && fail < 0) {
+            const double sq = sqrt(piv);
+            const double rs = 1.0 / sq;
+            if (lane == c) d[c] = sq;
+            else if (lane > c) d[c] *= rs;
+          }
+          const bool upd = c < w && fail < 0;
+#pragma unroll
+          for (int cc = 0; cc < DNB; ++cc) {
+            if (cc <= c) continue;  // compile-time: the trip count stays constant
+            const double lc = __shfl_sync(full, d[c], cc);  // L(cc, c)
+            if (upd && lane >= cc) d[cc] = fma(-d[c], lc, d[cc]);
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < DNB; ++c) {
+          if (lane < w && c < w && c <= lane) G[(long)(j + lane) + (long)(j + c) * ld] = d[c];
+          sL[lane * (DNB + 1) + c] = (c <= lane) ? d[c] : 0.0;
+        }
+        double dl = d[0];  // this lane's diagonal entry, without indexing d by a run-time value
+#pragma unroll
+        for (int c = 1; c < DNB; ++c)
+          if (c == lane) dl = d[c];
+        if (lane < w) sR[lane] = 1.0 / dl;
+        if (lane == 0) s_fail = fail >= 0 ? j + fail : -1;
+      }
+      __syncthreads();
+      if (s_fail >= 0) break;
+      // ---- 3. rows below the block: x := x L11^-T
+      for (int r = j + w + tid; r < n; r += DT) {
+        double x[DNB];
+#pragma unroll
+        for (int c = 0; c < DNB; ++c) x[c] = c < w ? G[(long)r + (long)(j + c) * ld] : 0.0;
+#pragma unroll
+        for (int k = 0; k < DNB; ++k) {
+          if (k < w) {
+            x[k] *= sR[k];
+#pragma unroll
+            for (int jj = k + 1; jj < DNB; ++jj) x[jj] = fma(-sL[jj * (DNB + 1) + k], x[k], x[jj]);
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < DNB; ++c)
+          if (c < w) G[(long)r + (long)(j + c) * ld] = x[c];
+      }
+      __syncthreads();
+    }
+    if (tid == 0) a.info[mi] = s_fail;
+    // log-determinant (fixed order: lane-strided partial sums, shuffle tree)
+    if (a.logdet && warp == 0) {
+      double sl = 0.0;
+      if (s_fail < 0)
+        for (int i = lane; i < n; i += 32) sl += log(G[(long)i + (long)i * ld]);
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) sl += __shfl_xor_sync(full, sl, off);
+      if (lane == 0) a.logdet[mi] = s_fail < 0 ? sl : __longlong_as_double(0x7ff8000000000000ll);
+    }
+    // solve with the factor when it succeeded
+    if (a.B && s_fail < 0) {
+      const int nrhs = a.nrhs;
+      double* Bm = a.B[mi];
+      const long ldb = a.ldb[mi];
+      double* sX = sC;
+      for (int e = tid; e < n * nrhs; e += DT) sX[e % n + (e / n) * DMAXN] = Bm[(long)(e % n) + (long)(e / n) * ldb];
+      __syncthreads();
+      block_solve<double>(G, ld, n, sX, nrhs, true, false, false, DMAXN);
+      block_solve<double>(G, ld, n, sX, nrhs, true, true, false, DMAXN);
+      for (int e = tid; e < n * nrhs; e += DT) Bm[(long)(e % n) + (long)(e / n) * ldb] = sX[e % n + (e / n) * DMAXN];
     }
     __syncthreads();
   }
@@ -408,6 +631,24 @@ __global__ void __launch_bounds__(BT, 1) lu_batched_kernel(BatchArgs<T> a) {
 
 template <typename T>
 int launch_batched(bool lu, BatchArgs<T> args, cudaStream_t st) {
+  if constexpr (sizeof(T) == 8) {
+    if (!lu) {
+      // FP64 Cholesky: the DMMA kernel (orders up to 1024)
+      static bool dattr = false;
+      if (!dattr) {
+        FB_CK(cudaFuncSetAttribute(chol_batched_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)DSMEM_BYTES));
+        dattr = true;
+      }
+      const int grid = std::min(ctx().num_sms, std::max(1, args.count));
+      const int ps = prof_begin(st);
+      chol_batched_dmma_kernel<<<grid, DT, DSMEM_BYTES, st>>>(args);
+      prof_end(ps, st, PROF_OTHER, 0.0);
+      count_launch();
+      FB_CK(cudaGetLastError());
+      return FLA_SUCCESS;
+    }
+  }
   static bool attr[2] = {false, false};
   const size_t smem = BSmem<T>::BYTES;
   if (!attr[lu ? 1 : 0]) {
@@ -457,7 +698,7 @@ int* nb_table(bool lu, bool f64) {
 // Host driver: order the matrices (largest first), launch once.
 template <typename T>
 int batched_factor(bool lu, int count, const int* h_n, T** d_A, const long* d_ld, const int* d_n, int** d_piv,
-                   int nrhs, T** d_B, const long* d_ldb, int* d_info, cudaStream_t st) {
+                   int nrhs, T** d_B, const long* d_ldb, int* d_info, cudaStream_t st, T* d_logdet) {
   if (count <= 0) return FLA_SUCCESS;
   std::vector<int> order(count);
   for (int i = 0; i < count; ++i) order[i] = i;
@@ -478,6 +719,7 @@ int batched_factor(bool lu, int count, const int* h_n, T** d_A, const long* d_ld
   a.B = d_B;
   a.ldb = d_ldb;
   a.info = d_info;
+  a.logdet = d_logdet;
   a.nb_of_size = nb_table(lu, sizeof(T) == 8);
   if (!a.nb_of_size) return FLA_FAILURE;
   // the host order must stay valid until the copy is done
@@ -485,9 +727,9 @@ int batched_factor(bool lu, int count, const int* h_n, T** d_A, const long* d_ld
   return launch_batched<T>(lu, a, st);
 }
 template int batched_factor<double>(bool, int, const int*, double**, const long*, const int*, int**, int, double**,
-                                    const long*, int*, cudaStream_t);
+                                    const long*, int*, cudaStream_t, double*);
 template int batched_factor<float>(bool, int, const int*, float**, const long*, const int*, int**, int, float**,
-                                   const long*, int*, cudaStream_t);
+                                   const long*, int*, cudaStream_t, float*);
 
 // Panel width per size bin: time every candidate width on a sample of each
 // bin's sizes (a scratch batch of SPD / general matrices) and keep the
@@ -620,7 +862,7 @@ namespace {
 
 template <typename T>
 int batched_entry(bool lu, int count, const int* n, T** A, const int* lda, int** piv, int nrhs, T** B,
-                  const int* ldb, int* info) {
+                  const int* ldb, int* info, T* logdet = nullptr) {
   using namespace fb;
   if (!ctx().initialized) FLA_Init();
   if (count < 0) {
@@ -632,9 +874,11 @@ int batched_entry(bool lu, int count, const int* n, T** A, const int* lda, int**
     set_last_error("batched: nrhs must be 0.." + std::to_string(BMAXRHS));
     return FLA_FAILURE;
   }
+  const int maxn = (!lu && sizeof(T) == 8) ? DMAXN : BMAXN;  // FP64 Cholesky: the DMMA kernel
   for (int i = 0; i < count; ++i) {
-    if (n[i] < 0 || n[i] > BMAXN || lda[i] < std::max(1, n[i]) || (nrhs > 0 && ldb[i] < std::max(1, n[i]))) {
-      set_last_error("batched: matrix " + std::to_string(i) + " has n outside 0..512 or a short leading dimension");
+    if (n[i] < 0 || n[i] > maxn || lda[i] < std::max(1, n[i]) || (nrhs > 0 && ldb[i] < std::max(1, n[i]))) {
+      set_last_error("batched: matrix " + std::to_string(i) + " has n outside 0.." + std::to_string(maxn) +
+                     " or a short leading dimension");
       return FLA_FAILURE;
     }
     if (!is_device_ptr(A[i]) || (lu && !is_device_ptr(piv[i])) || (nrhs > 0 && !is_device_ptr(B[i]))) {
@@ -646,8 +890,9 @@ int batched_entry(bool lu, int count, const int* n, T** A, const int* lda, int**
   // device copies of the argument arrays
   const size_t c = (size_t)count;
   // layout: A, B, piv pointers, ld, ldb (8 bytes each), n, info (4 bytes each)
-  char* m = (char*)ws_get(WS_MISC2, c * (8 * 5 + 4 * 2) + 1024);
+  char* m = (char*)ws_get(WS_MISC2, c * (8 * 6 + 4 * 2) + 1024);
   if (!m) return FLA_FAILURE;
+  T* dlogdet = logdet ? (T*)(m + c * 48 + 512) : nullptr;  // after the int arrays
   T** dA = (T**)m;
   T** dB = (T**)(m + c * 8);
   int** dpiv = (int**)(m + c * 16);
@@ -668,10 +913,11 @@ int batched_entry(bool lu, int count, const int* n, T** A, const int* lda, int**
   FB_CK(cudaMemcpyAsync(dldb, hldb.data(), sizeof(long) * c, cudaMemcpyHostToDevice, st));
   FB_CK(cudaMemcpyAsync(dn, n, sizeof(int) * c, cudaMemcpyHostToDevice, st));
   if (batched_factor<T>(lu, count, n, dA, dld, dn, lu ? dpiv : nullptr, nrhs, nrhs > 0 ? dB : nullptr, dldb, dinfo,
-                        st) != FLA_SUCCESS)
+                        st, dlogdet) != FLA_SUCCESS)
     return FLA_FAILURE;
   op_end(st);
   FB_CK(cudaMemcpyAsync(info, dinfo, sizeof(int) * c, cudaMemcpyDeviceToHost, st));
+  if (logdet) FB_CK(cudaMemcpyAsync(logdet, dlogdet, sizeof(T) * c, cudaMemcpyDeviceToHost, st));
   return sync_all();
 }
 
@@ -691,6 +937,17 @@ FLA_Error FLA_Chol_batched(FLA_Uplo uplo, int count, const int* n, double** A, c
     return FLA_FAILURE;
   }
   return batched_entry<double>(false, count, n, A, lda, nullptr, nrhs, B, ldb, info);
+}
+// No counterpart in the reference.  FLA_Chol_batched (FP64, lower) that also
+// returns logdet[i] = sum_j log L_i(j, j) (host array of count doubles;
+// NaN for matrices that fail), for batches of Gaussian-process likelihoods.
+FLA_Error FLA_B200_Chol_batched_logdet(int count, const int* n, double** A, const int* lda, int nrhs, double** B,
+                                       const int* ldb, double* logdet, int* info) {
+  if (!logdet && count > 0) {
+    fb::set_last_error("FLA_B200_Chol_batched_logdet: logdet is null");
+    return FLA_FAILURE;
+  }
+  return batched_entry<double>(false, count, n, A, lda, nullptr, nrhs, B, ldb, info, logdet);
 }
 FLA_Error FLA_B200_Chol_batched_f32(int count, const int* n, float** A, const int* lda, int nrhs, float** B,
                                     const int* ldb, int* info) {

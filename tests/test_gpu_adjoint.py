@@ -135,13 +135,15 @@ def test_gp_gradient_n8192_sampled_oracle_and_fd(cuda, flame, oracle):
     differences of the loss on the same 200 entries, each loss evaluated by
     FLA_Chol on the GPU."""
     torch = cuda
-    # nugget 0.1: the central differences of the loss (h = 1e-5) stay clear
-    # of its rounding noise at this size (with 1e-2 and h = 1e-6 the noise
-    # reaches 1e-5 relative)
-    n, h = 8192, 1e-5
+    # the GP of the benchmark configuration: length scale 0.3, nugget 1e-2,
+    # central differences with h = 1e-6.  Their rounding noise at this size
+    # is ~2e-5 relative (the loss is O(1e4) and K's condition number ~1e5),
+    # so they are held to 1e-4; the entry-wise oracle comparison is the
+    # tight check (1e-9).
+    n, h, fd_tol = 8192, 1e-6, 1e-4
     g = torch.Generator(device="cuda").manual_seed(8192)
     x = torch.rand((n, 3), dtype=torch.float64, device="cuda", generator=g)
-    K = torch.exp(-torch.cdist(x, x) ** 2 / (2 * 0.3 ** 2)) + 0.1 * torch.eye(n, dtype=torch.float64, device="cuda")
+    K = torch.exp(-torch.cdist(x, x) ** 2 / (2 * 0.3 ** 2)) + 1e-2 * torch.eye(n, dtype=torch.float64, device="cuda")
     K = _colmajor(0.5 * (K + K.t()))
     y = torch.randn((n, 1), dtype=torch.float64, device="cuda", generator=g)
     Ld = _colmajor(K)
@@ -184,4 +186,4 @@ def test_gp_gradient_n8192_sampled_oracle_and_fd(cuda, flame, oracle):
     for i, j in idx:
         fd = (loss_of(i, j, h) - loss_of(i, j, -h)) / (2 * h)
         an = float(Gh[i, j]) * (1 if i == j else 2)
-        assert abs(fd - an) <= 1e-5 * max(1.0, abs(an)), (i, j, fd, an)
+        assert abs(fd - an) <= fd_tol * max(1.0, abs(an)), (i, j, fd, an)

@@ -150,3 +150,87 @@ def test_batched_sharded_single_rank(cuda, flame, oracle):
                 assert rel_fro(np.tril(to_host(dev[i])), np.tril(Lo)) < 1e-12
     finally:
         dist.destroy_process_group()
+
+
+def test_chol_batched_fp64_to_order_1024_with_logdet(cuda, flame, oracle):
+    """The FP64 batched Cholesky (DMMA updates) at orders up to 1024: factors,
+    the solves of two right-hand sides and the log-determinants against the
+    oracle; a matrix that is not SPD fails at the oracle's column, with NaN
+    as its log-determinant, and does not disturb the others.  The strict
+    upper triangles are left alone."""
+    rng = seeded(1024)
+    sizes = [1, 7, 31, 32, 33, 96, 255, 511, 512, 513, 700, 1000, 1023, 1024] + list(rng.integers(1, 1025, size=6))
+    mats = [spd(rng, int(n)) for n in sizes]
+    bad = 11
+    mats[bad] = mats[bad].copy()
+    mats[bad][600, 600] = -1.0
+    dev = [to_dev(cuda, A) for A in mats]
+    rhs = [rng.standard_normal((int(n), 2)) for n in sizes]
+    drhs = [to_dev(cuda, b) for b in rhs]
+    r, info, logdet = flame.chol_batched_logdet(dev, rhs=drhs)
+    assert r == flame.FLA_SUCCESS, flame.last_error()
+    for i, A in enumerate(mats):
+        Lo, ro = oracle.chol(A)
+        assert info[i] == ro, (i, sizes[i], info[i], ro)
+        got = to_host(dev[i])
+        assert np.array_equal(np.triu(got, 1), np.triu(A, 1)), i
+        if ro != -1:
+            assert np.isnan(logdet[i])
+            continue
+        assert rel_fro(np.tril(got), np.tril(Lo)) < 1e-12, (i, sizes[i])
+        ld_o = float(np.log(np.diag(Lo)).sum())
+        assert abs(logdet[i] - ld_o) <= 1e-12 * max(1.0, abs(ld_o)), (i, logdet[i], ld_o)
+        Xo = oracle.chol_solve(Lo, rhs[i])
+        assert rel_fro(to_host(drhs[i]), Xo) < 1e-11, (i, sizes[i])
+
+
+def _gp_matrix(rng, n):
+    x = rng.uniform(0, 1, (n, 3))
+    d2 = ((x[:, None, :] - x[None, :, :]) ** 2).sum(-1)
+    return np.exp(-d2 / (2 * 0.3 ** 2)) + 1e-2 * np.eye(n), rng.standard_normal((n, 1))
+
+
+def test_256_batched_gps_loss_and_gradient(cuda, flame, oracle):
+    """256 Gaussian-process likelihoods with n uniform in [64, 1024]: forward
+    (batched Cholesky, alpha = K^-1 y, log-determinant) and backward (the
+    solve's adjoint formed from alpha and v = L^T alpha, then the batched
+    log-determinant and Cholesky adjoints) give dloss/dK; checked against
+    0.5 (K^-1 - alpha alpha^T) and the loss from the oracle's FLA_Chol and
+    triangular solves on a sample of 12 GPs (the largest and smallest
+    included), and for finiteness on all."""
+    torch = cuda
+    rng = seeded(256)
+    sizes = [int(v) for v in rng.integers(64, 1025, size=256)]
+    sizes[0], sizes[1] = 1024, 64
+    data = [_gp_matrix(rng, n) for n in sizes]
+    Ks = [to_dev(cuda, K) for K, _ in data]
+    al = [to_dev(cuda, y) for _, y in data]
+    r, info, logdet = flame.chol_batched_logdet(Ks, rhs=al)
+    assert r == flame.FLA_SUCCESS, flame.last_error()
+    assert all(v == -1 for v in info)
+    # loss_i = 0.5 y^T alpha + sum log L_ii; backward of 0.5 v^T v, v = L^-1 y:
+    # Lbar = -tril(alpha v^T) with v = L^T alpha; the log-determinant part is
+    # added by the batched adjoint (logdet_scale = 1)
+    Lbars = []
+    for Ld, a in zip(Ks, al):
+        L = torch.tril(Ld)
+        v = L.t() @ a
+        Lb = torch.empty_strided(tuple(Ld.shape), (1, Ld.shape[0]), dtype=torch.float64, device="cuda")
+        Lb.copy_(-torch.tril(a @ v.t()))
+        Lbars.append(Lb)
+    assert flame.chol_adjoint_batched(Ks, Lbars, 1.0) == flame.FLA_SUCCESS, flame.last_error()
+    losses = [0.5 * float((torch.from_numpy(y).cuda() * a).sum()) + ld for (K, y), a, ld in zip(data, al, logdet)]
+    assert all(np.isfinite(losses))
+    sample = [0, 1] + list(rng.choice(np.arange(2, 256), size=10, replace=False))
+    for i in sample:
+        K, y = data[i]
+        Lo, ro = oracle.chol(K)
+        assert ro == -1
+        n = K.shape[0]
+        Kinv = oracle.chol_solve(Lo, np.eye(n))
+        alpha = oracle.chol_solve(Lo, y)
+        loss_o = 0.5 * float(y[:, 0] @ alpha[:, 0]) + float(np.log(np.diag(Lo)).sum())
+        assert abs(losses[i] - loss_o) <= 1e-10 * max(1.0, abs(loss_o)), (i, losses[i], loss_o)
+        Ab = np.tril(to_host(Lbars[i]))
+        G = 0.5 * (Ab + Ab.T)
+        assert rel_fro(G, 0.5 * (Kinv - alpha @ alpha.T)) < 1e-9, (i, n)
