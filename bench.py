@@ -402,8 +402,58 @@ def batched_section(torch, dev, F, count):
                     "failed": int((info != -1).sum())}
         del src, work, bsrc, bwork, pivbuf
         torch.cuda.empty_cache()
-    out["note"] = "SIMT FP64/FP32 FMA kernels (one CTA per matrix, persistent grid); tflops includes the solves"
+    out["note"] = ("FP64 Cholesky: DMMA (FP64 tensor-core) left-looking kernel; FP32 Cholesky and LU: SIMT FMA "
+                   "kernels; one CTA per matrix, persistent grid, largest first; tflops includes the solves")
     return out
+
+
+def gp_batched_section(torch, dev, F, count=256):
+    """count Gaussian-process likelihoods, n ~ U{64..1024} (seed 256): K =
+    exp(-|xi-xj|^2 / (2 0.3^2)) + 1e-2 I for x ~ U[0,1]^3, y ~ N(0,1).
+    Forward: FLA_B200_Chol_batched_logdet (Cholesky, alpha = K^-1 y,
+    log-determinant) in one launch; backward: Lbar = -tril(alpha v^T),
+    v = L^T alpha (torch, untimed), then FLA_Chol_adjoint_batched with the
+    log-determinant term.  Device times of the library's calls; forward flops
+    n^3/3 + 2 n^2 per GP."""
+    rng = np.random.default_rng(256)
+    sizes = [int(v) for v in rng.integers(64, 1025, size=count)]
+    g = torch.Generator(device=dev).manual_seed(256)
+
+    def colmajor(t):
+        out = torch.empty_strided(tuple(t.shape), (1, t.shape[0]), dtype=t.dtype, device=t.device)
+        out.copy_(t)
+        return out
+    Ks0, ys = [], []
+    for n in sizes:
+        x = torch.rand((n, 3), dtype=torch.float64, device=dev, generator=g)
+        K = torch.exp(-torch.cdist(x, x) ** 2 / (2 * 0.3 ** 2)) + 1e-2 * torch.eye(n, dtype=torch.float64, device=dev)
+        Ks0.append(colmajor(K))
+        ys.append(colmajor(torch.randn((n, 1), dtype=torch.float64, device=dev, generator=g)))
+    fwd, bwd = [], []
+    for rep in range(4):
+        Ks = [K.clone() for K in Ks0]
+        al = [y.clone() for y in ys]
+        torch.cuda.synchronize()
+        r, info, logdet = F.chol_batched_logdet(Ks, rhs=al)
+        if r != F.FLA_SUCCESS or any(v != -1 for v in info):
+            raise RuntimeError("batched GP forward failed: %s" % F.last_error())
+        fms = F.last_op_ms()
+        Lbars = []
+        for Ld, a in zip(Ks, al):
+            v = torch.tril(Ld).t() @ a
+            Lbars.append(colmajor(-torch.tril(a @ v.t())))
+        torch.cuda.synchronize()
+        if F.chol_adjoint_batched(Ks, Lbars, 1.0) != F.FLA_SUCCESS:
+            raise RuntimeError("batched GP adjoint failed: %s" % F.last_error())
+        bms = F.last_op_ms()
+        if rep > 0:
+            fwd.append(fms)
+            bwd.append(bms)
+    flops = float(sum(n ** 3 / 3.0 + 2.0 * n * n for n in sizes))
+    fm = statistics.median(fwd)
+    return {"workload": "%d GPs, n ~ U{64..1024} (seed 256), FP64" % count,
+            "forward_ms": fm, "forward_tflops": flops / (fm * 1e-3) / 1e12, "adjoint_ms": statistics.median(bwd),
+            "largest_n": max(sizes), "total_rows": int(sum(sizes))}
 
 
 def qr_section(torch, dev, F, m, n, nrhs):
@@ -710,6 +760,7 @@ def run_ours(args, rank, world):
     # ---- batched factorizations + solves of many uneven matrices
     if rank == 0 and not args.no_batched:
         result["batched"] = batched_section(torch, dev, F, args.batch_count)
+        result["batched"]["gp_256"] = gp_batched_section(torch, dev, F)
 
     # ---- QR_UT + Apply_Q_UT and the Gaussian-process gradient
     if rank == 0 and not args.no_secondary:

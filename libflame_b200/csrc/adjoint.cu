@@ -27,8 +27,8 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
-
 #include <string>
+#include <vector>
 
 #include "common.h"
 
@@ -135,8 +135,14 @@ bool g_adj_attr = false;
 
 }  // namespace
 
+// Scratch of chol_adjoint_dev for order n: Dinv (AB x AB) then W (ldw x AB)
+// and S (AB x AB), in doubles.
+size_t chol_adjoint_scratch(long n) { return (size_t)AB * AB * 2 + (size_t)((n + 1) & ~1L) * AB; }
+
 // In place over Lb (lower triangle); L lower Cholesky factor; n x n, ld.
-int chol_adjoint_dev(const double* L, double* Lb, long ld, long n, cudaStream_t st) {
+// scratch: chol_adjoint_scratch(n) doubles of device memory, or nullptr for
+// the library's workspace (then calls must not overlap).
+int chol_adjoint_dev(const double* L, double* Lb, long ld, long n, cudaStream_t st, double* scratch) {
   if (n <= 0) return FLA_SUCCESS;
   if (!g_adj_attr) {
     FB_CK(cudaFuncSetAttribute(chol_adj_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ADJ_SMEM));
@@ -144,8 +150,9 @@ int chol_adjoint_dev(const double* L, double* Lb, long ld, long n, cudaStream_t 
   }
   const long nblk = (n + AB - 1) / AB;
   const long ldw = (n + 1) & ~1L;
-  double* Dinv = (double*)ws_get(WS_MISC, sizeof(double) * AB * AB);
-  double* W = (double*)ws_get(WS_MISC2, sizeof(double) * (size_t)ldw * AB + sizeof(double) * AB * AB);
+  double* Dinv = scratch ? scratch : (double*)ws_get(WS_MISC, sizeof(double) * AB * AB);
+  double* W = scratch ? scratch + (size_t)AB * AB
+                      : (double*)ws_get(WS_MISC2, sizeof(double) * (size_t)ldw * AB + sizeof(double) * AB * AB);
   if (!Dinv || !W) return FLA_FAILURE;
   double* S = W + (size_t)ldw * AB;  // (Dbar + Dbar^T), AB x AB
   auto Lat = [&](long i, long j) { return L + i + j * ld; };
@@ -244,7 +251,7 @@ FLA_Error FLA_Chol_adjoint(FLA_Uplo uplo, FLA_Obj L, FLA_Obj Lbar) {
   }
   cudaStream_t st = ctx().stream;
   op_begin(st);
-  if (chol_adjoint_dev((const double*)sl.dev, (double*)sb.dev, sl.ld, (long)L.m, st) != FLA_SUCCESS)
+  if (chol_adjoint_dev((const double*)sl.dev, (double*)sb.dev, sl.ld, (long)L.m, st, nullptr) != FLA_SUCCESS)
     return FLA_FAILURE;
   op_end(st);
   if (unstage(sb) != FLA_SUCCESS || sync_all() != FLA_SUCCESS) return FLA_FAILURE;
@@ -307,25 +314,55 @@ FLA_Error FLA_B200_Trsm_llnn_adjoint(FLA_Obj L, FLA_Obj X, FLA_Obj Xbar, FLA_Obj
 // Cholesky factor and Lbar[i] (device, same order and leading dimension)
 // the adjoint of L[i]; first Lbar[i](j, j) += logdet_scale / L[i](j, j) (the
 // adjoint of logdet_scale * sum_j log L(j, j); 0 skips it), then Lbar[i]'s
-// lower triangle is replaced by Abar[i] as FLA_Chol_adjoint does.  The
-// matrices are processed one after another with the blocked adjoint.
+// lower triangle is replaced by Abar[i] as FLA_Chol_adjoint does.  Each
+// matrix runs the blocked adjoint; the matrices, largest first, are spread
+// round-robin over a pool of streams with a scratch area each, so the small
+// per-block kernels of different matrices overlap.
 FLA_Error FLA_Chol_adjoint_batched(int count, const int* n, double** L, const int* ld, double** Lbar,
                                    double logdet_scale) {
   if (!ctx().initialized) FLA_Init();
+  long maxn = 0;
   for (int i = 0; i < count; ++i) {
     FB_REQUIRE(n[i] >= 0 && ld[i] >= std::max(1, n[i]), "FLA_Chol_adjoint_batched", "bad order or leading dimension");
     if (n[i] > 0 && (!is_device_ptr(L[i]) || !is_device_ptr(Lbar[i]))) {
       set_last_error("FLA_Chol_adjoint_batched: matrix " + std::to_string(i) + ": buffers must be device memory");
       return FLA_FAILURE;
     }
+    maxn = std::max<long>(maxn, n[i]);
   }
+  if (count <= 0 || maxn == 0) return FLA_SUCCESS;
+  constexpr int NS = 8;
+  static cudaStream_t pool[NS];
+  static cudaEvent_t ev[NS + 1];
+  static bool made = false;
+  if (!made) {
+    for (int q = 0; q < NS; ++q) FB_CK(cudaStreamCreateWithFlags(&pool[q], cudaStreamNonBlocking));
+    for (int q = 0; q <= NS; ++q) FB_CK(cudaEventCreateWithFlags(&ev[q], cudaEventDisableTiming));
+    made = true;
+  }
+  const size_t per = chol_adjoint_scratch(maxn);
+  double* scr = (double*)ws_get(WS_ADJ, sizeof(double) * per * NS);
+  if (!scr) return FLA_FAILURE;
+  std::vector<int> order(count);
+  for (int i = 0; i < count; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return n[x] > n[y]; });
   cudaStream_t st = ctx().stream;
   op_begin(st);
-  for (int i = 0; i < count; ++i) {
+  FB_CK(cudaEventRecord(ev[NS], st));
+  for (int q = 0; q < NS; ++q) FB_CK(cudaStreamWaitEvent(pool[q], ev[NS], 0));
+  // orders above 2048 reach the GEMM engine's split-K workspace, which the
+  // streams of the pool would share: one stream then
+  const int ns = maxn > 2048 ? 1 : NS;
+  for (int k = 0; k < count; ++k) {
+    const int i = order[k], q = k % ns;
     if (n[i] == 0) continue;
-    if (logdet_scale != 0.0 && logdet_adjoint_dev(L[i], Lbar[i], ld[i], n[i], logdet_scale, st) != FLA_SUCCESS)
+    if (logdet_scale != 0.0 && logdet_adjoint_dev(L[i], Lbar[i], ld[i], n[i], logdet_scale, pool[q]) != FLA_SUCCESS)
       return FLA_FAILURE;
-    if (chol_adjoint_dev(L[i], Lbar[i], ld[i], n[i], st) != FLA_SUCCESS) return FLA_FAILURE;
+    if (chol_adjoint_dev(L[i], Lbar[i], ld[i], n[i], pool[q], scr + per * q) != FLA_SUCCESS) return FLA_FAILURE;
+  }
+  for (int q = 0; q < NS; ++q) {
+    FB_CK(cudaEventRecord(ev[q], pool[q]));
+    FB_CK(cudaStreamWaitEvent(st, ev[q], 0));
   }
   op_end(st);
   return sync_all();

@@ -117,8 +117,10 @@ __device__ void left_update(T* P, int ldp, int R, int w, const T* G, long ld, in
 // (n x nrhs, ld BMAXN) in shared memory.  Lower (unit or not) forward sweep,
 // or the transposed (upper) backward sweep with the lower factor (Cholesky:
 // L^T; LU: the upper factor U is read as stored, upper = true).
+// sD: 32 x 33 shared scratch for op(F)'s diagonal blocks, so the serial
+// per-column steps of the warp solves read shared memory, not L2.
 template <typename T>
-__device__ void block_solve(const T* F, long ld, int n, T* X, int nrhs, bool lower, bool trans, bool unit,
+__device__ void block_solve(const T* F, long ld, int n, T* X, int nrhs, bool lower, bool trans, bool unit, T* sD,
                             int ldx = BMAXN) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
   // op(F) is lower triangular when (lower && !trans) or (!lower && trans)
@@ -127,22 +129,20 @@ __device__ void block_solve(const T* F, long ld, int n, T* X, int nrhs, bool low
   for (int bi = 0; bi < nblk; ++bi) {
     const int b = fwd ? bi : nblk - 1 - bi;
     const int b0 = b * 32, w = min(32, n - b0);
-    // op(F)(r, c) = trans ? F[c + r * ld] : F[r + c * ld]
+    // op(F)(r, c) = trans ? F[c + r * ld] : F[r + c * ld]; the block into sD
+    for (int e = tid; e < w * w; e += nt) {
+      const int r = e % w, c = e / w;
+      sD[r + c * 33] = trans ? F[(long)(b0 + c) + (long)(b0 + r) * ld] : F[(long)(b0 + r) + (long)(b0 + c) * ld];
+    }
+    __syncthreads();
     for (int q = warp; q < nrhs; q += nt / 32) {
       T y = lane < w ? X[b0 + lane + q * ldx] : T(0);
       for (int s = 0; s < w; ++s) {
         const int k = fwd ? s : w - 1 - s;
-        if (lane == k && !unit) {
-          const T d = trans ? F[(long)(b0 + k) + (long)(b0 + k) * ld] : F[(long)(b0 + k) + (long)(b0 + k) * ld];
-          y = y / d;
-        }
+        if (lane == k && !unit) y = y / sD[k + k * 33];
         const T yk = __shfl_sync(0xffffffffu, y, k);
         const bool below = fwd ? (lane > k && lane < w) : (lane < k);
-        if (below) {
-          const int r = b0 + lane, c = b0 + k;
-          const T o = trans ? F[(long)c + (long)r * ld] : F[(long)r + (long)c * ld];
-          y -= o * yk;
-        }
+        if (below) y -= sD[lane + k * 33] * yk;
       }
       if (lane < w) X[b0 + lane + q * ldx] = y;
     }
@@ -240,8 +240,8 @@ __global__ void __launch_bounds__(BT, 1) chol_batched_kernel(BatchArgs<T> a) {
       const long ldb = a.ldb[mi];
       for (int e = tid; e < n * nrhs; e += BT) sX[e % n + (e / n) * BMAXN] = Bm[(long)(e % n) + (long)(e / n) * ldb];
       __syncthreads();
-      block_solve<T>(G, ld, n, sX, nrhs, true, false, false);
-      block_solve<T>(G, ld, n, sX, nrhs, true, true, false);
+      block_solve<T>(G, ld, n, sX, nrhs, true, false, false, sChunk);
+      block_solve<T>(G, ld, n, sX, nrhs, true, true, false, sChunk);
       for (int e = tid; e < n * nrhs; e += BT) Bm[(long)(e % n) + (long)(e / n) * ldb] = sX[e % n + (e / n) * BMAXN];
     }
     __syncthreads();
@@ -271,38 +271,40 @@ __global__ void __launch_bounds__(BT, 1) chol_batched_kernel(BatchArgs<T> a) {
 constexpr int DT = 512;                 // threads per CTA
 constexpr int DMAXN = 1024;             // largest order
 constexpr int DNB = 32;                 // panel width
-constexpr int DKC = 8;                  // previous columns per staged chunk
+constexpr int DKC = 16;                 // previous columns per staged chunk (one warp each)
 constexpr int DPASS = 512;              // rows per update pass
-constexpr int DRP = DNB + DPASS + 8;    // chunk row stride (doubles): panel rows, pass rows, bank spread
+constexpr int DPO = 36;                 // offset of the pass rows in a staged column (doubles)
+constexpr int DRP = 2 + DPO + DPASS + 10;  // staged column stride: shift slot, panel rows, gap, pass rows, spare
 constexpr size_t DCHUNK = (size_t)DRP * DKC;
 constexpr size_t DSMEM_BYTES = (2 * DCHUNK + (size_t)DNB * (DNB + 1) + DNB) * sizeof(double) + 256;
 static_assert((size_t)DMAXN * BMAXRHS <= 2 * DCHUNK, "right-hand sides reuse the chunk buffers");
 
-__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
-               "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// Stage columns k0 .. k0 + 7 of rows j .. j + 31 (panel rows, buffer rows
-// 0 .. 31) and rows j + p0 .. j + p0 + np - 1 (buffer rows 32 ..) of G;
-// rows past the matrix, and the pad of the last 8-row tile, are zero.
-__device__ __forceinline__ void dchunk_issue(double* buf, const double* G, long ld, int j, int R, int p0, int np,
-                                             int k0) {
-  const int rows = DNB + ((np + 7) & ~7);
-  for (int e = threadIdx.x; e < rows * DKC; e += DT) {
-    const int r = e % rows, q = e / rows;
-    const int pr = r < DNB ? r : p0 + (r - DNB);  // row of the panel (0 .. R - 1)
-    const bool in = (r < DNB) ? (r < R) : (r - DNB < np);
-    double* d = buf + r + q * DRP;
-    if (in) cp_async8(d, G + (long)(j + pr) + (long)(k0 + q) * ld);
-    else *d = 0.0;
-  }
+// Stage columns k0 .. k0 + 15 of G with bulk copies issued by one warp:
+// lane (part, q) copies column k0 + q's panel rows j .. j + min(32, R) - 1
+// (part 0) or its pass rows j + p0 .. j + p0 + np - 1 (part 1).  A bulk copy
+// needs 16-byte aligned ends, so a column whose first element sits 8 bytes
+// past a boundary (odd leading dimensions) is copied from one element
+// earlier into one slot earlier: element r of staged column q lies at
+// buf + q DRP + shift[q] + r (panel rows) or + DPO + r (pass rows), shift[q]
+// = 2 - (misaligned).  The copies may read one element before the first
+// row and one after the last: rows j - 1 >= 31 and, since the staged
+// columns are left of the panel (column < j <= n - 1), at most one element
+// into the next column's storage.  Rows past R are left unwritten; they only
+// feed output rows or columns that are discarded.
+__device__ __forceinline__ void dchunk_issue_bulk(double* buf, int* shift, uint32_t bar, const double* G, long ld,
+                                                  int j, int R, int p0, int np, int k0) {
+  const int lane = threadIdx.x & 31, q = lane & 15, part = lane >> 4;
+  const double* src = G + (long)j + (long)(k0 + q) * ld + (part ? p0 : 0);
+  const int cnt = part ? np : min(DNB, R);
+  const int off = (int)((reinterpret_cast<uintptr_t>(src) >> 3) & 1);
+  const int sh = 2 - off;
+  const uint32_t bytes = (uint32_t)(8 * ((cnt + off + 1) & ~1));
+  const unsigned total = __reduce_add_sync(0xffffffffu, bytes);
+  if (lane == 0) mbar_arrive_expect_tx(bar, total);
+  if (part == 0) shift[q] = sh;
+  __syncwarp();
+  double* dst = buf + q * DRP + sh + (part ? DPO : 0) - off;
+  bulk_copy_g2s(smem_u32(dst), src - off, bytes, bar);
 }
 
 __global__ void __launch_bounds__(DT, 1) chol_batched_dmma_kernel(BatchArgs<double> a) {
@@ -311,8 +313,19 @@ __global__ void __launch_bounds__(DT, 1) chol_batched_dmma_kernel(BatchArgs<doub
   double* sL = sC + 2 * DCHUNK;                     // L11, row-major [DNB][DNB + 1]
   double* sR = sL + DNB * (DNB + 1);                // 1 / L11(k, k)
   __shared__ int s_next, s_fail;
+  __shared__ int s_shift[2][DKC];                   // column shifts of the two staged chunks
+  __shared__ __align__(8) unsigned long long s_bar[2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const unsigned full = 0xffffffffu;
+  const uint32_t bar0 = smem_u32(&s_bar[0]);
+  if (tid == 0) {
+    mbar_init(bar0, 1);
+    mbar_init(bar0 + 8, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  uint32_t uses[2] = {0u, 0u};  // completed phases per buffer (the same in every thread)
+  bool ok = true;               // false after a wait ran out (the results are then garbage)
   for (;;) {
     if (tid == 0) s_next = atomicAdd(a.counter, 1);
     __syncthreads();
@@ -329,7 +342,7 @@ __global__ void __launch_bounds__(DT, 1) chol_batched_dmma_kernel(BatchArgs<doub
       const int w = min(DNB, n - j), R = n - j;
       // ---- 1. the panel update, in passes of up to 512 rows
       if (j > 0) {
-        const int nch = j / DKC;  // j is a multiple of 32
+        const int nch = j / DKC;  // j is a multiple of 32, DKC = 16
         for (int p0 = 0; p0 < R; p0 += DPASS) {
           const int np = min(DPASS, R - p0);
           double acc[4][4][2];
@@ -337,21 +350,20 @@ __global__ void __launch_bounds__(DT, 1) chol_batched_dmma_kernel(BatchArgs<doub
           for (int i = 0; i < 4; ++i)
 #pragma unroll
             for (int ct = 0; ct < 4; ++ct) acc[i][ct][0] = acc[i][ct][1] = 0.0;
-          dchunk_issue(sC, G, ld, j, R, p0, np, 0);
-          cp_async_commit();
+          if (warp == 0) dchunk_issue_bulk(sC, s_shift[0], bar0, G, ld, j, R, p0, np, 0);
           for (int ch = 0; ch < nch; ++ch) {
-            if (ch + 1 < nch) {
-              dchunk_issue(sC + ((ch + 1) & 1) * DCHUNK, G, ld, j, R, p0, np, (ch + 1) * DKC);
-              cp_async_commit();
-              cp_async_wait<1>();
-            } else {
-              cp_async_wait<0>();
-            }
-            __syncthreads();
-            const double* C = sC + (ch & 1) * DCHUNK;
+            const int bsel = ch & 1;
+            if (warp == 0 && ch + 1 < nch)
+              dchunk_issue_bulk(sC + (bsel ^ 1) * DCHUNK, s_shift[bsel ^ 1], bar0 + 8 * (bsel ^ 1), G, ld, j, R, p0,
+                                np, (ch + 1) * DKC);
+            // after a wait has run out (error flag set) the rest is not waited for
+            if (ok && !mbar_wait(bar0 + 8 * bsel, uses[bsel] & 1u, a.err, 41)) ok = false;
+            ++uses[bsel];
+            const double* C = sC + bsel * DCHUNK;
 #pragma unroll
             for (int kk = 0; kk < DKC; kk += 4) {
-              const double* Ck = C + (kk + (lane & 3)) * DRP + (lane >> 2);
+              const int cq = kk + (lane & 3);
+              const double* Ck = C + cq * DRP + s_shift[bsel][cq] + (lane >> 2);
               double b[4];
 #pragma unroll
               for (int ct = 0; ct < 4; ++ct) b[ct] = Ck[ct * 8];
@@ -359,7 +371,7 @@ __global__ void __launch_bounds__(DT, 1) chol_batched_dmma_kernel(BatchArgs<doub
               for (int i = 0; i < 4; ++i) {
                 const int rt = warp + 16 * i;  // 8-row tile of the pass
                 if (rt * 8 < np) {
-                  const double av = Ck[DNB + rt * 8];
+                  const double av = Ck[DPO + rt * 8];
 #pragma unroll
                   for (int ct = 0; ct < 4; ++ct) dmma_884(acc[i][ct][0], acc[i][ct][1], av, b[ct]);
                 }
@@ -388,28 +400,41 @@ __global__ void __launch_bounds__(DT, 1) chol_batched_dmma_kernel(BatchArgs<doub
         double d[DNB];
 #pragma unroll
         for (int c = 0; c < DNB; ++c) d[c] = (lane < w && c < w && c <= lane) ? G[(long)(j + lane) + (long)(j + c) * ld] : 0.0;
+        // A run-time loop over the columns (a fully unrolled one is tens of
+        // KB of straight-line code that one warp runs once per panel, missing
+        // the instruction cache throughout); select chains over
+        // compile-time indices keep d in registers, and column c reaches
+        // the other lanes through shared memory (sL's first two rows as a
+        // two-slot buffer, written back only after the loop).
+        double* scol = sL;
         int fail = -1;
+#pragma unroll 1
+        for (int c = 0; c < w; ++c) {
+          double dc = d[0];  // this lane's entry of column c
 #pragma unroll
-        for (int c = 0; c < DNB; ++c) {
-          // columns past the block or after a failure change nothing (the
-          // loop is unrolled, so d stays in registers)
-          const double piv = __shfl_sync(full, d[c], c);
-          const bool live = c < w && fail < 0;
-          if (live && !(piv > 0.0)) fail = c;
-          if (live && fail < 0) {
-            const double sq = sqrt(piv);
-            const double rs = 1.0 / sq;
-            if (lane == c) d[c] = sq;
-            else if (lane > c) d[c] *= rs;
+          for (int q = 1; q < DNB; ++q)
+            if (q == c) dc = d[q];
+          const double piv = __shfl_sync(full, dc, c);
+          if (!(piv > 0.0)) {  // the same value in every lane
+            fail = c;
+            break;
           }
-          const bool upd = c < w && fail < 0;
+          const double sq = sqrt(piv);
+          const double rs = 1.0 / sq;
+          const double nc = lane == c ? sq : (lane > c ? dc * rs : dc);  // L(lane, c)
 #pragma unroll
-          for (int cc = 0; cc < DNB; ++cc) {
-            if (cc <= c) continue;  // compile-time: the trip count stays constant
-            const double lc = __shfl_sync(full, d[c], cc);  // L(cc, c)
-            if (upd && lane >= cc) d[cc] = fma(-d[c], lc, d[cc]);
+          for (int q = 0; q < DNB; ++q)
+            if (q == c) d[q] = nc;
+          double* col = scol + (c & 1) * DNB;
+          col[lane] = nc;
+          __syncwarp();
+#pragma unroll
+          for (int q = 0; q < DNB; ++q) {
+            const double lq = col[q];  // L(q, c)
+            if (q > c && lane >= q) d[q] = fma(-nc, lq, d[q]);
           }
         }
+        __syncwarp();
 #pragma unroll
         for (int c = 0; c < DNB; ++c) {
           if (lane < w && c < w && c <= lane) G[(long)(j + lane) + (long)(j + c) * ld] = d[c];
@@ -461,8 +486,8 @@ __global__ void __launch_bounds__(DT, 1) chol_batched_dmma_kernel(BatchArgs<doub
       double* sX = sC;
       for (int e = tid; e < n * nrhs; e += DT) sX[e % n + (e / n) * DMAXN] = Bm[(long)(e % n) + (long)(e / n) * ldb];
       __syncthreads();
-      block_solve<double>(G, ld, n, sX, nrhs, true, false, false, DMAXN);
-      block_solve<double>(G, ld, n, sX, nrhs, true, true, false, DMAXN);
+      block_solve<double>(G, ld, n, sX, nrhs, true, false, false, sL, DMAXN);
+      block_solve<double>(G, ld, n, sX, nrhs, true, true, false, sL, DMAXN);
       for (int e = tid; e < n * nrhs; e += DT) Bm[(long)(e % n) + (long)(e / n) * ldb] = sX[e % n + (e / n) * DMAXN];
     }
     __syncthreads();
@@ -621,8 +646,8 @@ __global__ void __launch_bounds__(BT, 1) lu_batched_kernel(BatchArgs<T> a) {
           }
         }
       __syncthreads();
-      block_solve<T>(G, ld, n, sX, nrhs, true, false, true);
-      block_solve<T>(G, ld, n, sX, nrhs, false, false, false);
+      block_solve<T>(G, ld, n, sX, nrhs, true, false, true, sChunk);
+      block_solve<T>(G, ld, n, sX, nrhs, false, false, false, sChunk);
       for (int e = tid; e < n * nrhs; e += BT) Bm[(long)(e % n) + (long)(e / n) * ldb] = sX[e % n + (e / n) * BMAXN];
     }
     __syncthreads();
@@ -720,6 +745,7 @@ int batched_factor(bool lu, int count, const int* h_n, T** d_A, const long* d_ld
   a.ldb = d_ldb;
   a.info = d_info;
   a.logdet = d_logdet;
+  a.err = ctx().d_status + ST_ERROR;
   a.nb_of_size = nb_table(lu, sizeof(T) == 8);
   if (!a.nb_of_size) return FLA_FAILURE;
   // the host order must stay valid until the copy is done
@@ -905,7 +931,7 @@ int batched_entry(bool lu, int count, const int* n, T** A, const int* lda, int**
     hld[i] = lda[i];
     if (nrhs > 0) hldb[i] = ldb[i];
   }
-  op_begin(st);
+  if (status_reset() != FLA_SUCCESS) return FLA_FAILURE;  // starts the op timing
   FB_CK(cudaMemcpyAsync(dA, A, sizeof(T*) * c, cudaMemcpyHostToDevice, st));
   if (nrhs > 0) FB_CK(cudaMemcpyAsync(dB, B, sizeof(T*) * c, cudaMemcpyHostToDevice, st));
   if (lu) FB_CK(cudaMemcpyAsync(dpiv, piv, sizeof(int*) * c, cudaMemcpyHostToDevice, st));
@@ -915,9 +941,10 @@ int batched_entry(bool lu, int count, const int* n, T** A, const int* lda, int**
   if (batched_factor<T>(lu, count, n, dA, dld, dn, lu ? dpiv : nullptr, nrhs, nrhs > 0 ? dB : nullptr, dldb, dinfo,
                         st, dlogdet) != FLA_SUCCESS)
     return FLA_FAILURE;
-  op_end(st);
   FB_CK(cudaMemcpyAsync(info, dinfo, sizeof(int) * c, cudaMemcpyDeviceToHost, st));
   if (logdet) FB_CK(cudaMemcpyAsync(logdet, dlogdet, sizeof(T) * c, cudaMemcpyDeviceToHost, st));
+  // ends the op timing; a wait that ran out makes the call fail
+  if (status_read(nullptr) != FLA_SUCCESS) return FLA_FAILURE;
   return sync_all();
 }
 

@@ -19,6 +19,7 @@ struct BatchArgs {
   int* info = nullptr;          // per matrix: -1 or the failing / first zero-pivot column
   const int* nb_of_size = nullptr;  // panel width by order
   T* logdet = nullptr;          // optional: per matrix sum_i log L(i, i) (FP64 Cholesky)
+  int* err = nullptr;           // status word for wait timeouts (FP64 Cholesky)
 };
 
 template <typename T>

@@ -108,6 +108,7 @@ enum WsSlot : int {
   WS_QR_T,          // FLA_QR_UT: the T factors of two panels (ping-pong)
   WS_QR_U,          //   unit lower trapezoids of the panel recursion
   WS_QR_W,          //   its W products
+  WS_ADJ,           // per-stream scratch of the batched Cholesky adjoint
   WS_PANEL_T,       // transposed copies of Cholesky panels (two, ping-pong)
   WS_SWEEP,         // ready flags of the one-launch triangular sweeps
   WS_NSLOTS

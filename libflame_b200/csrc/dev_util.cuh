@@ -179,6 +179,15 @@ __device__ __forceinline__ void st_async_b32(uint32_t raddr, uint32_t v, uint32_
                : "memory");
 }
 
+// Bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned)
+// from global memory into this CTA's shared memory, completing the bytes
+// on the mbarrier bar.  No multicast.
+__device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
 // Orders this thread's generic-proxy writes to shared memory before later
 // async-proxy reads of them (a bulk copy issued after a CTA barrier).
 __device__ __forceinline__ void fence_proxy_async_smem() {
