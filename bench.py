@@ -286,7 +286,7 @@ def mixed_ir_section(torch, dev, F, n, nrhs, cpu=False):
                     raise RuntimeError("mixed solver failed (%s, kappa %.0e, rep %d): %d %s"
                                        % (kind, kappa, rep, r, F.last_error()))
                 tmx.append(F.last_op_ms())
-                rec = {"iter": it, "path": "fp16 factors + refinement" if it >= 0 else "FP64 fallback"}
+                rec = {"iter": it, "path": "FP16 hi/lo split factors + refinement" if it >= 0 else "FP64 fallback"}
             f64, fmx = min(t64), min(tmx)
             rec.update({"fp64_ms": f64, "mixed_ms": fmx, "speedup": f64 / fmx,
                         "backward_error_fp64": berr(A, X64), "backward_error_mixed": berr(A, Xmx),
@@ -307,9 +307,9 @@ def mixed_ir_section(torch, dev, F, n, nrhs, cpu=False):
     del Q, V, work
     torch.cuda.empty_cache()
     return {"workload": "n=%d, nrhs=%d, A = Q diag(s) Q^T / U diag(s) V^T, s log-spaced to kappa" % (n, nrhs),
-            "solver": "default (adaptive): FP16 tensor-core factors + classic FP64 refinement while each step cuts "
-                      "the backward error >= 4x, else the FP64 factorization; gmres_ir: GMRES-IR on the FP16 "
-                      "factors (3xTF32, then FP64, when it stalls)",
+            "solver": "default (adaptive): FP16 hi/lo split (FP32-accurate) tcgen05 factors + classic FP64 "
+                      "refinement while each step cuts the backward error >= 4x, else the FP64 factorization; "
+                      "gmres_ir: GMRES-IR on plain FP16 factors (then the split, 3xTF32 and FP64 when it stalls)",
             "cases": out}
 
 

@@ -78,13 +78,15 @@ int           FLA_B200_LU_piv_panel_noalloc( int m, int n, double* A, int lda, i
  * iterative refinement restores FP64 accuracy; A is left unchanged.
  * prec: 0 BF16, 1 FP16 with power-of-two equilibration, 2 3xTF32
  * (FP32-accurate), 3 FP16 hi/lo split (FP32-accurate, on the 16-bit
- * tensor cores), -1 the library default (FLA_B200_IR_PREC, else FP16).
+ * tensor cores), -1 the library default (FLA_B200_IR_PREC, else the FP16
+ * hi/lo split).
  * solver: 0 classic refinement (dsgesv_'s), 1 GMRES-IR (GMRES in FP64
  * preconditioned by the low-precision factors, for ill-conditioned A),
  * 2 adaptive (classic refinement while each step cuts the backward error
- * at least fourfold, else straight to the FP64 factorization), -1 the
+ * at least fourfold, else the next format of the ladder below), -1 the
  * default (FLA_B200_IR_SOLVER = ir | gmres | auto, else adaptive).
- * Classic and GMRES-IR escalate to 3xTF32 before the FP64 factorization.
+ * A 16-bit format whose refinement stalls escalates to the FP16 hi/lo
+ * split; classic and GMRES-IR also to 3xTF32; then the FP64 factorization.
  * iter (optional) receives the
  * number of refinement steps, or -3 (low-precision factorization failed)
  * / -31 (no convergence in 30 steps) when the FP64 factorization of a copy

@@ -6,13 +6,12 @@
 namespace fb {
 
 // IR_AUTO: classic refinement while every step reduces the backward error at
-// least fourfold; otherwise the caller falls back to the FP64 factorization
-// (on B200 the FP32-accurate tensor-core factorization costs about as much as
-// the FP64 one, so no intermediate format is tried).
+// least fourfold; otherwise the caller escalates (a 16-bit format to the
+// FP32-accurate FP16 hi/lo split, that one to the FP64 factorization).
 enum IrSolver : int { IR_CLASSIC = 0, IR_GMRES = 1, IR_AUTO = 2 };
 
 struct IrConfig {
-  LowPrec prec = LP_FP16;   // format of the tensor-core updates (escalates to LP_TF32X3)
+  LowPrec prec = LP_FP16X3;  // format of the tensor-core updates: the FP16 hi/lo split (FP32-accurate)
   bool scale = true;        // power-of-two equilibration before rounding
   IrSolver solver = IR_AUTO;
   int itermax = 30;         // ITERMAX of dsgesv_/dsposv_

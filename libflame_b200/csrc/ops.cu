@@ -570,10 +570,12 @@ int mixed_solve_dev(bool chol, bool upper, DMat A, DMat B, DMat X, int* d_piv, c
     Ares.ld = ld;
   }
   // Escalation: the requested format first; if its factorization breaks
-  // down or the refinement stalls, the FP32-accurate tensor-core format
-  // (3xTF32, classic and GMRES-IR only); then the FP64 factorization.
+  // down or the refinement stalls, an FP32-accurate tensor-core format (the
+  // FP16 hi/lo split after a 16-bit format; 3xTF32 for classic and GMRES-IR
+  // refinement as well); then the FP64 factorization.
   int steps = 0, code = -31;
   std::vector<LowPrec> ladder{cfg.prec};
+  if (cfg.prec == LP_FP16 || cfg.prec == LP_BF16) ladder.push_back(LP_FP16X3);
   if (cfg.prec != LP_TF32X3 && cfg.solver != IR_AUTO) ladder.push_back(LP_TF32X3);
   static const bool trace = std::getenv("FLA_B200_IR_TRACE") != nullptr;
   for (LowPrec p : ladder) {
@@ -660,8 +662,8 @@ extern "C" {
 // src/map/common/lapacksrc/f2c/dsgesv.c:189-412: same arguments, checks and
 // ITER/INFO conventions; the single-precision factorization is the 16-bit
 // tensor-core LU (format and refinement from FLA_B200_IR_PREC /
-// FLA_B200_IR_SOLVER; by default FP16 with equilibration and the adaptive
-// refinement of FLA_B200_LU_piv_solve_mixed).  work and swork are not
+// FLA_B200_IR_SOLVER; by default the FP16 hi/lo split with equilibration
+// and the adaptive refinement of FLA_B200_LU_piv_solve_mixed).  work and swork are not
 // referenced (the library keeps its own workspace).
 int dsgesv_(int* n, int* nrhs, double* a, int* lda, int* ipiv, double* b, int* ldb, double* x, int* ldx,
             double* work, float* swork, int* iter, int* info) {
