@@ -53,7 +53,74 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-count", type=int, default=10000)
     ap.add_argument("--ir-n", type=int, default=16384)
+    ap.add_argument("--profile-op", default=None,
+                    choices=["lu", "chol", "qr", "apply_q", "mixed_spd", "mixed_general", "batched_chol"],
+                    help="run one operation twice at order --n (for ncu captures) and exit")
     return ap.parse_args()
+
+
+def profile_op(args):
+    """One operation at order n, twice (the second call is the one a capture
+    would look at), for ncu: lu / chol (FLA_LU_piv / FLA_Chol on n x n),
+    qr / apply_q (FLA_QR_UT on 2n x n, then FLA_Apply_Q_UT on 64 columns),
+    mixed_spd / mixed_general (the default mixed solvers, 32 right-hand
+    sides, kappa 1e2), batched_chol (n matrices of orders U{8..512}).
+    Prints one JSON line with the device times of the calls."""
+    import torch
+    import libflame_b200 as F
+    F.init()
+    dev = "cuda"
+    n = args.n
+    g = torch.Generator(device=dev).manual_seed(11)
+    out = {"profile_op": args.profile_op, "n": n, "ms": []}
+
+    def colmajor(t):
+        return t.t().contiguous().t()
+    for rep in range(2):
+        if args.profile_op == "lu":
+            A = colmajor(torch.rand((n, n), dtype=torch.float64, device=dev, generator=g) * 2 - 1)
+            p = torch.zeros(n, dtype=torch.int32, device=dev)
+            r = F.lu_piv(A, p)
+        elif args.profile_op == "chol":
+            G = torch.randn((n, n), dtype=torch.float64, device=dev, generator=g)
+            A = colmajor(G @ G.t() / n + torch.eye(n, dtype=torch.float64, device=dev))
+            r = F.chol(A)
+        elif args.profile_op in ("qr", "apply_q"):
+            A = colmajor(torch.randn((2 * n, n), dtype=torch.float64, device=dev, generator=g))
+            T = torch.zeros((n, 32), dtype=torch.float64, device=dev).t()
+            r = F.qr_ut(A, T)
+            if args.profile_op == "apply_q" and r == F.FLA_SUCCESS:
+                B = colmajor(torch.randn((2 * n, 64), dtype=torch.float64, device=dev, generator=g))
+                r = F.apply_q_ut(A, T, B)
+        elif args.profile_op in ("mixed_spd", "mixed_general"):
+            Q = torch.linalg.qr(torch.randn((n, n), dtype=torch.float64, device=dev, generator=g))[0]
+            s = torch.logspace(0, -2, n, dtype=torch.float64, device=dev)
+            A = (Q * s) @ Q.t()
+            if args.profile_op == "mixed_general":
+                V = torch.linalg.qr(torch.randn((n, n), dtype=torch.float64, device=dev, generator=g))[0]
+                A = (Q * s) @ V.t()
+            else:
+                A = (A + A.t()) / 2
+            A = colmajor(A)
+            B = colmajor(torch.randn((n, 32), dtype=torch.float64, device=dev, generator=g))
+            X = colmajor(torch.empty((n, 32), dtype=torch.float64, device=dev))
+            if args.profile_op == "mixed_spd":
+                r = F.chol_solve_mixed(A, B, X, F.FLA_LOWER_TRIANGULAR)[0]
+            else:
+                r = F.lu_piv_solve_mixed(A, B, X)[0]
+        else:
+            rng = np.random.default_rng(5)
+            mats = []
+            for m in rng.integers(8, 513, size=n):
+                m = int(m)
+                G = torch.randn((m, m), dtype=torch.float64, device=dev, generator=g)
+                mats.append(colmajor(G @ G.t() / m + torch.eye(m, dtype=torch.float64, device=dev)))
+            r = F.batched("chol", mats)[0]
+        torch.cuda.synchronize()
+        if r != F.FLA_SUCCESS:
+            raise RuntimeError("%s failed: %s" % (args.profile_op, F.last_error()))
+        out["ms"].append(F.last_op_ms())
+    print(json.dumps(out))
 
 
 # ---------------------------------------------------------------------------
@@ -795,6 +862,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.profile_op:
+        profile_op(args)
         return
     if world > 1:
         import datetime
