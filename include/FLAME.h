@@ -298,6 +298,52 @@ int dsgesv_( int* n, int* nrhs, double* a, int* lda, int* ipiv, double* b, int* 
 int dsposv_( char* uplo, int* n, int* nrhs, double* a, int* lda, double* b, int* ldb, double* x, int* ldx,
              double* work, float* swork, int* iter, int* info );
 
+/* ---- FLASH hierarchical objects and front-ends ----------------------------
+ * Depth-1 hierarchies (storage by blocks, in HBM): the leaves of an m x n
+ * object are b_m x b_n blocks (the last row and column smaller); the
+ * front-ends gather the blocks into a column-major HBM copy, run the flat
+ * entry point and scatter the result back, with the flat entry point's
+ * return values.  Depths above 1 are rejected. */
+/* src/base/flamec/hierarchy/main/FLASH_Obj.c:20-81, 143-175, 591-700, 765-780 */
+dim_t         FLASH_Obj_depth( FLA_Obj H );
+dim_t         FLASH_Obj_blocksizes( FLA_Obj H, dim_t* b_m, dim_t* b_n );
+FLA_Error     FLASH_Obj_create( FLA_Datatype datatype, dim_t m, dim_t n, dim_t depth, dim_t* b_mn, FLA_Obj* H );
+FLA_Error     FLASH_Obj_create_ext( FLA_Datatype datatype, dim_t m, dim_t n, dim_t depth, dim_t* b_m, dim_t* b_n,
+                                    FLA_Obj* H );
+FLA_Error     FLASH_Obj_create_hier_copy_of_flat( FLA_Obj F, dim_t depth, dim_t* b_mn, FLA_Obj* H );
+FLA_Error     FLASH_Obj_create_hier_copy_of_flat_ext( FLA_Obj F, dim_t depth, dim_t* b_m, dim_t* b_n, FLA_Obj* H );
+FLA_Error     FLASH_Obj_create_flat_copy_of_hier( FLA_Obj H, FLA_Obj* F );
+void          FLASH_Obj_free( FLA_Obj* H );
+FLA_Error     FLASH_Obj_flatten( FLA_Obj H, FLA_Obj F );
+FLA_Error     FLASH_Obj_hierarchify( FLA_Obj F, FLA_Obj H );
+/* src/base/flamec/hierarchy/main/FLASH_Copy_other.c:81-136 */
+FLA_Error     FLASH_Copy_flat_to_hier( FLA_Obj F, dim_t i, dim_t j, FLA_Obj H );
+FLA_Error     FLASH_Copy_hier_to_flat( dim_t i, dim_t j, FLA_Obj H, FLA_Obj F );
+/* src/base/flamec/hierarchy/main/FLASH_View.c:600-690 */
+dim_t         FLASH_Obj_scalar_length( FLA_Obj H );
+dim_t         FLASH_Obj_scalar_width( FLA_Obj H );
+dim_t         FLASH_Obj_scalar_min_dim( FLA_Obj H );
+dim_t         FLASH_Obj_scalar_max_dim( FLA_Obj H );
+/* src/lapack/dec/chol/front/flamec/FLASH_Chol.c:15-30, FLASH_Chol_solve.c */
+FLA_Error     FLASH_Chol( FLA_Uplo uplo, FLA_Obj A );
+FLA_Error     FLASH_Chol_solve( FLA_Uplo uplo, FLA_Obj A, FLA_Obj B, FLA_Obj X );
+/* src/lapack/dec/lu/piv/front/flamec/FLASH_LU_piv.c:15-41, FLASH_LU_piv_solve.c;
+ * p hierarchical (one column of blocks) or flat, relative pivots as FLA_LU_piv */
+FLA_Error     FLASH_LU_piv( FLA_Obj A, FLA_Obj p );
+FLA_Error     FLASH_LU_piv_solve( FLA_Obj A, FLA_Obj p, FLA_Obj B, FLA_Obj X );
+/* src/lapack/dec/q/qrut/front/flamec/FLASH_QR_UT.c, FLASH_QR_UT_create_hier_matrices.c,
+ * FLASH_QR_UT_solve.c: TW min_dim x min_dim with square b_flash blocks
+ * (b_alg == b_flash, min_dim(A) % b_flash == 0); block column q's T in TW's
+ * diagonal block (q, q), as the reference's algorithm-by-blocks stores it */
+FLA_Error     FLASH_QR_UT_create_hier_matrices( FLA_Obj A_flat, dim_t depth, dim_t* b_flash, FLA_Obj* A,
+                                                FLA_Obj* TW );
+FLA_Error     FLASH_QR_UT( FLA_Obj A, FLA_Obj TW );
+FLA_Error     FLASH_QR_UT_solve( FLA_Obj A, FLA_Obj TW, FLA_Obj B, FLA_Obj X );
+/* src/lapack/util/app/qut/front/flamec/FLASH_Apply_Q_UT.c, FLASH_Apply_Q_UT_create_workspace.c */
+FLA_Error     FLASH_Apply_Q_UT( FLA_Side side, FLA_Trans trans, FLA_Direct direct, FLA_Store storev,
+                                FLA_Obj A, FLA_Obj TW, FLA_Obj W, FLA_Obj B );
+FLA_Error     FLASH_Apply_Q_UT_create_workspace( FLA_Obj TW, FLA_Obj B, FLA_Obj* W );
+
 #ifdef __cplusplus
 }
 #endif

@@ -101,6 +101,35 @@ _SIGS = {
                                                C.c_void_p, C.c_void_p, C.c_void_p]),
     "FLA_Chol_adjoint_batched": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]),
     "FLA_B200_batched_tune": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "FLASH_Obj_depth": (C.c_ulong, [FLA_Obj]),
+    "FLASH_Obj_blocksizes": (C.c_ulong, [FLA_Obj, C.POINTER(C.c_ulong), C.POINTER(C.c_ulong)]),
+    "FLASH_Obj_create": (C.c_int, [C.c_int, C.c_ulong, C.c_ulong, C.c_ulong, C.POINTER(C.c_ulong),
+                                   C.POINTER(FLA_Obj)]),
+    "FLASH_Obj_create_ext": (C.c_int, [C.c_int, C.c_ulong, C.c_ulong, C.c_ulong, C.POINTER(C.c_ulong),
+                                       C.POINTER(C.c_ulong), C.POINTER(FLA_Obj)]),
+    "FLASH_Obj_create_hier_copy_of_flat": (C.c_int, [FLA_Obj, C.c_ulong, C.POINTER(C.c_ulong), C.POINTER(FLA_Obj)]),
+    "FLASH_Obj_create_hier_copy_of_flat_ext": (C.c_int, [FLA_Obj, C.c_ulong, C.POINTER(C.c_ulong),
+                                                         C.POINTER(C.c_ulong), C.POINTER(FLA_Obj)]),
+    "FLASH_Obj_create_flat_copy_of_hier": (C.c_int, [FLA_Obj, C.POINTER(FLA_Obj)]),
+    "FLASH_Obj_free": (None, [C.POINTER(FLA_Obj)]),
+    "FLASH_Obj_flatten": (C.c_int, [FLA_Obj, FLA_Obj]),
+    "FLASH_Obj_hierarchify": (C.c_int, [FLA_Obj, FLA_Obj]),
+    "FLASH_Copy_flat_to_hier": (C.c_int, [FLA_Obj, C.c_ulong, C.c_ulong, FLA_Obj]),
+    "FLASH_Copy_hier_to_flat": (C.c_int, [C.c_ulong, C.c_ulong, FLA_Obj, FLA_Obj]),
+    "FLASH_Obj_scalar_length": (C.c_ulong, [FLA_Obj]),
+    "FLASH_Obj_scalar_width": (C.c_ulong, [FLA_Obj]),
+    "FLASH_Obj_scalar_min_dim": (C.c_ulong, [FLA_Obj]),
+    "FLASH_Obj_scalar_max_dim": (C.c_ulong, [FLA_Obj]),
+    "FLASH_Chol": (C.c_int, [C.c_int, FLA_Obj]),
+    "FLASH_Chol_solve": (C.c_int, [C.c_int, FLA_Obj, FLA_Obj, FLA_Obj]),
+    "FLASH_LU_piv": (C.c_int, [FLA_Obj, FLA_Obj]),
+    "FLASH_LU_piv_solve": (C.c_int, [FLA_Obj, FLA_Obj, FLA_Obj, FLA_Obj]),
+    "FLASH_QR_UT_create_hier_matrices": (C.c_int, [FLA_Obj, C.c_ulong, C.POINTER(C.c_ulong), C.POINTER(FLA_Obj),
+                                                   C.POINTER(FLA_Obj)]),
+    "FLASH_QR_UT": (C.c_int, [FLA_Obj, FLA_Obj]),
+    "FLASH_QR_UT_solve": (C.c_int, [FLA_Obj, FLA_Obj, FLA_Obj, FLA_Obj]),
+    "FLASH_Apply_Q_UT": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, FLA_Obj, FLA_Obj, FLA_Obj, FLA_Obj]),
+    "FLASH_Apply_Q_UT_create_workspace": (C.c_int, [FLA_Obj, FLA_Obj, C.POINTER(FLA_Obj)]),
     "FLA_B200_batched_nb": (C.c_int, [C.c_int, C.c_int, C.c_int]),
     "FLA_Chol_adjoint": (C.c_int, [C.c_int, FLA_Obj, FLA_Obj]),
     "FLA_B200_Chol_logdet_adjoint": (C.c_int, [FLA_Obj, FLA_Obj, C.c_double, C.POINTER(C.c_double)]),

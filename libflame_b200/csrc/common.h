@@ -109,6 +109,10 @@ enum WsSlot : int {
   WS_QR_U,          //   unit lower trapezoids of the panel recursion
   WS_QR_W,          //   its W products
   WS_ADJ,           // per-stream scratch of the batched Cholesky adjoint
+  WS_FLASH0,        // column-major copies of hierarchical (FLASH) operands
+  WS_FLASH1,
+  WS_FLASH2,
+  WS_FLASH3,
   WS_PANEL_T,       // transposed copies of Cholesky panels (two, ping-pong)
   WS_SWEEP,         // ready flags of the one-launch triangular sweeps
   WS_NSLOTS

@@ -249,7 +249,7 @@ int dpotri_(char* uplo, int* n, double* a, int* lda, int* info) {
   FLA_Base_obj base;
   std::memset(&base, 0, sizeof(base));
   base.datatype = FLA_DOUBLE;
-  base.elemtype = FLA_MATRIX;
+  base.elemtype = FLA_SCALAR;
   base.m = base.n = (dim_t)*n;
   base.rs = 1;
   base.cs = (dim_t)*lda;

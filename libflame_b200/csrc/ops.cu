@@ -327,7 +327,7 @@ static int xerbla(const char* name, int pos, int* info) {
 static FLA_Obj raw_obj(FLA_Datatype dt, void* buf, long m, long n, long ld, FLA_Base_obj* base) {
   std::memset(base, 0, sizeof(*base));
   base->datatype = dt;
-  base->elemtype = FLA_MATRIX;
+  base->elemtype = FLA_SCALAR;
   base->m = (dim_t)m;
   base->n = (dim_t)n;
   base->rs = 1;

@@ -569,7 +569,7 @@ int dgeqrf_(int* m, int* n, double* a, int* lda, double* tau, double* work, int*
   FLA_Base_obj ba;
   std::memset(&ba, 0, sizeof(ba));
   ba.datatype = FLA_DOUBLE;
-  ba.elemtype = FLA_MATRIX;
+  ba.elemtype = FLA_SCALAR;
   ba.m = *m;
   ba.n = *n;
   ba.rs = 1;

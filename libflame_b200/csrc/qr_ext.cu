@@ -267,7 +267,7 @@ int xerbla_ret(const char* name, int* info) {
 FLA_Obj raw(void* buf, long m, long n, long ld, FLA_Base_obj* base) {
   std::memset(base, 0, sizeof(*base));
   base->datatype = FLA_DOUBLE;
-  base->elemtype = FLA_MATRIX;
+  base->elemtype = FLA_SCALAR;
   base->m = (dim_t)m;
   base->n = (dim_t)n;
   base->rs = 1;

@@ -376,7 +376,7 @@ int FLA_B200_num_sms(void) { return ctx().num_sms; }
 static void obj_init_base(FLA_Base_obj* b, FLA_Datatype dt, dim_t m, dim_t n) {
   std::memset(b, 0, sizeof(*b));
   b->datatype = dt;
-  b->elemtype = FLA_MATRIX;
+  b->elemtype = FLA_SCALAR;  // flat (FLA_Obj.c:57); FLA_MATRIX marks hierarchical objects
   b->m = m;
   b->n = n;
   b->m_inner = m;
