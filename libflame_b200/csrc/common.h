@@ -243,6 +243,9 @@ int transpose_dev(const double* src, long lds, double* dst, long ldd, long m, lo
 // Row interchanges on a matrix stored transposed (AT = A^T, column-major):
 // rows row0+i and row0+i+piv[i] of A (columns of AT) are exchanged, in
 // order, over the A-columns [c0, c0+n0) and [c1, c1+n1) (rows of AT).
+// U12 := inv(L11) A12 (unit lower L11 of order b) on transposed storage:
+// L11(i, j) at Ls[j + i ld], A12(i, c) at X[c + i ld] (c < ncols), overwritten.
+int u12_subst(const double* Ls, double* X, long ld, int b, long ncols, cudaStream_t st);
 int laswp_t_dev(double* AT, long ldt, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
                 cudaStream_t st);
 int laswp_t_f32(float* AT, long ldt, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,

@@ -7,8 +7,8 @@
 //   for each block of nb columns:
 //     [A11;A21], p1 := LU_piv([A11;A21])   lu_panel_factor (lu_panel.cu)
 //     pivot [A10;A20] and [A12;A22]         laswp_compose/apply kernels
-//     A12 := inv(tril_unit(A11)) A12         blocked: 32 x 32 diagonal-block
-//                                            inverses + DMMA GEMMs (u12_solve)
+//     A12 := inv(tril_unit(A11)) A12         forward substitution, one launch
+//                                            (u12_subst_kernel)
 //     A22 -= A21 A12                         DMMA GEMM engine
 // run on the transposed matrix, with the next panel factored on a second
 // stream while the trailing update runs (lu_piv_dev below).  Pivot choice is the reference's: the entry of
@@ -29,6 +29,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "common.h"
@@ -39,7 +40,6 @@ namespace fb {
 namespace {
 
 constexpr int PANEL_THREADS = 256;
-constexpr int U12_BS = 32;  // diagonal blocks of L11 inverted for the U12 solve
 constexpr int NBMAX = 128;
 constexpr size_t PANEL_SMEM_CAP = 200 * 1024;
 
@@ -213,9 +213,11 @@ __device__ void laswp_compose(const int* __restrict__ piv, int npiv, int reverse
     if (t < npiv) {
       slot = t;
     } else {
-      int first = i;  // first interchange with the same far target owns the slot
-      for (int i2 = 0; i2 < i; ++i2)
-        if (i2 + s_piv[i2] == t) { first = i2; break; }
+      // the first interchange with the same far target owns the slot
+      // (branch-free scan: the loads of the unrolled loop overlap)
+      int first = i;
+#pragma unroll 8
+      for (int i2 = i - 1; i2 >= 0; --i2) first = (i2 + s_piv[i2] == t) ? i2 : first;
       slot = npiv + first;
       if (first == i) s_row[slot] = t;
     }
@@ -540,35 +542,122 @@ int lu_blocksize() {
 // of AT and every interchange moves contiguous pieces; A is transposed in
 // at the start and back at the end (two streaming passes).
 //
-//   main stream, step k:  row interchanges of panel k left and right of it;
-//                         U12^T := A12^T inv(L11)^T as a DMMA GEMM
-//                         (inv(L11)^T = inv(L11^T) was formed next to the
-//                         panel);
+//   main stream, step k:  the next panel's columns only: row interchanges
+//                         of panel k, U12 (substitution), lookahead update
 //                         A22^T(next panel rows) -= U12^T(next) A21^T;
 //   side stream:          factor the next panel (cluster leaves, recursive
-//                         split) and invert its triangle;
-//   main stream:          A22^T(rest) -= U12^T(rest) A21^T, concurrently;
+//                         split);
+//   main stream:          concurrently, the other columns: interchanges
+//                         left of panel k and right of the next panel,
+//                         their U12 and A22^T(rest) -= U12^T(rest) A21^T;
 //                         then wait for the side stream.
-// The side stream has the higher priority, so the panel's CTAs are placed
-// as soon as trailing-update CTAs retire.
-// U12 := inv(L11) A12 on the transposed storage, blocked by U12_BS columns:
-// with T = L11^T (upper, unit; the b x b block at Ts, ld ldt), Y := X
-// inv(T) solves Y_0 = X_0 inv(T_00), Y_1 = (X_1 - Y_0 T_01) inv(T_11), ...
-// (X = A12^T, nr x b at W, ld ldw, overwritten; Y to Yout, ld ldy).  Inv
-// holds inv(T_jj) for the U12_BS x U12_BS diagonal blocks (ld U12_BS).
-// Inverting only these small, well-conditioned blocks keeps the solve as
-// backward stable as substitution; one explicit inverse of the whole of
-// L11 raises the factorization's backward error by about a sixth.
-int u12_solve(const double* Ts, long ldt, double* W, long ldw, const double* Inv, double* Yout, long ldy, long nr,
-              int b, cudaStream_t st) {
-  for (int c0 = 0; c0 < b; c0 += U12_BS) {
-    const int w = std::min(U12_BS, b - c0);
-    if (gemm_f64(st, false, false, nr, w, w, 1.0, W + (long)c0 * ldw, ldw, Inv + (long)(c0 / U12_BS) * U12_BS * U12_BS,
-                 U12_BS, 0.0, Yout + (long)c0 * ldy, ldy) != FLA_SUCCESS)
-      return FLA_FAILURE;
-    const int rest = b - c0 - w;
-    if (rest > 0 && gemm_f64(st, false, false, nr, rest, w, -1.0, Yout + (long)c0 * ldy, ldy,
-                             Ts + c0 + (long)(c0 + w) * ldt, ldt, 1.0, W + (long)(c0 + w) * ldw, ldw) != FLA_SUCCESS)
+// Only three launches stand between the end of one panel and the start of
+// the next.  The side stream has the higher priority, so the panel's CTAs
+// are placed as soon as trailing-update CTAs retire.
+// U12 := inv(L11) A12 on the transposed storage by forward substitution,
+// the order of dtrsm's left, lower, no-transpose, unit case
+// (src/flablas/f2c/dtrsm.c): for j = 0..b-1, rows i > j of every column c
+// lose L11(i, j) U12(j, c).  L11(i, j) is at Ls[j + i ld] (row i of L11 is
+// a contiguous column of A^T), A12(i, c) at X[c + i ld], overwritten.
+// The triangle (b <= 128) sits in shared memory; one warp per RV columns c
+// keeps rows lane, lane+32, lane+64, lane+96 of them in registers, and at
+// step j the owner lane broadcasts U12(j, c): no block barrier inside the
+// sweep, so a step costs one shuffle and a few FMAs of latency.
+constexpr int U12_WARPS = 16;
+constexpr int U12_LDS = NBMAX + 1;  // odd stride: a half-warp reads 16 banks
+// shared memory for a triangle of order b: whole 32-row groups (the sweep
+// reads the rows of every group it touches)
+inline size_t u12_smem(int b) { return sizeof(double) * (size_t)((b + 31) & ~31) * U12_LDS; }
+
+template <int RV>
+__global__ void __launch_bounds__(U12_WARPS * 32) u12_subst_kernel(const double* __restrict__ Ls,
+                                                                    double* __restrict__ X, long ld, int b,
+                                                                    int ncols) {
+  extern __shared__ double sL[];  // sL[i * U12_LDS + j] = L11(i, j), rows i < 32 ceil(b / 32)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i = warp; i < b; i += U12_WARPS)
+    for (int j = lane; j < b; j += 32) sL[i * U12_LDS + j] = Ls[j + (long)i * ld];
+  __syncthreads();
+  const int c0 = (blockIdx.x * U12_WARPS + warp) * RV;
+  if (c0 >= ncols) return;
+  double r[4][RV];
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int v = 0; v < RV; ++v) {
+      const int i = lane + 32 * m, c = c0 + v;
+      r[m][v] = (i < b && c < ncols) ? X[c + (long)i * ld] : 0.0;
+    }
+  // rows at or beyond b hold zeros and read unset shared memory of their
+  // group: they are never written back; groups at or beyond b are skipped
+  const int groups = (b + 31) >> 5;
+#pragma unroll
+  for (int slot = 0; slot < 4; ++slot) {
+    if (slot >= groups) break;
+    const int jend = min(32, b - 32 * slot);
+    for (int jj = 0; jj < jend; ++jj) {
+      const int j = 32 * slot + jj;
+      double y[RV];
+#pragma unroll
+      for (int v = 0; v < RV; ++v) y[v] = __shfl_sync(0xffffffffu, r[slot][v], jj);
+      const double l0 = sL[(lane + 32 * slot) * U12_LDS + j];
+      if (lane > jj) {
+#pragma unroll
+        for (int v = 0; v < RV; ++v) r[slot][v] = fma(-l0, y[v], r[slot][v]);
+      }
+#pragma unroll
+      for (int m = slot + 1; m < 4; ++m) {
+        if (m < groups) {
+          const double l = sL[(lane + 32 * m) * U12_LDS + j];
+#pragma unroll
+          for (int v = 0; v < RV; ++v) r[m][v] = fma(-l, y[v], r[m][v]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int v = 0; v < RV; ++v) {
+      const int i = lane + 32 * m, c = c0 + v;
+      if (i < b && c < ncols) X[c + (long)i * ld] = r[m][v];
+    }
+}
+
+template <int RV>
+void u12_subst_launch(const double* Ls, double* X, long ld, int b, int ncols, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(u12_subst_kernel<RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)u12_smem(NBMAX));
+    attr = true;
+  }
+  const unsigned grid = (unsigned)((ncols + U12_WARPS * RV - 1) / (U12_WARPS * RV));
+  u12_subst_kernel<RV><<<grid, U12_WARPS * 32, u12_smem(b), st>>>(Ls, X, ld, b, ncols);
+}
+
+// U12 := inv(L11) A12 for ncols columns (layout above), any b: blocks of
+// 128 rows, each solved by the kernel, the rows below updated by a GEMM.
+// Columns per warp grow with ncols so that the grid stays about one wave
+// (a 128-row triangle's 132 KB of shared memory allow one CTA per SM).
+int u12_subst(const double* Ls, double* X, long ld, int b, long ncols, cudaStream_t st) {
+  if (ncols <= 0 || b <= 0) return FLA_SUCCESS;
+  const int sms = ctx().num_sms;
+  for (int r0 = 0; r0 < b; r0 += NBMAX) {
+    const int bb = std::min(NBMAX, b - r0);
+    const double* L = Ls + r0 + (long)r0 * ld;
+    double* Y = X + (long)r0 * ld;
+    const int ps = prof_begin(st);
+    if (ncols <= (long)sms * U12_WARPS) u12_subst_launch<1>(L, Y, ld, bb, (int)ncols, st);
+    else if (ncols <= (long)sms * U12_WARPS * 2) u12_subst_launch<2>(L, Y, ld, bb, (int)ncols, st);
+    else if (ncols <= (long)sms * U12_WARPS * 4) u12_subst_launch<4>(L, Y, ld, bb, (int)ncols, st);
+    else u12_subst_launch<8>(L, Y, ld, bb, (int)ncols, st);
+    prof_end(ps, st, PROF_TRSM, (double)ncols * bb * bb);
+    count_launch();
+    FB_CK(cudaGetLastError());
+    const int rest = b - r0 - bb;
+    // U12^T[:, r0+bb:] -= U12^T[:, r0:r0+bb] L11^T[r0:r0+bb, r0+bb:]
+    if (rest > 0 && gemm_f64(st, false, false, ncols, rest, bb, -1.0, Y, ld, Ls + r0 + (long)(r0 + bb) * ld, ld,
+                             1.0, X + (long)(r0 + bb) * ld, ld) != FLA_SUCCESS)
       return FLA_FAILURE;
   }
   return FLA_SUCCESS;
@@ -585,11 +674,7 @@ int lu_piv_dev(DMat A, int* d_piv, int* info) {
   const int NBL = (int)std::min<long>(lu_blocksize(), mn);
   const long ldT = even(n);
   double* AT = (double*)ws_get(WS_REPACK, sizeof(double) * (size_t)ldT * (size_t)m);
-  // inverted U12_BS x U12_BS diagonal blocks of L11, each at stride U12_BS^2
-  const size_t xblocks = (size_t)(NBL + U12_BS - 1) / U12_BS;
-  double* X = (double*)ws_get(WS_MISC, sizeof(double) * xblocks * U12_BS * U12_BS);
-  double* W = (double*)ws_get(WS_MISC2, sizeof(double) * (size_t)(NBL + 1) * (size_t)even(n));
-  if (!AT || !X || !W) return FLA_FAILURE;
+  if (!AT) return FLA_FAILURE;
   if (status_reset() != FLA_SUCCESS) return FLA_FAILURE;
   cudaEvent_t ev_look = cx.ev[0], ev_panel = cx.ev[1];
   // element (i, j) of A inside AT
@@ -600,6 +685,7 @@ int lu_piv_dev(DMat A, int* d_piv, int* info) {
   // lookahead done, trailing update done; side stream: panel done), summed
   // and printed to stderr after the factorization
   static const bool trace = std::getenv("FLA_B200_LU_TRACE") != nullptr;
+  static const bool trace_all = trace && std::string(std::getenv("FLA_B200_LU_TRACE")) == "all";
   std::vector<cudaEvent_t> tev;
   auto tmark = [&](cudaStream_t s) {
     if (!trace) return;
@@ -608,51 +694,62 @@ int lu_piv_dev(DMat A, int* d_piv, int* info) {
     cudaEventRecord(e, s);
     tev.push_back(e);
   };
-  // first panel and its inverse triangle, on the main stream
+  auto tdrop = [&](size_t keep) {  // an incomplete step is not traced
+    for (size_t q = keep; q < tev.size(); ++q) cudaEventDestroy(tev[q]);
+    tev.resize(std::min(keep, tev.size()));
+  };
+  // first panel, on the main stream
   {
     const int b = (int)std::min<long>(NBL, mn);
     if (lu_panel_factor_t(AT, ldT, m, b, d_piv, 0, st) != FLA_SUCCESS) return FLA_FAILURE;
-    if (n > b && tri_inverse_blocks_bs(AT, ldT, b, U12_BS, false, true, X, st) != FLA_SUCCESS) return FLA_FAILURE;
   }
   for (long k = 0; k < mn; k += NBL) {
     const int b = (int)std::min<long>(NBL, mn - k);
     const long nr = n - k - b, m2 = m - k - b;
     const size_t tbase = tev.size();
     tmark(st);
-    if (laswp_t_dev(AT, ldT, (int)k, d_piv + k, b, 0, (int)k, (int)(k + b), (int)nr, st) != FLA_SUCCESS)
-      return FLA_FAILURE;
-    if (nr <= 0) continue;
-    // U12^T := A12^T inv(L11^T): A12^T is the nr x b block at t_at(k, k + b)
-    FB_CK(cudaMemcpy2DAsync(W, sizeof(double) * even(nr), t_at(k, k + b), sizeof(double) * ldT,
-                            sizeof(double) * nr, b, cudaMemcpyDeviceToDevice, st));
-    if (u12_solve(t_at(k, k), ldT, W, even(nr), X, t_at(k, k + b), ldT, nr, b, st) != FLA_SUCCESS)
-      return FLA_FAILURE;
-    if (m2 <= 0) continue;
-    const int nb2 = (int)std::min<long>(NBL, mn - k - b);  // next panel's width (0: none)
-    if (nb2 > 0) {
-      if (gemm_f64(st, false, false, nb2, m2, b, -1.0, t_at(k, k + b), ldT, t_at(k + b, k), ldT, 1.0,
-                   t_at(k + b, k + b), ldT) != FLA_SUCCESS)
+    // next panel's width (0: none); its columns go first, the rest of the
+    // step's work runs on this stream while the side stream factors it
+    const int nb2 = (nr > 0 && m2 > 0) ? (int)std::min<long>(NBL, mn - k - b) : 0;
+    if (nb2 == 0) {
+      if (laswp_t_dev(AT, ldT, (int)k, d_piv + k, b, 0, (int)k, (int)(k + b), (int)nr, st) != FLA_SUCCESS)
         return FLA_FAILURE;
-      FB_CK(cudaEventRecord(ev_look, st));
-      tmark(st);
-      FB_CK(cudaStreamWaitEvent(sd, ev_look, 0));
-      if (lu_panel_factor_t(t_at(k + b, k + b), ldT, m2, nb2, d_piv + k + b, (int)(k + b), sd) != FLA_SUCCESS)
-        return FLA_FAILURE;
-      if (nr > nb2 &&
-          tri_inverse_blocks_bs(t_at(k + b, k + b), ldT, nb2, U12_BS, false, true, X, sd) != FLA_SUCCESS)
-        return FLA_FAILURE;
-      FB_CK(cudaEventRecord(ev_panel, sd));
-      tmark(sd);
+      if (nr <= 0) {
+        tdrop(tbase);
+        continue;
+      }
+      if (u12_subst(t_at(k, k), t_at(k, k + b), ldT, b, nr, st) != FLA_SUCCESS) return FLA_FAILURE;
+      tdrop(tbase);
+      continue;
     }
+    // the next panel's columns: interchanges, U12, lookahead update
+    if (laswp_t_dev(AT, ldT, (int)k, d_piv + k, b, (int)(k + b), nb2, 0, 0, st) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    if (u12_subst(t_at(k, k), t_at(k, k + b), ldT, b, nb2, st) != FLA_SUCCESS) return FLA_FAILURE;
+    if (gemm_f64(st, false, false, nb2, m2, b, -1.0, t_at(k, k + b), ldT, t_at(k + b, k), ldT, 1.0,
+                 t_at(k + b, k + b), ldT) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    FB_CK(cudaEventRecord(ev_look, st));
+    tmark(st);
+    FB_CK(cudaStreamWaitEvent(sd, ev_look, 0));
+    if (lu_panel_factor_t(t_at(k + b, k + b), ldT, m2, nb2, d_piv + k + b, (int)(k + b), sd) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    FB_CK(cudaEventRecord(ev_panel, sd));
+    tmark(sd);
+    // the rest, beside the panel: interchanges left of the panel and right of
+    // the next one (disjoint from the columns the side stream works on),
+    // U12 of the remaining columns, trailing update
+    if (laswp_t_dev(AT, ldT, (int)k, d_piv + k, b, 0, (int)k, (int)(k + b + nb2), (int)(nr - nb2), st) !=
+        FLA_SUCCESS)
+      return FLA_FAILURE;
+    if (u12_subst(t_at(k, k), t_at(k, k + b + nb2), ldT, b, nr - nb2, st) != FLA_SUCCESS) return FLA_FAILURE;
     if (nr > nb2 &&
         gemm_f64(st, false, false, nr - nb2, m2, b, -1.0, t_at(k, k + b + nb2), ldT, t_at(k + b, k), ldT, 1.0,
                  t_at(k + b, k + b + nb2), ldT) != FLA_SUCCESS)
       return FLA_FAILURE;
-    if (nb2 > 0) {
-      tmark(st);
-      if (tev.size() != tbase + 4) tev.resize(tbase);  // incomplete step: not traced
-    }
-    if (nb2 > 0) FB_CK(cudaStreamWaitEvent(st, ev_panel, 0));
+    tmark(st);
+    if (tev.size() != tbase + 4) tdrop(tbase);
+    FB_CK(cudaStreamWaitEvent(st, ev_panel, 0));
   }
   if (transpose_dev(AT, ldT, A.p, A.ld, n, m, false, st) != FLA_SUCCESS) return FLA_FAILURE;
   const int rs = status_read(info);
@@ -671,7 +768,7 @@ int lu_piv_dev(DMat A, int* d_piv, int* info) {
       trail += t;
       crit += a + std::max(p, t);
       if (p > t) ++panel_bound;
-      if (q % 16 == 0 || q + 1 == steps)
+      if (trace_all || q % 16 == 0 || q + 1 == steps)
         std::fprintf(stderr, "libflame_b200 lu: step %4zu  lookahead %.3f ms  panel %.3f ms  trailing %.3f ms\n", q, a, p,
                      t);
     }

@@ -866,8 +866,8 @@ int lu_panel_factor_t(double* P, long ld, long M, int w, int* d_piv, int gcol, c
   const int w2 = w - w1;
   if (lu_panel_factor_t(P, ld, M, w1, d_piv, gcol, st) != FLA_SUCCESS) return FLA_FAILURE;
   if (laswp_t_dev(P, ld, 0, d_piv, w1, w1, w2, 0, 0, st) != FLA_SUCCESS) return FLA_FAILURE;
-  // U12^T (w2 x w1 at P + w1): each row y solves L11 y = x
-  if (trsm_right_block(P, ld, P + w1, ld, w2, w1, false, true, true, st) != FLA_SUCCESS) return FLA_FAILURE;
+  // U12 := inv(L11) U12 (U12^T is the w2 x w1 block at P + w1)
+  if (u12_subst(P, P + w1, ld, w1, w2, st) != FLA_SUCCESS) return FLA_FAILURE;
   if (M > w1) {
     if (gemm_f64(st, false, false, w2, M - w1, w1, -1.0, P + w1, ld, P + (long)w1 * ld, ld, 1.0,
                  P + w1 + (long)w1 * ld, ld) != FLA_SUCCESS)
