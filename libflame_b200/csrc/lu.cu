@@ -672,6 +672,20 @@ int lu_piv_dev(DMat A, int* d_piv, int* info) {
   if (mn == 0) return FLA_SUCCESS;
   auto even = [](long x) { return (x + 1) & ~1L; };  // TMA: 16-byte leading dimensions
   const int NBL = (int)std::min<long>(lu_blocksize(), mn);
+  // Width of the panel starting at column k: twice NBL while more than
+  // wide_rows rows remain (the trailing updates dominate there, and K = 2 NBL
+  // halves each update tile's fixed cost), NBL after (the panels dominate;
+  // at n = 16384 that is the last ~8000 rows, and an n = 8192 factorization
+  // is panel-bound from the start).  FLA_B200_LU_WIDE_ROWS overrides it.
+  static const long wide_rows = [] {
+    long v = 8192;
+    if (const char* e = std::getenv("FLA_B200_LU_WIDE_ROWS")) v = std::atol(e);
+    return v;
+  }();
+  auto width = [&](long k) -> int {
+    const int w = (NBL <= 128 && m - k > wide_rows) ? 2 * NBL : NBL;
+    return (int)std::min<long>(w, mn - k);
+  };
   const long ldT = even(n);
   double* AT = (double*)ws_get(WS_REPACK, sizeof(double) * (size_t)ldT * (size_t)m);
   if (!AT) return FLA_FAILURE;
@@ -700,17 +714,17 @@ int lu_piv_dev(DMat A, int* d_piv, int* info) {
   };
   // first panel, on the main stream
   {
-    const int b = (int)std::min<long>(NBL, mn);
+    const int b = width(0);
     if (lu_panel_factor_t(AT, ldT, m, b, d_piv, 0, st) != FLA_SUCCESS) return FLA_FAILURE;
   }
-  for (long k = 0; k < mn; k += NBL) {
-    const int b = (int)std::min<long>(NBL, mn - k);
+  for (long k = 0, b = 0; k < mn; k += b) {
+    b = width(k);
     const long nr = n - k - b, m2 = m - k - b;
     const size_t tbase = tev.size();
     tmark(st);
     // next panel's width (0: none); its columns go first, the rest of the
     // step's work runs on this stream while the side stream factors it
-    const int nb2 = (nr > 0 && m2 > 0) ? (int)std::min<long>(NBL, mn - k - b) : 0;
+    const int nb2 = (nr > 0 && m2 > 0 && k + b < mn) ? width(k + b) : 0;
     if (nb2 == 0) {
       if (laswp_t_dev(AT, ldT, (int)k, d_piv + k, b, 0, (int)k, (int)(k + b), (int)nr, st) != FLA_SUCCESS)
         return FLA_FAILURE;
