@@ -59,6 +59,9 @@ struct LeafArgs {
   int* piv;    // out: w relative pivots
   int* info;   // atomicMin of the first zero-pivot column
   int* err;    // wait-timeout flag (register-resident leaf)
+  int pl, pr;  // register-resident leaf: columns of the enclosing panel left
+               // of the leaf and right of it, which receive the leaf's row
+               // interchanges at its end (0, 0: none)
 };
 
 // Shared-memory layout of one CTA (doubles unless noted):
@@ -480,6 +483,67 @@ __device__ __forceinline__ void rleaf_column_at(int j, double (&rv)[RPT][W], int
   }
 }
 
+// The leaf's row interchanges (row j <-> row s_r[j], j = 0..W-1, in order)
+// applied to the other columns of the enclosing panel: pl columns left of
+// the leaf and pr right of it (FLA_Apply_pivots on A10/A12 of the panel
+// recursion, done here instead of by separate launches).  The interchanges
+// move at most 2W rows: the W leaf rows and the distinct far targets.  Their
+// composition (the row that ends in each slot) is formed once; each CTA of
+// the cluster then gathers its share of the columns for those rows into
+// shared memory and writes them back permuted.  The leaf's own columns are
+// not touched, so no CTA waits for another.
+template <int W>
+__device__ void rleaf_apply_pivots(const LeafArgs& a, const int* s_r, int c, int C, double* buf) {
+  __shared__ int s_tgt[W];       // slot receiving row j's interchange partner
+  __shared__ int s_row[2 * W];   // leaf-relative row of each slot (-1: unused)
+  __shared__ int s_src[2 * W];   // slot whose original row ends in this slot
+  const int tid = threadIdx.x;
+  __syncthreads();  // s_r complete
+  for (int q = tid; q < 2 * W; q += blockDim.x) s_row[q] = q < W ? q : -1;
+  __syncthreads();
+  if (tid < W) {
+    const int t = s_r[tid];
+    int slot = t;
+    if (t >= W) {  // far target: the first interchange with it owns the slot
+      int first = tid;
+      for (int i2 = tid - 1; i2 >= 0; --i2) first = s_r[i2] == t ? i2 : first;
+      slot = W + first;
+      if (first == tid) s_row[slot] = t;
+    }
+    s_tgt[tid] = slot;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int q = 0; q < 2 * W; ++q) s_src[q] = q;
+    for (int i = 0; i < W; ++i) {
+      const int b = s_tgt[i];
+      const int x = s_src[i];
+      s_src[i] = s_src[b];
+      s_src[b] = x;
+    }
+  }
+  __syncthreads();
+  const int tot = a.pl + a.pr;
+  const int per = (tot + C - 1) / C;
+  const int cb = c * per, ce = min(tot, cb + per);
+  const int cap = (RLEAF_NW * 32 * (W + 1)) / (2 * W);  // columns per pass
+  for (int c0 = cb; c0 < ce; c0 += cap) {
+    const int n = min(cap, ce - c0);
+    for (int e = tid; e < 2 * W * n; e += blockDim.x) {
+      const int q = e / n, t = e - q * n;
+      const int col = (c0 + t) < a.pl ? (c0 + t) - a.pl : W + (c0 + t - a.pl);
+      if (s_row[q] >= 0) buf[e] = a.P[col + (long)s_row[q] * a.ld];
+    }
+    __syncthreads();
+    for (int e = tid; e < 2 * W * n; e += blockDim.x) {
+      const int q = e / n, t = e - q * n;
+      const int col = (c0 + t) < a.pl ? (c0 + t) - a.pl : W + (c0 + t - a.pl);
+      if (s_row[q] >= 0 && s_src[q] != q) a.P[col + (long)s_row[q] * a.ld] = buf[s_src[q] * n + t];
+    }
+    __syncthreads();
+  }
+}
+
 template <int W, int RPT>
 __global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs a) {
   using Slot = RSlot<W>;
@@ -504,6 +568,8 @@ __global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs 
   }
 
   double* tile = reinterpret_cast<double*>(rleaf_smem + rleaf_tile_offset(W, C)) + warp * 32 * (W + 1);
+  __shared__ int s_r[W];  // pivot row of every column (leaf-relative)
+  bool done = true;       // uniform in the CTA: false if a wait ran out
   double rv[RPT][W];
   rleaf_load<W, RPT>(rv, a, r0, rows, tile, warp, lane);
   int first_null = -1;
@@ -573,7 +639,10 @@ __global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs 
         ok = mbar_wait_cluster(fullp, ph, a.err, 21);
       }
       // the CTA leaves the loop together if the (bounded) wait ran out
-      if (__syncthreads_or(ok ? 0 : 1)) break;
+      if (__syncthreads_or(ok ? 0 : 1)) {
+        done = false;
+        break;
+      }
       if (warp != 0) (void)mbar_try_wait_cluster(fullp, ph);  // acquire of the completed phase
       const Slot* hs = lane < C ? (lane == c ? best : cslot + par * C + lane) : best;
       unsigned long long gk = lane < C ? hs->key : 0ull;
@@ -595,6 +664,8 @@ __global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs 
     }
     const double piv = u[j];
     if (c == 0 && tid == 0) a.piv[j] = r - j;
+    if (tid == 0) s_r[j] = r;
+    if (tid == 0) s_r[j] = r;
     bv = -1.0;
     bi = INT_MAX;
     bk = 0;
@@ -617,6 +688,7 @@ __global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs 
   }
   rleaf_store<W, RPT>(rv, a, r0, rows, tile, warp, lane);
   if (c == 0 && tid == 0 && first_null >= 0) atomicMin(a.info, a.gcol + first_null);
+  if (done && a.pl + a.pr > 0) rleaf_apply_pivots<W>(a, s_r, c, C, reinterpret_cast<double*>(rleaf_smem + rleaf_tile_offset(W, C)));
   // no CTA leaves while another may still copy into its shared memory
   if (C > 1) cluster.sync();
 }
@@ -708,13 +780,13 @@ bool rleaf_geometry(long M, int w, int* C, int* R) {
   return true;
 }
 
-int rleaf_launch(double* P, long ld, long M, int w, int* d_piv, int gcol, cudaStream_t st) {
+int rleaf_launch(double* P, long ld, long M, int w, int* d_piv, int gcol, cudaStream_t st, int pl = 0, int pr = 0) {
   int C = 0, R = 0;
   if (!rleaf_geometry(M, w, &C, &R)) {
     set_last_error("LU panel leaf does not fit in a cluster");
     return FLA_FAILURE;
   }
-  LeafArgs la;
+  LeafArgs la = {};
   la.P = P;
   la.ld = ld;
   la.M = (int)M;
@@ -725,6 +797,8 @@ int rleaf_launch(double* P, long ld, long M, int w, int* d_piv, int gcol, cudaSt
   la.piv = d_piv;
   la.info = ctx().d_status + ST_INFO;
   la.err = ctx().d_status + ST_ERROR;
+  la.pl = pl;
+  la.pr = pr;
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -790,7 +864,7 @@ int leaf_launch(double* P, long ld, long M, int w, int* d_piv, int gcol, bool rm
     set_last_error("LU panel leaf does not fit in a cluster");
     return FLA_FAILURE;
   }
-  LeafArgs la;
+  LeafArgs la = {};
   la.P = P;
   la.ld = ld;
   la.M = (int)M;
@@ -855,9 +929,43 @@ int lu_panel_factor(double* P, long ld, long M, int w, int* d_piv, int gcol, cud
 // panel at P[i * ld + j]): row interchanges move contiguous pieces of
 // columns of A^T, the top-right solve is a row-wise solve with L11 (held as
 // the upper triangle L11^T), and the update is A22^T -= U12^T A21^T.
+// Panel recursion in which every leaf is register-resident and applies its
+// row interchanges to the other columns of the panel itself (pl columns left
+// of this sub-panel, pr right of it): the joins need no interchange launches.
+int panel_rec_reg(double* P, long ld, long M, int w, int* d_piv, int gcol, int pl, int pr, cudaStream_t st) {
+  int C, R;
+  if (rleaf_geometry(M, w, &C, &R)) return rleaf_launch(P, ld, M, w, d_piv, gcol, st, pl, pr);
+  const int w1 = std::max(8, (w / 2) & ~7);
+  const int w2 = w - w1;
+  if (panel_rec_reg(P, ld, M, w1, d_piv, gcol, pl, pr + w2, st) != FLA_SUCCESS) return FLA_FAILURE;
+  // U12 := inv(L11) U12 (U12^T is the w2 x w1 block at P + w1)
+  if (u12_subst(P, P + w1, ld, w1, w2, st) != FLA_SUCCESS) return FLA_FAILURE;
+  if (M > w1) {
+    if (gemm_f64(st, false, false, w2, M - w1, w1, -1.0, P + w1, ld, P + (long)w1 * ld, ld, 1.0,
+                 P + w1 + (long)w1 * ld, ld) != FLA_SUCCESS)
+      return FLA_FAILURE;
+    if (panel_rec_reg(P + w1 + (long)w1 * ld, ld, M - w1, w2, d_piv + w1, gcol + w1, pl + w1, pr, st) != FLA_SUCCESS)
+      return FLA_FAILURE;
+  }
+  return FLA_SUCCESS;
+}
+
+// True when every leaf of the recursion below (halves rounded down to
+// multiples of 8, leaves of 8, 16 or 32 columns) fits the register leaf:
+// the rows only shrink down the recursion, so the top M decides.
+bool panel_all_reg(long M, int w) {
+  int C, R;
+  if (w % 8 != 0) return false;
+  if (rleaf_geometry(M, w, &C, &R)) return true;
+  if (w <= 32) return false;
+  const int w1 = std::max(8, (w / 2) & ~7);
+  return panel_all_reg(M, w1) && panel_all_reg(M, w - w1);
+}
+
 int lu_panel_factor_t(double* P, long ld, long M, int w, int* d_piv, int gcol, cudaStream_t st) {
   if (leaf_setup() != FLA_SUCCESS) return FLA_FAILURE;
   if (w <= 0 || M <= 0) return FLA_SUCCESS;
+  if (w > 32 && panel_all_reg(M, w)) return panel_rec_reg(P, ld, M, w, d_piv, gcol, 0, 0, st);
   int C, R, lds;
   size_t smem;
   if (rleaf_geometry(M, w, &C, &R)) return rleaf_launch(P, ld, M, w, d_piv, gcol, st);
