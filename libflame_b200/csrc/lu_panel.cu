@@ -301,16 +301,18 @@ __global__ void __launch_bounds__(LEAF_THREADS, 1) lu_leaf_cluster_kernel(LeafAr
 // rank-1 updates never touch memory.  Per column:
 //  1. each warp finds its candidate (largest magnitude, smallest row among
 //     equals) with three redux.sync reductions over a 64-bit ordering key,
-//     and the lane holding it writes the whole row, with the key and row
-//     index, into the warp's slot in shared memory; the owner of row j
-//     writes row j beside them;
-//  2. one CTA barrier; every warp reduces the 16 slot headers the same way
-//     and so knows the CTA's candidate and where its row lies;
-//  3. (clusters only) warp 0 bulk-copies the CTA's candidate slot, and row j
-//     if this CTA owns it, into every other CTA's shared memory, each copy
-//     completing bytes on the receiver's mbarrier; warp 0 waits for the
-//     column's bytes, a second CTA barrier releases the other warps, and
-//     every warp reduces the C candidate headers to the winner;
+//     and the lane holding it writes the key and row index (16 bytes) into
+//     the warp's header in shared memory; the owner of row j writes row j;
+//  2. one CTA barrier; every warp reduces the 16 headers the same way, and
+//     the one thread holding the CTA's candidate writes its row into the
+//     CTA's exchange slot (sixteen warps each storing a whole row cost a
+//     quarter of the column time);
+//  3. (clusters only) once that thread has arrived on a local mbarrier, warp
+//     0 bulk-copies the slot, and row j if this CTA owns it, into every
+//     other CTA's shared memory, each copy completing bytes on the
+//     receiver's mbarrier, and waits for the column's bytes; a second CTA
+//     barrier releases the other warps, and every warp reduces the C slot
+//     headers to the winner;
 //  4. each thread exchanges, scales and updates its own rows and forms its
 //     candidate for the next column.
 // Same pivot order, tie rule, null-column and NaN handling as
@@ -331,12 +333,20 @@ struct RSlot {
   double v[W];
 };
 
-// Layout: wslot [2][16] (the warps' candidates), cslot [2][C] (the CTAs'
-// candidates), rowj [2][W], two mbarriers, then one 32 x (W + 1) staging
+// A warp's candidate: ordering key and row.
+struct RHdr {
+  unsigned long long key;
+  int row;
+  int pad;
+};
+
+// Layout: hdr [2][16] (the warps' candidates), cslot [2][C] (the CTAs'
+// candidates with their rows), rowj [2][W], four mbarriers (peers' copies
+// and this CTA's slot written, by parity), then one 32 x (W + 1) staging
 // tile per warp for the coalesced load and store of the slab.
 __host__ __device__ inline size_t rleaf_tile_offset(int w, int C) {
   const size_t slot = 16 + 8 * (size_t)w;
-  return 2 * (RLEAF_NW + (size_t)C) * slot + 16 * (size_t)w + 16;
+  return 2 * RLEAF_NW * sizeof(RHdr) + 2 * (size_t)C * slot + 16 * (size_t)w + 32;
 }
 __host__ __device__ inline size_t rleaf_smem_bytes(int w, int C) {
   return rleaf_tile_offset(w, C) + sizeof(double) * RLEAF_NW * 32 * ((size_t)w + 1) + 128;
@@ -552,16 +562,19 @@ __global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs 
   const int C = (int)cluster.num_blocks();
   const int c = (int)cluster.block_rank();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  Slot* wslot = reinterpret_cast<Slot*>(rleaf_smem);                               // [2][16]
-  Slot* cslot = wslot + 2 * RLEAF_NW;                                              // [2][C]
+  RHdr* hdr = reinterpret_cast<RHdr*>(rleaf_smem);                                 // [2][16]
+  Slot* cslot = reinterpret_cast<Slot*>(rleaf_smem + 2 * RLEAF_NW * sizeof(RHdr));   // [2][C]
   double* rowj = reinterpret_cast<double*>(cslot + 2 * C);                         // [2][W]
-  const uint32_t full0 = smem_u32(rowj + 2 * W);                                   // 2 mbarriers
+  const uint32_t full0 = smem_u32(rowj + 2 * W);                                   // 2 mbarriers: peers' copies
+  const uint32_t ready0 = full0 + 16;                                              // 2: own slot written
   const int r0 = c * a.R;
   const int rows = max(0, min(a.R, a.M - r0));
   if (C > 1) {
     if (tid == 0) {
       mbar_init(full0, 1);
       mbar_init(full0 + 8, 1);
+      mbar_init(ready0, 1);
+      mbar_init(ready0 + 8, 1);
       fence_barrier_init();
     }
     cluster.sync();  // every CTA's barriers exist before the first copy
@@ -590,17 +603,17 @@ __global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs 
   for (int j = 0; j < W; ++j) {
     const int par = j & 1;
     const bool own_j = j >= r0 && j < r0 + rows;  // uniform in the CTA
-    // ---- 1. the warp's candidate into its slot; row j by its owner
+    // ---- 1. the warp's candidate header; row j by its owner
     {
       unsigned long long wk = rleaf_key(bv, bi);
       int wi = bi;
       rleaf_argmax_warp(wk, wi);
-      Slot* ws = wslot + par * RLEAF_NW + warp;
       if (wi == INT_MAX ? lane == 0 : wi == bi) {
-        ws->key = wk;
-        ws->row = wi;
-        if (wi != INT_MAX) rleaf_store_row<W, RPT>(rv, bk, ws->v);
-        if (C > 1) fence_proxy_async_smem();
+        RHdr h;
+        h.key = wk;
+        h.row = wi;
+        h.pad = 0;
+        hdr[par * RLEAF_NW + warp] = h;
       }
       if (own_j && tid == ((j - r0) & (RLEAF_THREADS - 1))) {
         rleaf_store_row<W, RPT>(rv, (j - r0) / RLEAF_THREADS, rowj + par * W);
@@ -608,17 +621,25 @@ __global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs 
       }
     }
     __syncthreads();
-    // ---- 2. the CTA's candidate (every warp, same data, same result)
-    const Slot* best;
+    // ---- 2. the CTA's candidate (every warp, same data, same result); its
+    // holder writes it, with its row, into the CTA's slot
+    Slot* mine = cslot + par * C + c;
+    const Slot* best = mine;
     int r;
     {
-      const Slot* hs = wslot + par * RLEAF_NW + (lane < RLEAF_NW ? lane : 0);
+      const RHdr* hs = hdr + par * RLEAF_NW + (lane < RLEAF_NW ? lane : 0);
       unsigned long long ck = lane < RLEAF_NW ? hs->key : 0ull;
-      const int mine = lane < RLEAF_NW ? hs->row : INT_MAX;
-      int ci = mine;
+      int ci = lane < RLEAF_NW ? hs->row : INT_MAX;
       rleaf_argmax_warp(ck, ci);
-      const unsigned m = __ballot_sync(0xffffffffu, lane < RLEAF_NW && mine == ci);
-      best = wslot + par * RLEAF_NW + (m ? __ffs(m) - 1 : 0);
+      if (ci == INT_MAX ? tid == 0 : ci == bi) {
+        mine->key = ck;
+        mine->row = ci;
+        if (ci != INT_MAX) rleaf_store_row<W, RPT>(rv, bk, mine->v);
+        if (C > 1) {
+          fence_proxy_async_smem();
+          mbar_arrive(ready0 + 8 * par);
+        }
+      }
       r = ci;
     }
     // ---- 3. exchange with the other CTAs of the cluster
@@ -627,32 +648,36 @@ __global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs 
       const uint32_t ph = (uint32_t)((j >> 1) & 1);
       bool ok = true;
       if (warp == 0) {
-        if (lane < C && lane != c) {
-          const uint32_t rbar = mapa_shared(fullp, (uint32_t)lane);
-          bulk_copy_to_peer(mapa_shared(smem_u32(cslot + par * C + c), (uint32_t)lane), smem_u32(best),
-                            (uint32_t)sizeof(Slot), rbar);
-          if (own_j)
-            bulk_copy_to_peer(mapa_shared(smem_u32(rowj + par * W), (uint32_t)lane), smem_u32(rowj + par * W),
-                              (uint32_t)(8 * W), rbar);
+        ok = mbar_wait(ready0 + 8 * par, ph, a.err, 22);  // the slot is written
+        if (ok) {
+          if (lane < C && lane != c) {
+            const uint32_t rbar = mapa_shared(fullp, (uint32_t)lane);
+            bulk_copy_to_peer(mapa_shared(smem_u32(mine), (uint32_t)lane), smem_u32(mine), (uint32_t)sizeof(Slot),
+                              rbar);
+            if (own_j)
+              bulk_copy_to_peer(mapa_shared(smem_u32(rowj + par * W), (uint32_t)lane), smem_u32(rowj + par * W),
+                                (uint32_t)(8 * W), rbar);
+          }
+          if (lane == 0) mbar_arrive_expect_tx(fullp, (uint32_t)((C - 1) * sizeof(Slot) + (own_j ? 0 : 8 * W)));
+          ok = mbar_wait_cluster(fullp, ph, a.err, 21);
         }
-        if (lane == 0) mbar_arrive_expect_tx(fullp, (uint32_t)((C - 1) * sizeof(Slot) + (own_j ? 0 : 8 * W)));
-        ok = mbar_wait_cluster(fullp, ph, a.err, 21);
       }
-      // the CTA leaves the loop together if the (bounded) wait ran out
+      // the CTA leaves the loop together if a (bounded) wait ran out
       if (__syncthreads_or(ok ? 0 : 1)) {
         done = false;
         break;
       }
       if (warp != 0) (void)mbar_try_wait_cluster(fullp, ph);  // acquire of the completed phase
-      const Slot* hs = lane < C ? (lane == c ? best : cslot + par * C + lane) : best;
+      const Slot* hs = cslot + par * C + (lane < C ? lane : c);
       unsigned long long gk = lane < C ? hs->key : 0ull;
-      const int mine = lane < C ? hs->row : INT_MAX;
-      int gi = mine;
+      const int gm = lane < C ? hs->row : INT_MAX;
+      int gi = gm;
       rleaf_argmax_warp(gk, gi);
-      const unsigned m = __ballot_sync(0xffffffffu, lane < C && mine == gi);
-      const int q = m ? __ffs(m) - 1 : c;
-      best = q == c ? best : cslot + par * C + q;
+      const unsigned m = __ballot_sync(0xffffffffu, lane < C && gm == gi);
+      best = cslot + par * C + (m ? __ffs(m) - 1 : c);
       r = gi;
+    } else {
+      __syncthreads();  // the CTA's candidate row is visible to every warp
     }
     const double* u = best->v;  // the pivot row
     const double* oldj = rowj + par * W;
@@ -664,7 +689,6 @@ __global__ void __launch_bounds__(RLEAF_THREADS, 1) lu_leaf_reg_kernel(LeafArgs 
     }
     const double piv = u[j];
     if (c == 0 && tid == 0) a.piv[j] = r - j;
-    if (tid == 0) s_r[j] = r;
     if (tid == 0) s_r[j] = r;
     bv = -1.0;
     bi = INT_MAX;
