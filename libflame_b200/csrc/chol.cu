@@ -30,6 +30,9 @@ constexpr int IB = 32;         // inner block
 constexpr int LDS = NB + 1;    // SMEM leading dimension (odd: spreads banks)
 constexpr int POTRF_THREADS = 256;
 constexpr int POTRF_SMEM = NB * LDS * 8;
+// Block columns of at most this many rows below the diagonal block are
+// solved by substitution; taller ones through inv(L11) and a DMMA GEMM.
+constexpr long CHOL_SUBST_ROWS = 4096;
 
 __device__ __forceinline__ bool guard_failed(const int* info) {
   return *((volatile const int*)info) != INT_MAX;
@@ -231,6 +234,9 @@ int chol_lower_enqueue(DMat A, cudaStream_t st) {
     FB_CK(cudaGetLastError());
     const long m2 = n - k - b;
     if (m2 <= 0) return FLA_SUCCESS;
+    // a short block column: forward substitution in one launch (the latency
+    // of the inverse, the copy and the product would dominate it)
+    if (m2 <= CHOL_SUBST_ROWS) return trsm_rlt_subst(at(k, k), at(k + b, k), ld, b, m2, info, (int)(k + b), s);
     const long ldl = (b + 1) & ~1L;  // TMA: 16-byte leading dimensions
     if (tri_inverse_lower(at(k, k), ld, b, false, Linv, ldl, s) != FLA_SUCCESS) return FLA_FAILURE;
     const long ldw = (m2 + 1) & ~1L;

@@ -246,6 +246,10 @@ int transpose_dev(const double* src, long lds, double* dst, long ldd, long m, lo
 // U12 := inv(L11) A12 (unit lower L11 of order b) on transposed storage:
 // L11(i, j) at Ls[j + i ld], A12(i, c) at X[c + i ld] (c < ncols), overwritten.
 int u12_subst(const double* Ls, double* X, long ld, int b, long ncols, cudaStream_t st);
+// X := X inv(L)^T (X ncols x b, L non-unit lower of order b <= 128, both
+// column-major with leading dimension ld), by forward substitution.
+int trsm_rlt_subst(const double* L, double* X, long ld, int b, long ncols, const int* guard, int guard_limit,
+                   cudaStream_t st);
 int laswp_t_dev(double* AT, long ldt, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
                 cudaStream_t st);
 int laswp_t_f32(float* AT, long ldt, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,

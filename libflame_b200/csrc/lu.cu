@@ -567,16 +567,34 @@ constexpr int U12_WARPS = 16;
 constexpr int U12_LDS = NBMAX + 1;  // odd stride: a half-warp reads 16 banks
 // shared memory for a triangle of order b: whole 32-row groups (the sweep
 // reads the rows of every group it touches)
-inline size_t u12_smem(int b) { return sizeof(double) * (size_t)((b + 31) & ~31) * U12_LDS; }
+// (and, after it, the reciprocals of the diagonal for the non-unit form)
+inline size_t u12_smem(int b) { return sizeof(double) * ((size_t)((b + 31) & ~31) * U12_LDS + NBMAX); }
 
-template <int RV>
+// NU = false: unit lower L11 with L11(i, j) at Ls[j + i ld] (the LU on A^T).
+// NU = true:  non-unit lower L11 with L11(i, j) at Ls[i + j ld] (column-
+//             major, the Cholesky's A21 := A21 inv(L11)^T, rows of A21 as
+//             the right-hand sides); each solved entry is first multiplied
+//             by the reciprocal of its pivot (dtrsm's R,L,T,N case).
+// Returns at once when *guard holds a failing column below guard_limit.
+template <int RV, bool NU>
 __global__ void __launch_bounds__(U12_WARPS * 32) u12_subst_kernel(const double* __restrict__ Ls,
                                                                     double* __restrict__ X, long ld, int b,
-                                                                    int ncols) {
+                                                                    int ncols, const int* guard, int guard_limit) {
   extern __shared__ double sL[];  // sL[i * U12_LDS + j] = L11(i, j), rows i < 32 ceil(b / 32)
+  double* sR = sL + ((b + 31) & ~31) * U12_LDS;
+  if (guard && *((volatile const int*)guard) < guard_limit) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int i = warp; i < b; i += U12_WARPS)
-    for (int j = lane; j < b; j += 32) sL[i * U12_LDS + j] = Ls[j + (long)i * ld];
+  if (NU) {
+    for (int j = warp; j < b; j += U12_WARPS)
+      for (int i = lane; i < b; i += 32) {
+        const double v = Ls[i + (long)j * ld];
+        sL[i * U12_LDS + j] = v;
+        if (i == j) sR[j] = 1.0 / v;
+      }
+  } else {
+    for (int i = warp; i < b; i += U12_WARPS)
+      for (int j = lane; j < b; j += 32) sL[i * U12_LDS + j] = Ls[j + (long)i * ld];
+  }
   __syncthreads();
   const int c0 = (blockIdx.x * U12_WARPS + warp) * RV;
   if (c0 >= ncols) return;
@@ -600,6 +618,14 @@ __global__ void __launch_bounds__(U12_WARPS * 32) u12_subst_kernel(const double*
       double y[RV];
 #pragma unroll
       for (int v = 0; v < RV; ++v) y[v] = __shfl_sync(0xffffffffu, r[slot][v], jj);
+      if (NU) {
+        const double rc = sR[j];
+#pragma unroll
+        for (int v = 0; v < RV; ++v) {
+          y[v] *= rc;
+          if (lane == jj) r[slot][v] = y[v];
+        }
+      }
       const double l0 = sL[(lane + 32 * slot) * U12_LDS + j];
       if (lane > jj) {
 #pragma unroll
@@ -624,15 +650,38 @@ __global__ void __launch_bounds__(U12_WARPS * 32) u12_subst_kernel(const double*
     }
 }
 
-template <int RV>
-void u12_subst_launch(const double* Ls, double* X, long ld, int b, int ncols, cudaStream_t st) {
+template <int RV, bool NU = false>
+void u12_subst_launch(const double* Ls, double* X, long ld, int b, int ncols, cudaStream_t st,
+                      const int* guard = nullptr, int guard_limit = 0) {
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(u12_subst_kernel<RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)u12_smem(NBMAX));
+    cudaFuncSetAttribute(u12_subst_kernel<RV, NU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)u12_smem(NBMAX));
     attr = true;
   }
   const unsigned grid = (unsigned)((ncols + U12_WARPS * RV - 1) / (U12_WARPS * RV));
-  u12_subst_kernel<RV><<<grid, U12_WARPS * 32, u12_smem(b), st>>>(Ls, X, ld, b, ncols);
+  u12_subst_kernel<RV, NU><<<grid, U12_WARPS * 32, u12_smem(b), st>>>(Ls, X, ld, b, ncols, guard, guard_limit);
+}
+
+// X := X inv(L)^T for an ncols x b block X (column-major, ld ld) and a
+// non-unit lower L of order b <= 128 (column-major, same ld): the
+// Cholesky's A21 := A21 inv(L11)^T by forward substitution in one launch.
+int trsm_rlt_subst(const double* L, double* X, long ld, int b, long ncols, const int* guard, int guard_limit,
+                   cudaStream_t st) {
+  if (ncols <= 0 || b <= 0) return FLA_SUCCESS;
+  if (b > NBMAX) {
+    set_last_error("trsm_rlt_subst: triangle wider than 128");
+    return FLA_FAILURE;
+  }
+  const int sms = ctx().num_sms;
+  const int ps = prof_begin(st);
+  if (ncols <= (long)sms * U12_WARPS) u12_subst_launch<1, true>(L, X, ld, b, (int)ncols, st, guard, guard_limit);
+  else if (ncols <= (long)sms * U12_WARPS * 2) u12_subst_launch<2, true>(L, X, ld, b, (int)ncols, st, guard, guard_limit);
+  else if (ncols <= (long)sms * U12_WARPS * 4) u12_subst_launch<4, true>(L, X, ld, b, (int)ncols, st, guard, guard_limit);
+  else u12_subst_launch<8, true>(L, X, ld, b, (int)ncols, st, guard, guard_limit);
+  prof_end(ps, st, PROF_TRSM, (double)ncols * b * b);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
 }
 
 // U12 := inv(L11) A12 for ncols columns (layout above), any b: blocks of
