@@ -584,16 +584,33 @@ __global__ void __launch_bounds__(U12_WARPS * 32) u12_subst_kernel(const double*
   double* sR = sL + ((b + 31) & ~31) * U12_LDS;
   if (guard && *((volatile const int*)guard) < guard_limit) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (NU) {
-    for (int j = warp; j < b; j += U12_WARPS)
-      for (int i = lane; i < b; i += 32) {
-        const double v = Ls[i + (long)j * ld];
-        sL[i * U12_LDS + j] = v;
-        if (i == j) sR[j] = 1.0 / v;
+  // The triangle: lanes run along its contiguous index e (a column of L11
+  // for NU, a row for the transposed storage), each warp takes every
+  // sixteenth line o; sixteen loads per lane are in flight before they are
+  // stored (one memory round trip per batch, not per entry).
+  for (int o0 = warp; o0 < b; o0 += U12_WARPS * 4) {
+    double v[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int o = o0 + a * U12_WARPS, e = lane + 32 * q;
+        v[a][q] = (o < b && e < b) ? Ls[e + (long)o * ld] : 0.0;
       }
-  } else {
-    for (int i = warp; i < b; i += U12_WARPS)
-      for (int j = lane; j < b; j += 32) sL[i * U12_LDS + j] = Ls[j + (long)i * ld];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int o = o0 + a * U12_WARPS, e = lane + 32 * q;
+        if (o < b && e < b) {
+          if (NU) {
+            sL[e * U12_LDS + o] = v[a][q];  // L11(e, o)
+            if (e == o) sR[o] = 1.0 / v[a][q];
+          } else {
+            sL[o * U12_LDS + e] = v[a][q];  // L11(o, e)
+          }
+        }
+      }
   }
   __syncthreads();
   const int c0 = (blockIdx.x * U12_WARPS + warp) * RV;
