@@ -250,6 +250,9 @@ int u12_subst(const double* Ls, double* X, long ld, int b, long ncols, cudaStrea
 // column-major with leading dimension ld), by forward substitution.
 int trsm_rlt_subst(const double* L, double* X, long ld, int b, long ncols, const int* guard, int guard_limit,
                    cudaStream_t st);
+// The same with an FP32 X (ld ldx) and an FP64 L (ld ldl), solved in FP64.
+int trsm_rlt_subst_f32(const double* L, long ldl, float* X, long ldx, int b, long ncols, const int* guard,
+                       int guard_limit, cudaStream_t st);
 int laswp_t_dev(double* AT, long ldt, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,
                 cudaStream_t st);
 int laswp_t_f32(float* AT, long ldt, int row0, const int* d_piv, int npiv, int c0, int n0, int c1, int n1,

@@ -576,10 +576,14 @@ inline size_t u12_smem(int b) { return sizeof(double) * ((size_t)((b + 31) & ~31
 //             the right-hand sides); each solved entry is first multiplied
 //             by the reciprocal of its pivot (dtrsm's R,L,T,N case).
 // Returns at once when *guard holds a failing column below guard_limit.
-template <int RV, bool NU>
+// TX: the element type of X (float for the low-precision Cholesky's
+// factors: loaded into FP64, solved in FP64, rounded back); X has its own
+// leading dimension ldx.
+template <int RV, bool NU, typename TX = double>
 __global__ void __launch_bounds__(U12_WARPS * 32) u12_subst_kernel(const double* __restrict__ Ls,
-                                                                    double* __restrict__ X, long ld, int b,
-                                                                    int ncols, const int* guard, int guard_limit) {
+                                                                    TX* __restrict__ X, long ld, int b,
+                                                                    int ncols, const int* guard, int guard_limit,
+                                                                    long ldx) {
   extern __shared__ double sL[];  // sL[i * U12_LDS + j] = L11(i, j), rows i < 32 ceil(b / 32)
   double* sR = sL + ((b + 31) & ~31) * U12_LDS;
   if (guard && *((volatile const int*)guard) < guard_limit) return;
@@ -621,7 +625,7 @@ __global__ void __launch_bounds__(U12_WARPS * 32) u12_subst_kernel(const double*
 #pragma unroll
     for (int v = 0; v < RV; ++v) {
       const int i = lane + 32 * m, c = c0 + v;
-      r[m][v] = (i < b && c < ncols) ? X[c + (long)i * ld] : 0.0;
+      r[m][v] = (i < b && c < ncols) ? (double)X[c + (long)i * ldx] : 0.0;
     }
   // rows at or beyond b hold zeros and read unset shared memory of their
   // group: they are never written back; groups at or beyond b are skipped
@@ -663,20 +667,22 @@ __global__ void __launch_bounds__(U12_WARPS * 32) u12_subst_kernel(const double*
 #pragma unroll
     for (int v = 0; v < RV; ++v) {
       const int i = lane + 32 * m, c = c0 + v;
-      if (i < b && c < ncols) X[c + (long)i * ld] = r[m][v];
+      if (i < b && c < ncols) X[c + (long)i * ldx] = (TX)r[m][v];
     }
 }
 
-template <int RV, bool NU = false>
-void u12_subst_launch(const double* Ls, double* X, long ld, int b, int ncols, cudaStream_t st,
-                      const int* guard = nullptr, int guard_limit = 0) {
+template <int RV, bool NU = false, typename TX = double>
+void u12_subst_launch(const double* Ls, TX* X, long ld, int b, int ncols, cudaStream_t st,
+                      const int* guard = nullptr, int guard_limit = 0, long ldx = -1) {
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(u12_subst_kernel<RV, NU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)u12_smem(NBMAX));
+    cudaFuncSetAttribute(u12_subst_kernel<RV, NU, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)u12_smem(NBMAX));
     attr = true;
   }
   const unsigned grid = (unsigned)((ncols + U12_WARPS * RV - 1) / (U12_WARPS * RV));
-  u12_subst_kernel<RV, NU><<<grid, U12_WARPS * 32, u12_smem(b), st>>>(Ls, X, ld, b, ncols, guard, guard_limit);
+  u12_subst_kernel<RV, NU, TX><<<grid, U12_WARPS * 32, u12_smem(b), st>>>(Ls, X, ld, b, ncols, guard, guard_limit,
+                                                                         ldx < 0 ? ld : ldx);
 }
 
 // X := X inv(L)^T for an ncols x b block X (column-major, ld ld) and a
@@ -695,6 +701,32 @@ int trsm_rlt_subst(const double* L, double* X, long ld, int b, long ncols, const
   else if (ncols <= (long)sms * U12_WARPS * 2) u12_subst_launch<2, true>(L, X, ld, b, (int)ncols, st, guard, guard_limit);
   else if (ncols <= (long)sms * U12_WARPS * 4) u12_subst_launch<4, true>(L, X, ld, b, (int)ncols, st, guard, guard_limit);
   else u12_subst_launch<8, true>(L, X, ld, b, (int)ncols, st, guard, guard_limit);
+  prof_end(ps, st, PROF_TRSM, (double)ncols * b * b);
+  count_launch();
+  FB_CK(cudaGetLastError());
+  return FLA_SUCCESS;
+}
+
+// The same for an FP32 X (ld ldx) against an FP64 L (ld ldl): the
+// low-precision Cholesky's A21 := A21 inv(L11)^T with L11 its FP64
+// diagonal factor, solved in FP64 and rounded to FP32.
+int trsm_rlt_subst_f32(const double* L, long ldl, float* X, long ldx, int b, long ncols, const int* guard,
+                       int guard_limit, cudaStream_t st) {
+  if (ncols <= 0 || b <= 0) return FLA_SUCCESS;
+  if (b > NBMAX) {
+    set_last_error("trsm_rlt_subst_f32: triangle wider than 128");
+    return FLA_FAILURE;
+  }
+  const int sms = ctx().num_sms;
+  const int ps = prof_begin(st);
+  if (ncols <= (long)sms * U12_WARPS)
+    u12_subst_launch<1, true, float>(L, X, ldl, b, (int)ncols, st, guard, guard_limit, ldx);
+  else if (ncols <= (long)sms * U12_WARPS * 2)
+    u12_subst_launch<2, true, float>(L, X, ldl, b, (int)ncols, st, guard, guard_limit, ldx);
+  else if (ncols <= (long)sms * U12_WARPS * 4)
+    u12_subst_launch<4, true, float>(L, X, ldl, b, (int)ncols, st, guard, guard_limit, ldx);
+  else
+    u12_subst_launch<8, true, float>(L, X, ldl, b, (int)ncols, st, guard, guard_limit, ldx);
   prof_end(ps, st, PROF_TRSM, (double)ncols * b * b);
   count_launch();
   FB_CK(cudaGetLastError());

@@ -526,8 +526,10 @@ struct LpWork {
   uint16_t* PW[2] = {nullptr, nullptr};  // Cholesky: packed outer panels (n x NBO), ping-pong
   long plane = 0, planeX = 0;  // lo-plane offsets (LP_TF32X3: floats; LP_FP16X3: 16-bit elements)
   long planeW = 0;
-  double* P64 = nullptr;    // FP64 panel (MB x n)
+  double* P64 = nullptr;    // FP64 panel (MB x n); Cholesky: the FP64 diagonal
+                            // factors, block q at q MB (MB + 1), ld MB
   double* X64 = nullptr;    // FP64 inverse blocks (2 x MB x MB)
+  double* Xall = nullptr;   // Cholesky: inverses of all diagonal factors (q MB MB)
 };
 
 int lp_workspace(long n, LpFactor* f, LpWork* w) {
@@ -537,7 +539,8 @@ int lp_workspace(long n, LpFactor* f, LpWork* w) {
   const size_t pk = lp_packed_bytes(LP_TF32X3, (long)np, MB), px = lp_packed_bytes(LP_TF32X3, MB, MB);
   const size_t pw = lp_packed_bytes(LP_TF32X3, (long)np, NBO);
   char* p16 = (char*)ws_get(WS_LP1, 4 * pk + px + 2 * pw + 4096);
-  char* p64 = (char*)ws_get(WS_LP3, sizeof(double) * ((size_t)MB * np + 2 * (size_t)MB * MB) + 1024);
+  const size_t p64n = (size_t)(MB + 1) * (np + MB);  // P64 in either use
+  char* p64 = (char*)ws_get(WS_LP3, sizeof(double) * (p64n + 2 * (size_t)MB * MB + (size_t)MB * (np + MB)) + 1024);
   const long nblk = (n + MB - 1) / MB;
   char* pinv = (char*)ws_get(WS_LP4, sizeof(float) * 2 * (size_t)nblk * MB * MB + sizeof(double) * 2 * np +
                                          sizeof(int) * 2 * np + 1024);
@@ -553,7 +556,8 @@ int lp_workspace(long n, LpFactor* f, LpWork* w) {
   w->plane = (long)MB * (long)np;
   w->planeX = (long)MB * MB;
   w->P64 = (double*)p64;
-  w->X64 = w->P64 + (size_t)MB * np;
+  w->X64 = w->P64 + p64n;
+  w->Xall = w->X64 + 2 * (size_t)MB * MB;
   f->inv1 = (float*)pinv;
   f->inv2 = f->inv1 + (size_t)nblk * MB * MB;
   f->sr = (double*)(f->inv2 + (size_t)nblk * MB * MB);
@@ -733,24 +737,20 @@ int lp_chol_factor_shift(DMat A, bool upper, LowPrec prec, bool scale, double si
   int* info = cx.d_status + ST_INFO;
   auto at = [&](long i, long j) { return F + i + j * ldf; };
 
-  // 128-column sub-panel at column j: diagonal block in FP64, its inverse,
-  // and A21 := A21 inv(L11)^T
+  // 128-column sub-panel at column j: diagonal block in FP64 (kept, in the
+  // diagonal layout of P64, for the correction sweeps' inverses), then
+  // A21 := A21 inv(L11)^T by forward substitution in FP64 in one launch
+  // (rather than the inverse, two 16-bit packings and a tensor-core
+  // product on the panel's critical chain)
   auto sub = [&](long j, cudaStream_t s) -> int {
     const int b = (int)std::min<long>(MB, n - j);
-    const long kb = j / MB;
-    if (convert2d<double, float>(s, at(j, j), ldf, w.P64, MB, b, b) != FLA_SUCCESS) return FLA_FAILURE;
-    if (potrf_diag_dev(w.P64, MB, b, (int)j, s) != FLA_SUCCESS) return FLA_FAILURE;
-    if (tri_inverse(w.P64, MB, b, true, false, w.X64, MB, s) != FLA_SUCCESS) return FLA_FAILURE;
-    if (convert2d<float, double>(s, w.P64, MB, at(j, j), ldf, b, b) != FLA_SUCCESS) return FLA_FAILURE;
-    if (convert2d<float, double>(s, w.X64, MB, f->inv1 + kb * MB * MB, MB, b, b) != FLA_SUCCESS) return FLA_FAILURE;
+    double* L64 = w.P64 + (j / MB) * (long)MB * (MB + 1);
+    if (convert2d<double, float>(s, at(j, j), ldf, L64, MB, b, b) != FLA_SUCCESS) return FLA_FAILURE;
+    if (potrf_diag_dev(L64, MB, b, (int)j, s) != FLA_SUCCESS) return FLA_FAILURE;
+    if (convert2d<float, double>(s, L64, MB, at(j, j), ldf, b, b) != FLA_SUCCESS) return FLA_FAILURE;
     const long m2 = n - j - b;
     if (m2 <= 0) return FLA_SUCCESS;
-    // B(c, kk) = inv(L11)(c, kk)
-    if (pack16<double>(s, prec, w.X64, 1, MB, w.PX, MB, b, b, 1.f, w.planeX) != FLA_SUCCESS) return FLA_FAILURE;
-    if (pack16<float>(s, prec, at(j + b, j), 1, ldf, w.PC, MB, m2, b, 1.f, w.plane) != FLA_SUCCESS)
-      return FLA_FAILURE;
-    return lp_gemm(s, prec, m2, b, b, 1.f, w.PC, MB, w.PX, MB, 0.f, at(j + b, j), ldf, GEMM_FULL, 0, info,
-                   (int)(j + b), w.plane, w.planeX);
+    return trsm_rlt_subst_f32(L64, MB, at(j + b, j), ldf, b, m2, info, (int)(j + b), s);
   };
   // Outer panel at column k: its sub-panels, the first one updating the
   // second's columns, then the rows below the panel packed into PW.
@@ -794,6 +794,11 @@ int lp_chol_factor_shift(DMat A, bool upper, LowPrec prec, bool scale, double si
       return FLA_FAILURE;
     FB_CK(cudaStreamWaitEvent(st, ev_panel, 0));
   }
+  // inverses of every diagonal factor for the correction sweeps, in one
+  // launch off the factorization's chain, rounded to FP32
+  const long nblk = (n + MB - 1) / MB;
+  if (tri_inverse_blocks(w.P64, MB, n, true, false, w.Xall, st) != FLA_SUCCESS) return FLA_FAILURE;
+  if (convert2d<float, double>(st, w.Xall, MB, f->inv1, MB, MB, nblk * MB) != FLA_SUCCESS) return FLA_FAILURE;
   if (lp_couplings(f, st) != FLA_SUCCESS) return FLA_FAILURE;
   int inf = -1;
   if (status_read(&inf) != FLA_SUCCESS) return FLA_FAILURE;
