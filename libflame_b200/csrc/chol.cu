@@ -40,60 +40,117 @@ __device__ __forceinline__ bool guard_failed(const int* info) {
 
 // Factor the b x b (b <= 128) lower-triangular diagonal block at A (ld) in
 // place.  gcol = global index of its first column (for the info word).
-// Per 32-column step: (a) warp 0 factors the 32 x 32 diagonal block with one
-// row per lane in registers (the columns are broadcast by shuffles), (b) one
-// thread per row below solves X := X inv(L11)^T with its row in registers,
-// (c) the trailing lower triangle is updated by a 16 x 16 thread grid, each
-// thread a 6 x 6 interleaved tile (rows ty + 16a, columns tx + 16b), so the
-// shared-memory loads of one warp are broadcasts or consecutive words.
+// Per 32-column chunk: (a) warp 0 factors the 32 x 32 diagonal block with
+// one row per lane in registers, (b) one thread per row below solves
+// X := X inv(L11)^T with its row in registers, (c) the trailing lower
+// triangle of the block is updated, each thread a register tile of
+// interleaved rows and columns (the shared-memory loads of one warp are
+// broadcasts or consecutive words).  The update of the next chunk's 32
+// columns comes first; warp 0 then factors the next diagonal block while
+// the other seven warps update the columns beyond it.
+// The pivot chain of (a) carries register values only: the next pivot is
+// formed by its own lane from its own multiplier (fma(-l, l, a), the value
+// the shared-memory column broadcast gives) and shuffled; each pivot's
+// reciprocal square root is one rsqrt, its square root d * rsqrt(d).
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+// S[r + c*LDS] -= sum_k S[r + (jb+k)*LDS] S[c + (jb+k)*LDS] (k < w) for the
+// rows r in [r_lo, b) and columns c in [c_lo, c_hi), c <= r: thread (tx, ty)
+// of a TX x TY grid owns rows r_lo + ty + TY a (a < RA) and columns c_lo +
+// tx + TX q (q < CQ).
+template <int TX, int TY, int RA, int CQ>
+__device__ __forceinline__ void syrk_tile(double* S, int jb, int w, int r_lo, int c_lo, int c_hi, int b, int t) {
+  const int tx = t % TX, ty = t / TX;
+  double acc[RA][CQ];
+#pragma unroll
+  for (int a = 0; a < RA; ++a)
+#pragma unroll
+    for (int q = 0; q < CQ; ++q) acc[a][q] = 0.0;
+  int ri[RA], ci[CQ];
+#pragma unroll
+  for (int a = 0; a < RA; ++a) ri[a] = min(r_lo + ty + TY * a, b - 1);
+#pragma unroll
+  for (int q = 0; q < CQ; ++q) ci[q] = min(c_lo + tx + TX * q, b - 1);
+  for (int k = 0; k < w; ++k) {
+    const double* col = S + (jb + k) * LDS;
+    double xr[RA], xc[CQ];
+#pragma unroll
+    for (int a = 0; a < RA; ++a) xr[a] = col[ri[a]];
+#pragma unroll
+    for (int q = 0; q < CQ; ++q) xc[q] = col[ci[q]];
+#pragma unroll
+    for (int a = 0; a < RA; ++a)
+#pragma unroll
+      for (int q = 0; q < CQ; ++q) acc[a][q] += xr[a] * xc[q];
+  }
+#pragma unroll
+  for (int a = 0; a < RA; ++a)
+#pragma unroll
+    for (int q = 0; q < CQ; ++q) {
+      const int r = r_lo + ty + TY * a, c = c_lo + tx + TX * q;
+      if (r < b && c < c_hi && c <= r) S[r + c * LDS] -= acc[a][q];
+    }
+}
+
+// (a): warp 0 factors the w x w diagonal block at (jb, jb).  Every update is
+// unconditional (no divergent branches in the chain): a lane only ever reads
+// a[c] of its own row for c <= lane, and entries above the diagonal or past
+// w never reach those.  After a failing pivot the rest of the block is not
+// meaningful; the failing column is what is reported.
+__device__ __forceinline__ void potrf_diag32(double* S, int jb, int w, int lane, double* s_rinv, double* s_col,
+                                             int* s_fail) {
+  double a[IB];
+#pragma unroll
+  for (int c = 0; c < IB; ++c)  // rows past w: unit pivots
+    a[c] = (c <= lane && lane < w) ? S[(jb + lane) + (jb + c) * LDS] : (c == lane ? 1.0 : 0.0);
+  int fail = -1;
+  double d = __shfl_sync(0xffffffffu, a[0], 0);
+#pragma unroll
+  for (int j = 0; j < IB; ++j) {
+    if (!(d > 0.0) && fail < 0 && j < w) fail = j;  // <= 0 or NaN
+    const double rinv = rsqrt(d), sd = d * rinv;
+    a[j] = lane == j ? sd : (lane > j ? a[j] * rinv : a[j]);
+    if (lane == 0) s_rinv[j] = rinv;
+    const double lj = a[j];
+    if (j + 1 < IB) {
+      // lane j + 1's next pivot from its own multiplier, then the broadcast
+      const double dn = fma(-lj, lj, a[j + 1]);
+      d = __shfl_sync(0xffffffffu, dn, j + 1);
+      double* col = s_col + (j & 1) * IB;  // double-buffered column
+      col[lane] = lj;
+      __syncwarp();
+#pragma unroll
+      for (int c = j + 1; c < IB; ++c) a[c] = fma(-lj, col[c], a[c]);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < IB; ++c)
+    if (c <= lane && lane < w) S[(jb + lane) + (jb + c) * LDS] = a[c];
+  if (lane == 0 && fail >= 0) *s_fail = jb + fail;
+}
+
 __global__ void __launch_bounds__(POTRF_THREADS, 1) potrf_diag_kernel(double* A, long ld, int b, int gcol,
                                                                    int* info) {
   extern __shared__ double S[];  // S[r + c*LDS]
   __shared__ int s_fail;
   __shared__ double s_rinv[IB];
-  __shared__ double s_col[IB];
+  __shared__ double s_col[2 * IB];
   if (guard_failed(info)) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // load lower triangle (and diagonal); upper part of S is never read
-  load_block_f64<POTRF_THREADS, false>(A, ld, b, S, LDS, [](int r, int c) { return r >= c; });
+  // load the lower triangle (and diagonal) with asynchronous copies, all in
+  // flight at once; the upper part of S is never read
+  for (int c = warp; c < b; c += POTRF_THREADS / 32)
+    for (int r = c + lane; r < b; r += 32) cp_async8(S + r + c * LDS, A + r + (long)c * ld);
+  asm volatile("cp.async.wait_all;" ::: "memory");
   if (tid == 0) s_fail = -1;
   __syncthreads();
-
-  for (int jb = 0; jb < b; jb += IB) {
-    const int w = min(IB, b - jb);
-    // (a) unblocked Cholesky of the w x w diagonal block, row `lane` in a[].
-    //     Every update is unconditional (no divergent branches in the
-    //     chain): a lane only ever reads a[c] of its own row for c <= lane,
-    //     and entries above the diagonal or past w never reach those.
-    //     After a failing pivot the rest of the block is not meaningful;
-    //     the failing column is what is reported.
-    if (warp == 0) {
-      double a[IB];
-#pragma unroll
-      for (int c = 0; c < IB; ++c)  // rows past w: unit pivots
-        a[c] = (c <= lane && lane < w) ? S[(jb + lane) + (jb + c) * LDS] : (c == lane ? 1.0 : 0.0);
-      int fail = -1;
-#pragma unroll
-      for (int j = 0; j < IB; ++j) {
-        const double d = __shfl_sync(0xffffffffu, a[j], j);
-        if (!(d > 0.0) && fail < 0 && j < w) fail = j;  // <= 0 or NaN
-        const double sd = sqrt(d), rinv = 1.0 / sd;
-        a[j] = lane == j ? sd : (lane > j ? a[j] * rinv : a[j]);
-        if (lane == 0) s_rinv[j] = rinv;
-        const double lj = a[j];
-        s_col[lane] = lj;
-        __syncwarp();
-#pragma unroll
-        for (int c = j + 1; c < IB; ++c) a[c] -= lj * s_col[c];
-        __syncwarp();
-      }
-#pragma unroll
-      for (int c = 0; c < IB; ++c)
-        if (c <= lane && lane < w) S[(jb + lane) + (jb + c) * LDS] = a[c];
-      if (lane == 0 && fail >= 0) s_fail = jb + fail;
-    }
-    __syncthreads();
+  if (warp == 0) potrf_diag32(S, 0, min(IB, b), lane, s_rinv, s_col, &s_fail);
+  __syncthreads();
+  for (int jb = 0;;) {
     if (s_fail >= 0) break;
+    const int w = min(IB, b - jb);
     const int r0 = jb + w;  // first row below the diagonal block
     // (b) rows below: X := X inv(L11)^T, one thread per row (right-looking,
     //     multiply by the reciprocal of the pivot like dtrsm R,L,T,N).
@@ -113,43 +170,20 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) potrf_diag_kernel(double* A,
         if (c < w) S[r + (jb + c) * LDS] = x[c];
     }
     __syncthreads();
-    // (c) trailing lower triangle of the block: S22 -= X X^T
-    const int m2 = b - r0;
-    if (m2 > 0) {
-      const int tx = tid & 15, ty = tid >> 4;
-      double acc[6][6];
-#pragma unroll
-      for (int i = 0; i < 6; ++i)
-#pragma unroll
-        for (int j = 0; j < 6; ++j) acc[i][j] = 0.0;
-      int ri[6], ci[6];
-#pragma unroll
-      for (int i = 0; i < 6; ++i) {
-        ri[i] = min(r0 + ty + 16 * i, b - 1);
-        ci[i] = min(r0 + tx + 16 * i, b - 1);
-      }
-      for (int k = 0; k < w; ++k) {
-        const double* col = S + (jb + k) * LDS;
-        double xr[6], xc[6];
-#pragma unroll
-        for (int i = 0; i < 6; ++i) {
-          xr[i] = col[ri[i]];
-          xc[i] = col[ci[i]];
-        }
-#pragma unroll
-        for (int i = 0; i < 6; ++i)
-#pragma unroll
-          for (int j = 0; j < 6; ++j) acc[i][j] += xr[i] * xc[j];
-      }
-#pragma unroll
-      for (int i = 0; i < 6; ++i)
-#pragma unroll
-        for (int j = 0; j < 6; ++j) {
-          const int r = r0 + ty + 16 * i, c = r0 + tx + 16 * j;
-          if (r < b && c <= r) S[r + c * LDS] -= acc[i][j];
-        }
+    if (r0 >= b) break;
+    const int w2 = min(IB, b - r0);
+    // (c) first the next chunk's columns (all rows below r0) ...
+    syrk_tile<32, 8, 12, 1>(S, jb, w, r0, r0, r0 + w2, b, tid);
+    __syncthreads();
+    // ... then warp 0 factors the next diagonal block while the other warps
+    // update the columns beyond it
+    if (warp == 0) {
+      potrf_diag32(S, r0, w2, lane, s_rinv, s_col, &s_fail);
+    } else if (r0 + w2 < b) {
+      syrk_tile<16, 14, 5, 4>(S, jb, w, r0 + w2, r0 + w2, b, b, tid - 32);
     }
     __syncthreads();
+    jb = r0;
   }
   // write back the lower triangle (the strictly upper part of A is untouched)
   for (int c = warp; c < b; c += POTRF_THREADS / 32)
