@@ -419,8 +419,8 @@ __global__ void __launch_bounds__(DT, 1) chol_batched_dmma_kernel(BatchArgs<doub
             fail = c;
             break;
           }
-          const double sq = sqrt(piv);
-          const double rs = 1.0 / sq;
+          const double rs = rsqrt(piv);  // one sequence: the chain's latency
+          const double sq = piv * rs;
           const double nc = lane == c ? sq : (lane > c ? dc * rs : dc);  // L(lane, c)
 #pragma unroll
           for (int q = 0; q < DNB; ++q)
