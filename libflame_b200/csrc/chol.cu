@@ -15,6 +15,7 @@
 // src/base/flamec/blis/include/blis_macro_defs.h:134-136) records the
 // zero-based global column in the status block; every later kernel of the
 // factorization sees it and returns without touching memory.
+#include <algorithm>
 #include <climits>
 #include <cstdlib>
 
@@ -32,7 +33,15 @@ constexpr int POTRF_THREADS = 256;
 constexpr int POTRF_SMEM = NB * LDS * 8;
 // Block columns of at most this many rows below the diagonal block are
 // solved by substitution; taller ones through inv(L11) and a DMMA GEMM.
-constexpr long CHOL_SUBST_ROWS = 4096;
+// FLA_B200_CHOL_SUBST_ROWS overrides it for tuning.
+long chol_subst_rows() {
+  static long v = -1;
+  if (v < 0) {
+    v = 4096;
+    if (const char* e = std::getenv("FLA_B200_CHOL_SUBST_ROWS")) v = std::max(0L, std::atol(e));
+  }
+  return v;
+}
 
 __device__ __forceinline__ bool guard_failed(const int* info) {
   return *((volatile const int*)info) != INT_MAX;
@@ -270,7 +279,7 @@ int chol_lower_enqueue(DMat A, cudaStream_t st) {
     if (m2 <= 0) return FLA_SUCCESS;
     // a short block column: forward substitution in one launch (the latency
     // of the inverse, the copy and the product would dominate it)
-    if (m2 <= CHOL_SUBST_ROWS) return trsm_rlt_subst(at(k, k), at(k + b, k), ld, b, m2, info, (int)(k + b), s);
+    if (m2 <= chol_subst_rows()) return trsm_rlt_subst(at(k, k), at(k + b, k), ld, b, m2, info, (int)(k + b), s);
     const long ldl = (b + 1) & ~1L;  // TMA: 16-byte leading dimensions
     if (tri_inverse_lower(at(k, k), ld, b, false, Linv, ldl, s) != FLA_SUCCESS) return FLA_FAILURE;
     const long ldw = (m2 + 1) & ~1L;
